@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Throughput of the PLM/minmod + HLLC + SSP-RK2 hydro step on B200.
+
+Workload: 3D 256^3 periodic box (16,777,216 cells), seeded smooth random state,
+gamma = 5/3, CFL 0.4; each step is one SSP-RK2 step with the CFL dt recomputed
+on the device from the new state.  Metric: Mcell-updates/s (cells x steps / s),
+whole job.  Both precision modes run: VB_MIXED (float32 reconstruction and
+HLLC, float64 state) is the headline `value`; VB_FP64 (bit-identical to the
+reference's float64 arithmetic) is reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 the script runs under torchrun, one rank per GPU; every rank
+integrates its own independent 256^3 instance (weak scaling, no data-path
+collective) and rank 0 prints the max-over-ranks timing.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "vespa.jl_b200")]
+
+METRIC = ("Mcell-updates/s 3D 256³ PLM+HLLC RK2 (fp64 vs fp32/fp64 split); %HBM; adj/fwd")
+UNIT = "Mcell-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+BYTES_PER_CELL_STAGE = {1: 80, 2: 120}  # 5 float64 fields: stage 1 R(U)+W(U1), stage 2 R(U1)+R(U)+W(U)
+DATA = ("synthetic: seeded smooth random periodic state (rho = 1 + 0.3 x mean of 8 random sine "
+        "modes, velocity components uniform in [-0.5, 0.5], p = 1 + 0.2 U[-1, 1]); no dataset")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256, help="cells per axis of the cube")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- ranks
+class Ranks:
+    def __init__(self, n_gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.dist = dist
+            self.torch = torch
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier(device_ids=[self.local])
+
+    def max(self, x: float) -> float:
+        if not self.dist:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.dist:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        self.dist.all_reduce(t)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel: str, cells: int):
+    """Per-launch DRAM traffic of `kernel` scaled to `cells`, from the committed
+    ncu summary (profiles/traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)[kernel]
+        return float(d["bytes_per_cell"]) * cells
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+# ----------------------------------------------------------------- CPU baseline
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def oracle_rate(n: int, steps: int, budget_s: float, nthreads: int):
+    """Oracle (per-cell gather, OpenMP) Mcell-updates/s on an n^3 sample of the
+    benchmark's generator; runs up to `steps` RK2 steps or until `budget_s`."""
+    from oracle import oracle as O
+    import vespa_b200 as vb
+    prob = vb.smooth_random_problem((n, n, n))
+    U = vb.initial_state(prob)
+    g = O.grid_from_problem(prob)
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        dt = O.compute_dt(g, U)
+        O.step(g, U, dt, mode=1, nthreads=nthreads)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return n ** 3 * done / el / 1e6, done, el
+
+
+def choose_sample(nthreads: int, target_s: float):
+    """Largest cube from the ladder whose single step fits target_s."""
+    from oracle import oracle as O
+    O.build()
+    rate, _, _ = oracle_rate(32, 1, 60.0, nthreads)  # Mcell-updates/s estimate
+    n = 32
+    for cand in (48, 64, 96, 128, 192, 256):
+        if cand ** 3 / (rate * 1e6) <= target_s:
+            n = cand
+    return n, rate
+
+
+def cpu_baseline(nthreads: int) -> dict:
+    n, _ = choose_sample(nthreads, 6.0)
+    rate, done, el = oracle_rate(n, 64, 15.0, nthreads)
+    return {"value": round(rate, 3), "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{done} RK2 step(s) of a {n}^3 periodic box from the same generator "
+                      f"({el:.1f} s), C oracle per-cell gather with OpenMP"}
+
+
+def run_reference(args, ranks: Ranks):
+    """--impl reference: the CPU restatement of the reference's algorithm (the
+    reference's Julia path cannot run on this box) on all host cores."""
+    if ranks.rank != 0:
+        return
+    nthreads = cpu_threads()
+    n, rate0 = choose_sample(nthreads, 4.0)
+    from oracle import oracle as O
+    import vespa_b200 as vb
+    prob = vb.smooth_random_problem((n, n, n))
+    U = vb.initial_state(prob)
+    g = O.grid_from_problem(prob)
+    for _ in range(args.warmup):
+        O.step(g, U, O.compute_dt(g, U), mode=1, nthreads=nthreads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.step(g, U, O.compute_dt(g, U), mode=1, nthreads=nthreads)
+    el = time.perf_counter() - t0
+    value = n ** 3 * args.steps / el / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(el / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+        "config": {"workload": f"3D periodic PLM/minmod+HLLC SSP-RK2, {n}^3 sample per step of the "
+                               f"256^3 workload (CPU-bounded), CFL 0.4, gamma 5/3",
+                   "cells_per_step": n ** 3, "parallelism": f"{nthreads} host threads"},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": nthreads,
+                         "kind": "port",
+                         "sample": f"{args.steps} timed RK2 steps of a {n}^3 box; the "
+                                   "reference's Julia path cannot run here (no Julia), so the "
+                                   "C restatement of its algorithm stands in"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- our arm
+def run_ours(args, ranks: Ranks):
+    import numpy as np
+    import vespa_b200 as vb
+
+    n = args.n
+    cells = n ** 3
+    K, W = args.steps, args.warmup
+    ctx = vb.Context(ranks.local)
+    prob = vb.smooth_random_problem((n, n, n), seed=vb.problem.DEFAULT_SEED + ranks.rank)
+    U0 = vb.initial_state(prob)
+    mesh = vb.B200Mesh(prob.dims, prob.domain)
+    out = {}
+    clocks = None
+    for prec in ("fp64", "mixed"):
+        sim = vb.Simulation(mesh, prob, precision=prec, ctx=ctx, initial=U0)
+        vb.run_steps_async(sim, W)
+        ctx.synchronize()
+        ranks.barrier()
+        sampler = ClockSampler(ranks.local) if prec == "mixed" else None
+        if sampler:
+            sampler.start()
+        l0 = ctx.launch_count
+        ctx.mark(0)
+        vb.run_steps_async(sim, K)
+        ctx.mark(1)
+        ms = ctx.elapsed_ms(0, 1)
+        launches = ctx.launch_count - l0
+        if sampler:
+            clocks = sampler.stop()
+        ranks.barrier()
+        ms_max = ranks.max(ms)
+        out[prec] = {"ms": ms_max, "launches": launches, **sim.profile_step(5)}
+        sim.close()
+
+    # end to end through the public API: pinned host state in, K steps, state out
+    import torch
+    h_in = torch.empty((5, cells), dtype=torch.float64, pin_memory=True)
+    h_out = torch.empty((5, cells), dtype=torch.float64, pin_memory=True)
+    h_in.numpy()[...] = U0
+    sim = vb.Simulation(mesh, prob, precision="mixed", ctx=ctx, initial=U0)
+    ranks.barrier()
+    ctx.mark(2)
+    sim.upload(h_in.numpy())
+    vb.evolve(sim, tfinal=math.inf, max_steps=K)
+    sim.state(out=h_out.numpy())
+    ctx.mark(3)
+    e2e_ms = ranks.max(ctx.elapsed_ms(2, 3))
+    sim.close()
+
+    hbm, hbm_kind = measured_hbm()
+    mixed = out["mixed"]
+    total_cells = cells * ranks.world
+    value = total_cells * K / (mixed["ms"] / 1e3) / 1e6
+    fp64_value = total_cells * K / (out["fp64"]["ms"] / 1e3) / 1e6
+
+    def roofline(d, kname):
+        bytes_launch = BYTES_PER_CELL_STAGE[2] * cells
+        achieved = bytes_launch / (d["ms_stage2"] / 1e3) / 1e9
+        traffic = ncu_traffic(kname, cells)
+        return {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "peak_source": hbm_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_launch,
+                "step_hbm_frac": round(200 * cells / (d["ms"] / K / 1e3) / 1e9 / hbm, 4)}
+
+    cpu = None
+    if ranks.world == 1 and ranks.rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cpu_threads())
+
+    if ranks.rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ranks.world,
+        "steps": K, "warmup": W, "ms_per_step": round(mixed["ms"] / K, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 reconstruction+HLLC / f64 state, accumulation, reductions",
+        "data": DATA,
+        "config": {"workload": f"3D {n}^3 periodic PLM/minmod+HLLC SSP-RK2, gamma 5/3, CFL 0.4, "
+                               "dt recomputed on device each step",
+                   "cells_per_gpu": cells, "precision": "mixed",
+                   "l2": "inputs larger than L2 (671 MB per state buffer)",
+                   "parallelism": f"one independent instance per GPU x{ranks.world}"},
+        "fp64": {"value": round(fp64_value, 1), "unit": UNIT,
+                 "ms_per_step": round(out["fp64"]["ms"] / K, 4),
+                 "speedup_mixed_over_fp64": round(value / fp64_value, 3),
+                 "roofline": roofline(out["fp64"], "stage2_fp64")},
+        "roofline": roofline(mixed, "stage2_mixed"),
+        "kernels_ms": {p: {k: round(v, 4) for k, v in out[p].items() if k.startswith("ms_")}
+                       for p in out},
+        "e2e": {"value": round(total_cells * K / (e2e_ms / 1e3) / 1e6, 1), "unit": UNIT,
+                "h2d_bytes_per_step": int(5 * 8 * cells / K),
+                "d2h_bytes_per_step": int(5 * 8 * cells / K),
+                "what": f"vb_grid_upload of the state from pinned host memory, vb_evolve of {K} "
+                        "steps, vb_grid_download; device time of the whole sequence"},
+        "gpu_launches": mixed["launches"],
+        "clocks": clocks,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ranks = Ranks(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ranks)
+        else:
+            run_ours(args, ranks)
+    finally:
+        ranks.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,149 @@
+/*
+ * vespa_b200.h -- C ABI of libvespa_b200.so, the B200 (sm_100a) implementation
+ * of Vespa.jl's finite-volume hydro step: PLM/minmod reconstruction, the HLLC
+ * Riemann solver, the ideal-gas EOS, SSP-RK2 stages, the CFL reduction and the
+ * conserved totals, with the state resident in device memory.
+ *
+ * Conventions (all entry points):
+ *   - every function returns an int status (vb_status); 0 is success and no
+ *     C++ exception crosses the ABI.  vb_last_error() returns the calling
+ *     thread's last error message.
+ *   - host pointers are borrowed for the duration of the call only; device
+ *     buffers are owned by the opaque vb_ctx / vb_grid handles.
+ *   - the conserved state is structure-of-arrays float64, five fields
+ *     (rho, rho*vx, rho*vy, rho*vz, E), each ncell long, cells column-major
+ *     with x fastest (Julia's CartesianIndices order, RefMesh field views).
+ *   - face batches are 5 float64 per face, contiguous (Julia's
+ *     Vector{NTuple{5,Float64}} reinterpreted as a 5 x nf matrix).
+ *   - axes are 1-based (1 = x, 2 = y, 3 = z) as in the reference.
+ *   - calls are ordered on the context's CUDA stream and return after the
+ *     stream has drained unless the name ends in _async.
+ *   - one context per host thread; a context is not thread-safe.
+ */
+#ifndef VESPA_B200_H
+#define VESPA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VB_ABI_VERSION 1
+
+typedef enum {
+    VB_OK = 0,
+    VB_EINVAL = 1,      /* bad argument */
+    VB_ECUDA = 2,       /* CUDA runtime error (message in vb_last_error) */
+    VB_ENOMEM = 3,      /* device or pinned allocation failed */
+    VB_ENONFINITE = 4,  /* a non-finite or negative density/pressure reached the CFL reduction */
+    VB_ETIMEOUT = 5,    /* a bounded device wait gave up */
+    VB_ENOTSUP = 6      /* configuration not supported by this build */
+} vb_status;
+
+/* Boundary conditions, lib/MeshInterface/src/MeshInterface.jl:74-83. */
+enum { VB_BC_OUTFLOW = 0, VB_BC_PERIODIC = 1, VB_BC_REFLECTING = 2 };
+
+/* Precision modes.  VB_FP64: every operation in float64 in the reference's
+ * order, no fused multiply-add (bit-identical to the CPU restatement).
+ * VB_MIXED: float64 state, pressure recovery, flux-difference accumulation and
+ * reductions; float32 reconstruction and HLLC. */
+enum { VB_FP64 = 0, VB_MIXED = 1 };
+
+typedef struct vb_ctx vb_ctx;
+typedef struct vb_grid vb_grid;
+
+/* Uniform-mesh problem: mirrors Problem (src/problem.jl:20-50) on a RefMesh
+ * UniformMesh (lib/RefMesh/src/RefMesh.jl:89-100).  Unused axes are ignored. */
+typedef struct {
+    int32_t ndim;        /* 1..3 */
+    int32_t bc_lo[3];    /* VB_BC_* per axis, lo side */
+    int32_t bc_hi[3];    /* VB_BC_* per axis, hi side */
+    int32_t flags;       /* reserved, must be 0 */
+    int64_t dims[3];     /* interior cells per axis */
+    double lo[3];        /* domain lower bounds */
+    double hi[3];        /* domain upper bounds */
+    double gamma;        /* adiabatic index, IdealHydro(γ) src/equationset.jl:31-33 */
+    double cfl;          /* Courant number, Problem.cfl */
+    double aexp;         /* expansion factor in dt/(aexp*V), src/driver.jl:297-307; 1.0 without cosmology */
+} vb_problem_desc;
+
+int vb_abi_version(void);
+
+/* Thread-local message of the last failed call; returns its full length. */
+int vb_last_error(char *buf, size_t len);
+
+/* Context: one CUDA device, one stream, cached scratch buffers. */
+int vb_ctx_create(int device, vb_ctx **out);
+int vb_ctx_destroy(vb_ctx *ctx);
+int vb_ctx_synchronize(vb_ctx *ctx);
+/* The context's cudaStream_t (as void*), e.g. to time it with CUDA events. */
+int vb_ctx_stream(vb_ctx *ctx, void **stream);
+/* Number of kernels this context has launched so far (graph nodes included). */
+int vb_ctx_launch_count(vb_ctx *ctx, int64_t *count);
+/* CUDA-event timing on the context's stream (the reference's Instrumented
+ * span timing, lib/MeshInterface/src/instrument.jl:30-95, moved to device
+ * time): vb_ctx_mark records event `slot` (0..15); vb_ctx_elapsed_ms waits
+ * for the later mark and returns the device time between two marks. */
+int vb_ctx_mark(vb_ctx *ctx, int slot);
+int vb_ctx_elapsed_ms(vb_ctx *ctx, int slot_a, int slot_b, float *ms);
+
+/* Batched HLLC face fluxes from gathered left/right primitive states.
+ * Replaces Vespa.compute_face_fluxes!(::KAFlux, model, F, WL, WR, axisv)
+ * (ext/VespaKAFluxExt.jl:37-63; contract src/ka_flux.jl:40-53): WL, WR and F
+ * are host arrays of 5*nf float64, axis holds nf 1-based axes, gamma is
+ * adiabatic_index(model).  Bit-identical to HostBatchedFlux. */
+int vb_hllc_faces(vb_ctx *ctx, int64_t nf, const double *WL, const double *WR,
+                  const int32_t *axis, double gamma, double *F);
+/* Same on device pointers, asynchronous on the context's stream. */
+int vb_hllc_faces_device_async(vb_ctx *ctx, int64_t nf, const double *dWL, const double *dWR,
+                               const int32_t *daxis, double gamma, double *dF);
+
+/* Device-resident uniform grid: Simulation(UniformMesh, prob) state, u0 and
+ * stage buffers (src/driver.jl:27-79).  precision is VB_FP64 or VB_MIXED. */
+int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *desc, int precision, vb_grid **out);
+int vb_grid_destroy(vb_grid *grid);
+int vb_grid_ncell(const vb_grid *grid, int64_t *ncell);
+/* State I/O: 5*ncell float64 host arrays (the `sv` field views). */
+int vb_grid_upload(vb_grid *grid, const double *U);
+int vb_grid_download(vb_grid *grid, double *U);
+/* Device pointer of the state (5*ncell float64), valid until vb_grid_destroy. */
+int vb_grid_device_state(vb_grid *grid, double **dU);
+/* Simulation clock (sim.t, sim.step). */
+int vb_grid_set_time(vb_grid *grid, double t, int64_t step);
+int vb_grid_get_time(vb_grid *grid, double *t, int64_t *step);
+
+/* compute_dt(sim), src/driver.jl:169-199: cfl / max over cells and axes of
+ * (|v_d| + c) / w_d; +Inf when the gas is at rest. */
+int vb_compute_dt(vb_grid *grid, double *dt);
+/* step!(sim, dt), src/driver.jl:333-359: one SSP-RK2 step, advances t. */
+int vb_step(vb_grid *grid, double dt);
+/* evolve!(sim), src/driver.jl:483-508: steps with dt = min(compute_dt,
+ * tfinal - t) until t >= tfinal*(1-1e-12) or max_steps steps (max_steps < 0:
+ * no limit).  dt is computed on the device; the loop runs as CUDA graphs. */
+int vb_evolve(vb_grid *grid, double tfinal, int64_t max_steps, double *t, int64_t *nsteps);
+/* nsteps CFL-limited steps without a final time, queued on the stream. */
+int vb_run_steps_async(vb_grid *grid, int64_t nsteps);
+/* conserved_totals(sim), src/diagnostics.jl:16-31: sum of U*V per field. */
+int vb_conserved_totals(vb_grid *grid, double out[5]);
+/* Profiling aid: runs nsteps CFL-limited steps with an event pair around
+ * every launch and returns the mean device time of each kernel of the step
+ * (dt finalisation, stage 1, stage 2) in milliseconds. */
+int vb_grid_profile_step(vb_grid *grid, int nsteps, double *ms_finalize, double *ms_stage1,
+                         double *ms_stage2);
+
+/* Boundary-flux register (BoundaryFluxRegister, src/reflux.jl:113-132): while
+ * enabled, every domain-boundary face accumulates (0.5*dt*F)*area per RK2
+ * stage.  Planes are stored per axis d (1..ndim) and side (lo, hi), five
+ * components each, the flux axis collapsed and the other axes column-major
+ * with the lowest axis fastest (the bflux_plane raster, src/reflux.jl:148-191). */
+int vb_bflux_enable(vb_grid *grid, int enable);
+int vb_bflux_size(const vb_grid *grid, int64_t *n);
+int vb_bflux_read(vb_grid *grid, double *out, int64_t n);
+int vb_bflux_clear(vb_grid *grid);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VESPA_B200_H */

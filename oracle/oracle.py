@@ -1,0 +1,209 @@
+"""ctypes binding of the CPU oracle (oracle/vespa_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py``; the product package never imports it.
+
+Arrays follow the conventions of ``vespa_oracle.h``: the state is a
+``(5, ncell)`` float64 array (structure of arrays, x fastest) and face batches
+are ``(nf, 5)`` float64 arrays (five components contiguous per face).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvespa_oracle.so")
+
+BC_OUTFLOW, BC_PERIODIC, BC_REFLECTING = 0, 1, 2
+
+
+class VoGrid(C.Structure):
+    _fields_ = [
+        ("ndim", C.c_int32),
+        ("bc_lo", C.c_int32 * 3),
+        ("bc_hi", C.c_int32 * 3),
+        ("reserved", C.c_int32),
+        ("dims", C.c_int64 * 3),
+        ("lo", C.c_double * 3),
+        ("hi", C.c_double * 3),
+        ("gamma", C.c_double),
+        ("cfl", C.c_double),
+        ("aexp", C.c_double),
+    ]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        gp = C.POINTER(VoGrid)
+        L.vo_cons2prim.argtypes = [dp, C.c_double, dp]
+        L.vo_prim2cons.argtypes = [dp, C.c_double, dp]
+        L.vo_minmod.argtypes = [C.c_double, C.c_double]
+        L.vo_minmod.restype = C.c_double
+        L.vo_hllc_flux.argtypes = [dp, dp, C.c_double, C.c_int, dp]
+        L.vo_compute_face_fluxes.argtypes = [C.c_int64, dp, dp, C.POINTER(C.c_int32),
+                                             C.c_double, dp]
+        L.vo_ncell.argtypes = [gp]
+        L.vo_ncell.restype = C.c_int64
+        L.vo_compute_dt.argtypes = [gp, dp]
+        L.vo_compute_dt.restype = C.c_double
+        L.vo_accumulate_flux.argtypes = [gp, dp, dp, dp, C.c_double]
+        L.vo_accumulate_flux_gather.argtypes = [gp, dp, dp, C.c_int]
+        L.vo_step.argtypes = [gp, dp, dp, dp, C.c_double, dp, C.c_int, C.c_int]
+        L.vo_evolve.argtypes = [gp, dp, dp, dp, C.c_double, C.c_int64, dp, C.c_int, C.c_int]
+        L.vo_evolve.restype = C.c_int64
+        L.vo_conserved_totals.argtypes = [gp, dp, dp]
+        L.vo_bflux_size.argtypes = [gp]
+        L.vo_bflux_size.restype = C.c_int64
+        L.vo_exact_riemann_star.argtypes = [dp, dp, C.c_double, dp]
+        L.vo_exact_riemann_sample.argtypes = [dp, dp, C.c_double, C.c_double, dp]
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def make_grid(dims, lo, hi, bc_lo, bc_hi, gamma, cfl=0.4, aexp=1.0) -> VoGrid:
+    """Grid descriptor; ``dims/lo/hi/bc_*`` are per-axis sequences (length 1-3)."""
+    nd = len(dims)
+    g = VoGrid()
+    g.ndim = nd
+    for d in range(3):
+        g.dims[d] = int(dims[d]) if d < nd else 1
+        g.lo[d] = float(lo[d]) if d < nd else 0.0
+        g.hi[d] = float(hi[d]) if d < nd else 1.0
+        g.bc_lo[d] = int(bc_lo[d]) if d < nd else BC_PERIODIC
+        g.bc_hi[d] = int(bc_hi[d]) if d < nd else BC_PERIODIC
+    g.gamma = float(gamma)
+    g.cfl = float(cfl)
+    g.aexp = float(aexp)
+    return g
+
+
+def grid_from_problem(prob) -> VoGrid:
+    """Oracle grid for a product ``Problem`` (duck-typed: dims/domain/bcs/gamma/cfl)."""
+    lo = [d[0] for d in prob.domain]
+    hi = [d[1] for d in prob.domain]
+    bc_lo = [b[0] for b in prob.bc_pairs()]
+    bc_hi = [b[1] for b in prob.bc_pairs()]
+    return make_grid(prob.dims, lo, hi, bc_lo, bc_hi, prob.gamma, prob.cfl)
+
+
+def ncell(g: VoGrid) -> int:
+    return int(lib().vo_ncell(C.byref(g)))
+
+
+def cons2prim(U, gamma):
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    W = np.empty(5)
+    lib().vo_cons2prim(_dp(U), gamma, _dp(W))
+    return W
+
+
+def prim2cons(W, gamma):
+    W = np.ascontiguousarray(W, dtype=np.float64)
+    U = np.empty(5)
+    lib().vo_prim2cons(_dp(W), gamma, _dp(U))
+    return U
+
+
+def hllc_flux(WL, WR, gamma, dim):
+    WL = np.ascontiguousarray(WL, dtype=np.float64)
+    WR = np.ascontiguousarray(WR, dtype=np.float64)
+    F = np.empty(5)
+    lib().vo_hllc_flux(_dp(WL), _dp(WR), gamma, int(dim), _dp(F))
+    return F
+
+
+def compute_face_fluxes(WL, WR, axis, gamma):
+    WL = np.ascontiguousarray(WL, dtype=np.float64)
+    WR = np.ascontiguousarray(WR, dtype=np.float64)
+    ax = np.ascontiguousarray(axis, dtype=np.int32)
+    nf = ax.shape[0]
+    F = np.empty((nf, 5))
+    lib().vo_compute_face_fluxes(nf, _dp(WL), _dp(WR), ax.ctypes.data_as(C.POINTER(C.c_int32)),
+                                 gamma, _dp(F))
+    return F
+
+
+def compute_dt(g: VoGrid, U) -> float:
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    return float(lib().vo_compute_dt(C.byref(g), _dp(U)))
+
+
+def accumulate_flux(g: VoGrid, U, gather=False, nthreads=0):
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    acc = np.empty_like(U)
+    if gather:
+        lib().vo_accumulate_flux_gather(C.byref(g), _dp(U), _dp(acc), int(nthreads))
+    else:
+        lib().vo_accumulate_flux(C.byref(g), _dp(U), _dp(acc), None, 0.0)
+    return acc
+
+
+def step(g: VoGrid, U, dt, mode=0, nthreads=0, bflux=None):
+    """One SSP-RK2 step in place on ``U`` (a (5, ncell) float64 array)."""
+    assert U.dtype == np.float64 and U.flags.c_contiguous
+    u0 = np.empty_like(U)
+    acc = np.empty_like(U)
+    bp = _dp(bflux) if bflux is not None else None
+    lib().vo_step(C.byref(g), _dp(U), _dp(u0), _dp(acc), float(dt), bp, int(mode), int(nthreads))
+    return U
+
+
+def evolve(g: VoGrid, U, tfinal, max_steps=-1, t0=0.0, mode=0, nthreads=0):
+    """evolve! in place; returns (t, nsteps)."""
+    assert U.dtype == np.float64 and U.flags.c_contiguous
+    u0 = np.empty_like(U)
+    acc = np.empty_like(U)
+    t = C.c_double(t0)
+    n = lib().vo_evolve(C.byref(g), _dp(U), _dp(u0), _dp(acc), float(tfinal), int(max_steps),
+                        C.byref(t), int(mode), int(nthreads))
+    return t.value, int(n)
+
+
+def conserved_totals(g: VoGrid, U):
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    out = np.empty(5)
+    lib().vo_conserved_totals(C.byref(g), _dp(U), _dp(out))
+    return out
+
+
+def bflux_size(g: VoGrid) -> int:
+    return int(lib().vo_bflux_size(C.byref(g)))
+
+
+def exact_riemann_star(WL, WR, gamma):
+    WL = np.ascontiguousarray(WL, dtype=np.float64)
+    WR = np.ascontiguousarray(WR, dtype=np.float64)
+    out = np.empty(2)
+    lib().vo_exact_riemann_star(_dp(WL), _dp(WR), gamma, _dp(out))
+    return out
+
+
+def exact_riemann_sample(WL, WR, gamma, s):
+    WL = np.ascontiguousarray(WL, dtype=np.float64)
+    WR = np.ascontiguousarray(WR, dtype=np.float64)
+    out = np.empty(3)
+    lib().vo_exact_riemann_sample(_dp(WL), _dp(WR), gamma, float(s), _dp(out))
+    return out

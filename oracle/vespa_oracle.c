@@ -1,0 +1,632 @@
+/*
+ * vespa_oracle.c -- CPU oracle for the Vespa.jl finite-volume hydro step.
+ *
+ * TEST INFRASTRUCTURE ONLY (see vespa_oracle.h): the checker for the CUDA
+ * library and the timed CPU baseline, never part of the product path.
+ *
+ * Every expression below is written in the reference's operation order so a
+ * correctly rounded evaluation of the same expression tree agrees bit for bit.
+ * Build with -ffp-contract=off and without -ffast-math (oracle/Makefile does):
+ * Julia never fuses a multiply-add in these kernels, so neither may we.
+ *
+ * Parity status: pinned against the reference's known-answer tests (Sod vs the
+ * exact Riemann solution and conservation, test/test_sod.jl:32-43; boundary-flux
+ * identity, test/test_boundary_flux.jl:35) and Toro's published Sod star state;
+ * bit-level agreement with the reference's own outputs is unpinned because the
+ * reference (Julia) cannot run here.
+ */
+#include "vespa_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* Julia's Base.min / Base.max for IEEE floats: the sign of x - y picks the
+ * result, NaN propagates (base/math.jl). */
+static inline double jl_min(double x, double y)
+{
+    double diff = x - y;
+    if (isnan(x) || isnan(y)) return diff;
+    return signbit(diff) ? x : y;
+}
+static inline double jl_max(double x, double y)
+{
+    double diff = x - y;
+    if (isnan(x) || isnan(y)) return diff;
+    return signbit(diff) ? y : x;
+}
+
+/* ---------------------------------------------------------------- eos.jl */
+
+/* cons2prim, src/eos.jl:8-25 (pressure floor max(p, 1e-12 * kinetic) at :24) */
+void vo_cons2prim(const double *U, double gamma, double *W)
+{
+    double g = gamma;
+    double rho = U[0];
+    double inv = 1.0 / rho;
+    double vx = U[1] * inv;
+    double vy = U[2] * inv;
+    double vz = U[3] * inv;
+    double kinetic = 0.5 * rho * (vx * vx + vy * vy + vz * vz);
+    double p = (g - 1.0) * (U[4] - kinetic);
+    W[0] = rho;
+    W[1] = vx;
+    W[2] = vy;
+    W[3] = vz;
+    W[4] = jl_max(p, 1e-12 * kinetic);
+}
+
+/* prim2cons, src/eos.jl:28-32 */
+void vo_prim2cons(const double *W, double gamma, double *U)
+{
+    double rho = W[0], vx = W[1], vy = W[2], vz = W[3], p = W[4];
+    double E = p / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy + vz * vz);
+    U[0] = rho;
+    U[1] = rho * vx;
+    U[2] = rho * vy;
+    U[3] = rho * vz;
+    U[4] = E;
+}
+
+/* ---------------------------------------------------------- reconstruct.jl */
+
+/* minmod, src/reconstruct.jl:6-12 */
+double vo_minmod(double a, double b)
+{
+    if (a * b <= 0.0) return 0.0;
+    return fabs(a) < fabs(b) ? a : b;
+}
+
+/* limited_slope, src/reconstruct.jl:15-16 */
+static inline double limited_slope(double l, double c, double r)
+{
+    return vo_minmod(c - l, r - c);
+}
+
+/* ---------------------------------------------------------------- riemann.jl */
+
+/* euler_flux, src/riemann.jl:9-20; dim is 1-based */
+static void euler_flux(const double *W, double gamma, int dim, double *F)
+{
+    double rho = W[0], vx = W[1], vy = W[2], vz = W[3], p = W[4];
+    double un = W[dim];
+    double E = p / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy + vz * vz);
+    double m1 = rho * vx, m2 = rho * vy, m3 = rho * vz;
+    F[0] = rho * un;
+    F[1] = m1 * un + (dim == 1 ? p : 0.0);
+    F[2] = m2 * un + (dim == 2 ? p : 0.0);
+    F[3] = m3 * un + (dim == 3 ? p : 0.0);
+    F[4] = (E + p) * un;
+}
+
+/* _hllc_star, src/riemann.jl:69-88 */
+static void hllc_star(const double *W, const double *U, const double *F, double SK,
+                      double Sstar, int dim, double *out)
+{
+    double rho = W[0];
+    double un = W[dim];
+    double p = W[4];
+    double E = U[4];
+    double factor = rho * (SK - un) / (SK - Sstar);
+    double vstar[3] = {W[1], W[2], W[3]};
+    vstar[dim - 1] = Sstar;
+    double Estar = E / rho + (Sstar - un) * (Sstar + p / (rho * (SK - un)));
+    double Ustar[5] = {factor, factor * vstar[0], factor * vstar[1], factor * vstar[2],
+                       factor * Estar};
+    for (int k = 0; k < 5; ++k) out[k] = F[k] + SK * (Ustar[k] - U[k]);
+}
+
+/* hllc_flux, src/riemann.jl:33-66 (Davis wave speeds, no HLL fallback) */
+void vo_hllc_flux(const double *WL, const double *WR, double gamma, int dim, double *F)
+{
+    double rhoL = WL[0], rhoR = WR[0];
+    double pL = WL[4], pR = WR[4];
+    double unL = WL[dim], unR = WR[dim];
+    double g = gamma;
+    double cL = sqrt(g * pL / rhoL);
+    double cR = sqrt(g * pR / rhoR);
+    double SL = jl_min(unL - cL, unR - cR);
+    double SR = jl_max(unL + cL, unR + cR);
+    double UL[5], UR[5], FL[5], FR[5];
+    vo_prim2cons(WL, gamma, UL);
+    vo_prim2cons(WR, gamma, UR);
+    euler_flux(WL, gamma, dim, FL);
+    euler_flux(WR, gamma, dim, FR);
+    if (SL >= 0.0) {
+        memcpy(F, FL, sizeof FL);
+        return;
+    } else if (SR <= 0.0) {
+        memcpy(F, FR, sizeof FR);
+        return;
+    }
+    double Sstar = (pR - pL + rhoL * unL * (SL - unL) - rhoR * unR * (SR - unR)) /
+                   (rhoL * (SL - unL) - rhoR * (SR - unR));
+    if (Sstar >= 0.0)
+        hllc_star(WL, UL, FL, SL, Sstar, dim, F);
+    else
+        hllc_star(WR, UR, FR, SR, Sstar, dim, F);
+}
+
+/* compute_face_fluxes!(::HostBatchedFlux, ...), src/ka_flux.jl:48-53 */
+void vo_compute_face_fluxes(int64_t nf, const double *WL, const double *WR,
+                            const int32_t *axis, double gamma, double *F)
+{
+    for (int64_t f = 0; f < nf; ++f)
+        vo_hllc_flux(WL + 5 * f, WR + 5 * f, gamma, (int)axis[f], F + 5 * f);
+}
+
+/* ------------------------------------------------ RefMesh geometry/topology */
+
+typedef struct {
+    int nd;
+    int64_t n[3];
+    int64_t stride[3];
+    int64_t ncell;
+    double w[3];
+    double area[3];
+    double vol;
+} geom_t;
+
+static void make_geom(const vo_grid *g, geom_t *G)
+{
+    G->nd = g->ndim;
+    int64_t s = 1;
+    for (int d = 0; d < 3; ++d) {
+        G->n[d] = d < g->ndim ? g->dims[d] : 1;
+        G->stride[d] = s;
+        s *= G->n[d];
+    }
+    G->ncell = s;
+    /* _width, lib/RefMesh/src/RefMesh.jl:122-123 */
+    for (int d = 0; d < g->ndim; ++d) G->w[d] = (g->hi[d] - g->lo[d]) / (double)g->dims[d];
+    /* face_area, RefMesh.jl:135-142 */
+    for (int d = 0; d < g->ndim; ++d) {
+        double a = 1.0;
+        for (int e = 0; e < g->ndim; ++e)
+            if (e != d) a *= G->w[e];
+        G->area[d] = a;
+    }
+    /* cell_volume = prod(_width), RefMesh.jl:127 (left fold) */
+    double v = G->w[0];
+    for (int d = 1; d < g->ndim; ++d) v = v * G->w[d];
+    G->vol = v;
+}
+
+int64_t vo_ncell(const vo_grid *g)
+{
+    geom_t G;
+    make_geom(g, &G);
+    return G.ncell;
+}
+
+static inline int64_t coord_of(const geom_t *G, int64_t lin, int d)
+{
+    return (lin / G->stride[d]) % G->n[d];
+}
+
+/* neighbor, RefMesh.jl:147-161: linear index of the neighbour, or -1 for a
+ * domain boundary; periodic wraps to the opposite edge. d is 0-based. */
+static inline int64_t neighbor(const vo_grid *g, const geom_t *G, int64_t lin, int d, int hi)
+{
+    int64_t c = coord_of(G, lin, d);
+    int64_t n = G->n[d];
+    int64_t j = c + (hi ? 1 : -1);
+    if (j >= 0 && j < n) return lin + (j - c) * G->stride[d];
+    int bc = hi ? g->bc_hi[d] : g->bc_lo[d];
+    if (bc == VO_BC_PERIODIC) {
+        int64_t jw = j < 0 ? n - 1 : 0;
+        return lin + (jw - c) * G->stride[d];
+    }
+    return -1;
+}
+
+static inline void load_U(const geom_t *G, const double *U, int64_t lin, double *u)
+{
+    for (int k = 0; k < 5; ++k) u[k] = U[k * G->ncell + lin];
+}
+
+/* _W, src/driver.jl:137 */
+static inline void prim_at(const vo_grid *g, const geom_t *G, const double *U, int64_t lin,
+                           double *W)
+{
+    double u[5];
+    load_U(G, U, lin, u);
+    vo_cons2prim(u, g->gamma, W);
+}
+
+/* ghost_state, src/driver.jl:117-122 (Outflow copy; Reflecting negates the
+ * normal velocity, momentum_indices(model)[axis]); d is 0-based. */
+static inline void ghost_state(const double *W, int bc, int d, double *out)
+{
+    for (int k = 0; k < 5; ++k) out[k] = W[k];
+    if (bc == VO_BC_REFLECTING) out[1 + d] = -W[1 + d];
+}
+
+/* _plm_slope, src/driver.jl:145-159 */
+static void plm_slope(const vo_grid *g, const geom_t *G, const double *U, int64_t lin,
+                      const double *Wc, int d, double *s)
+{
+    double WL[5], WR[5];
+    int64_t nlo = neighbor(g, G, lin, d, 0);
+    int64_t nhi = neighbor(g, G, lin, d, 1);
+    if (nlo < 0)
+        ghost_state(Wc, g->bc_lo[d], d, WL);
+    else
+        prim_at(g, G, U, nlo, WL);
+    if (nhi < 0)
+        ghost_state(Wc, g->bc_hi[d], d, WR);
+    else
+        prim_at(g, G, U, nhi, WR);
+    for (int k = 0; k < 5; ++k) s[k] = limited_slope(WL[k], Wc[k], WR[k]);
+}
+
+/* _face_value, src/driver.jl:227-233 */
+static void face_value(const vo_grid *g, const geom_t *G, const double *U, int64_t lin, int d,
+                       int hi, double *out)
+{
+    double Wi[5], s[5];
+    prim_at(g, G, U, lin, Wi);
+    plm_slope(g, G, U, lin, Wi, d, s);
+    double h = hi ? 0.5 : -0.5;
+    for (int k = 0; k < 5; ++k) out[k] = Wi[k] + h * s[k];
+}
+
+/* _acc_add!, src/driver.jl:98-99: acc[cell] += s * F */
+static inline void acc_add(const geom_t *G, double *acc, int64_t lin, const double *F, double s)
+{
+    for (int k = 0; k < 5; ++k) acc[k * G->ncell + lin] += s * F[k];
+}
+
+/* bflux plane offset for (axis d, side, component k): dense planes with the
+ * flux axis collapsed, remaining axes column-major, dim-0 fastest
+ * (src/reflux.jl:148-166 plane raster order). */
+static int64_t bflux_plane_index(const geom_t *G, int64_t lin, int d)
+{
+    int64_t idx = 0, mul = 1;
+    for (int e = 0; e < G->nd; ++e) {
+        if (e == d) continue;
+        idx += coord_of(G, lin, e) * mul;
+        mul *= G->n[e];
+    }
+    return idx;
+}
+static int64_t bflux_base(const geom_t *G, int d, int side)
+{
+    int64_t off = 0;
+    for (int e = 0; e < d; ++e) off += 2 * 5 * (G->ncell / G->n[e]);
+    return off + (int64_t)side * 5 * (G->ncell / G->n[d]);
+}
+
+int64_t vo_bflux_size(const vo_grid *g)
+{
+    geom_t G;
+    make_geom(g, &G);
+    return bflux_base(&G, G.nd, 0);
+}
+
+/* _bflux_capture!, src/reflux.jl:125-132: reg += (scale * f) * area */
+static void bflux_capture(const geom_t *G, double *bflux, double scale, int d, int side,
+                          int64_t lin, const double *F, double area)
+{
+    if (!bflux) return;
+    int64_t P = G->ncell / G->n[d];
+    int64_t base = bflux_base(G, d, side) + bflux_plane_index(G, lin, d);
+    for (int k = 0; k < 5; ++k) bflux[base + k * P] += scale * F[k] * area;
+}
+
+/* accumulate_flux! + for_each_face (src/driver.jl:209-281,
+ * lib/RefMesh/src/RefMesh.jl:187-197): cells column-major; per cell and axis,
+ * the hi face, then the lo face only when it is a domain boundary. */
+void vo_accumulate_flux(const vo_grid *g, const double *U, double *acc, double *bflux,
+                        double bscale)
+{
+    geom_t G;
+    make_geom(g, &G);
+    memset(acc, 0, sizeof(double) * 5 * G.ncell);
+    double WL[5], WR[5], Wg[5], F[5];
+    for (int64_t lin = 0; lin < G.ncell; ++lin) {
+        for (int d = 0; d < G.nd; ++d) {
+            double a = G.area[d];
+            int64_t nhi = neighbor(g, &G, lin, d, 1);
+            if (nhi >= 0) {
+                /* interior <-> interior, driver.jl:236-253 */
+                face_value(g, &G, U, lin, d, 1, WL);
+                face_value(g, &G, U, nhi, d, 0, WR);
+                vo_hllc_flux(WL, WR, g->gamma, d + 1, F);
+                acc_add(&G, acc, lin, F, a);
+                acc_add(&G, acc, nhi, F, -a);
+            } else {
+                /* hi-side domain boundary, driver.jl:256-267 */
+                face_value(g, &G, U, lin, d, 1, WL);
+                ghost_state(WL, g->bc_hi[d], d, Wg);
+                vo_hllc_flux(WL, Wg, g->gamma, d + 1, F);
+                acc_add(&G, acc, lin, F, a);
+                bflux_capture(&G, bflux, bscale, d, 1, lin, F, a);
+            }
+            int64_t nlo = neighbor(g, &G, lin, d, 0);
+            if (nlo < 0) {
+                /* lo-side domain boundary, driver.jl:270-281 */
+                face_value(g, &G, U, lin, d, 0, WR);
+                ghost_state(WR, g->bc_lo[d], d, Wg);
+                vo_hllc_flux(Wg, WR, g->gamma, d + 1, F);
+                bflux_capture(&G, bflux, bscale, d, 0, lin, F, a);
+                acc_add(&G, acc, lin, F, -a);
+            }
+        }
+    }
+}
+
+/* Per-cell gather with the same per-cell summation order as the enumeration
+ * above: each contribution is keyed by (emitting cell, axis, sub-order) and the
+ * keys are sorted, so the result is bit-identical to vo_accumulate_flux while
+ * cells can be processed in parallel.  The face flux itself is a pure function
+ * of the state, so recomputing it per adjacent cell changes nothing. */
+typedef struct {
+    int64_t owner;
+    int d;
+    int sub;
+    double s;
+    double F[5];
+} contrib_t;
+
+static void gather_cell(const vo_grid *g, const geom_t *G, const double *U, int64_t lin,
+                        double *accv)
+{
+    contrib_t c[6];
+    int nc = 0;
+    double WL[5], WR[5], Wg[5];
+    for (int d = 0; d < G->nd; ++d) {
+        double a = G->area[d];
+        int64_t nhi = neighbor(g, G, lin, d, 1);
+        contrib_t *h = &c[nc++];
+        h->owner = lin;
+        h->d = d;
+        h->sub = 0;
+        h->s = a;
+        face_value(g, G, U, lin, d, 1, WL);
+        if (nhi >= 0) {
+            face_value(g, G, U, nhi, d, 0, WR);
+            vo_hllc_flux(WL, WR, g->gamma, d + 1, h->F);
+        } else {
+            ghost_state(WL, g->bc_hi[d], d, Wg);
+            vo_hllc_flux(WL, Wg, g->gamma, d + 1, h->F);
+        }
+        int64_t nlo = neighbor(g, G, lin, d, 0);
+        contrib_t *l = &c[nc++];
+        l->d = d;
+        l->s = -a;
+        face_value(g, G, U, lin, d, 0, WR);
+        if (nlo >= 0) {
+            /* emitted by nlo's hi query: interior face (nlo, lin) */
+            l->owner = nlo;
+            l->sub = 1;
+            face_value(g, G, U, nlo, d, 1, WL);
+            vo_hllc_flux(WL, WR, g->gamma, d + 1, l->F);
+        } else {
+            l->owner = lin;
+            l->sub = 2;
+            ghost_state(WR, g->bc_lo[d], d, Wg);
+            vo_hllc_flux(Wg, WR, g->gamma, d + 1, l->F);
+        }
+    }
+    /* insertion sort on (owner, d, sub) */
+    for (int i = 1; i < nc; ++i) {
+        contrib_t t = c[i];
+        int j = i - 1;
+        while (j >= 0 && (c[j].owner > t.owner ||
+                          (c[j].owner == t.owner &&
+                           (c[j].d > t.d || (c[j].d == t.d && c[j].sub > t.sub))))) {
+            c[j + 1] = c[j];
+            --j;
+        }
+        c[j + 1] = t;
+    }
+    for (int k = 0; k < 5; ++k) {
+        double acc = 0.0;
+        for (int i = 0; i < nc; ++i) acc += c[i].s * c[i].F[k];
+        accv[k * G->ncell + lin] = acc;
+    }
+}
+
+void vo_accumulate_flux_gather(const vo_grid *g, const double *U, double *acc, int nthreads)
+{
+    geom_t G;
+    make_geom(g, &G);
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+#endif
+    for (int64_t lin = 0; lin < G.ncell; ++lin) gather_cell(g, &G, U, lin, acc);
+    (void)nthreads;
+}
+
+/* compute_dt, src/driver.jl:169-199 (no gravity, no cosmology) */
+double vo_compute_dt(const vo_grid *g, const double *U)
+{
+    geom_t G;
+    make_geom(g, &G);
+    double invdt = 0.0;
+    double W[5];
+    for (int64_t lin = 0; lin < G.ncell; ++lin) {
+        prim_at(g, &G, U, lin, W);
+        double c = sqrt(g->gamma * W[4] / W[0]); /* sound_speed, src/eos.jl:35 */
+        for (int d = 0; d < G.nd; ++d) {
+            double vd = W[1 + d];
+            invdt = jl_max(invdt, (fabs(vd) + c) / G.w[d]);
+        }
+    }
+    invdt = jl_max(invdt, 0.0);
+    if (invdt == 0.0) return INFINITY;
+    return g->cfl / invdt;
+}
+
+/* step!, src/driver.jl:333-359 with _copy_state! (285-290), _euler_apply!
+ * (297-307) and _rk2_combine! (310-321).  mode 0 = faithful serial face
+ * enumeration, mode 1 = per-cell gather (OpenMP). */
+void vo_step(const vo_grid *g, double *U, double *u0, double *acc, double dt, double *bflux,
+             int mode, int nthreads)
+{
+    geom_t G;
+    make_geom(g, &G);
+    int64_t n5 = 5 * G.ncell;
+    double bscale = 0.5 * dt;
+    memcpy(u0, U, sizeof(double) * n5);
+    if (mode == 0)
+        vo_accumulate_flux(g, U, acc, bflux, bscale);
+    else
+        vo_accumulate_flux_gather(g, U, acc, nthreads);
+    double invV = dt / (g->aexp * G.vol);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(nthreads > 0 ? nthreads : omp_get_max_threads()) if (mode == 1)
+#endif
+    for (int64_t i = 0; i < n5; ++i) U[i] = u0[i] - invV * acc[i];
+    if (mode == 0)
+        vo_accumulate_flux(g, U, acc, bflux, bscale);
+    else
+        vo_accumulate_flux_gather(g, U, acc, nthreads);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(nthreads > 0 ? nthreads : omp_get_max_threads()) if (mode == 1)
+#endif
+    for (int64_t i = 0; i < n5; ++i) U[i] = 0.5 * u0[i] + 0.5 * (U[i] - invV * acc[i]);
+}
+
+/* evolve!, src/driver.jl:483-508 (single-rate path, no regrid/callback) */
+int64_t vo_evolve(const vo_grid *g, double *U, double *u0, double *acc, double tfinal,
+                  int64_t max_steps, double *t, int mode, int nthreads)
+{
+    int64_t n = 0;
+    while (*t < tfinal * (1.0 - 1e-12)) {
+        if (max_steps >= 0 && n >= max_steps) break;
+        double dt = jl_min(vo_compute_dt(g, U), tfinal - *t);
+        vo_step(g, U, u0, acc, dt, NULL, mode, nthreads);
+        *t += dt;
+        ++n;
+    }
+    return n;
+}
+
+/* conserved_totals, src/diagnostics.jl:16-31 (serial column-major sum) */
+void vo_conserved_totals(const vo_grid *g, const double *U, double *out)
+{
+    geom_t G;
+    make_geom(g, &G);
+    double tot[5] = {0, 0, 0, 0, 0};
+    for (int64_t lin = 0; lin < G.ncell; ++lin)
+        for (int k = 0; k < 5; ++k) tot[k] += U[k * G.ncell + lin] * G.vol;
+    memcpy(out, tot, sizeof tot);
+}
+
+/* ---------------------------------------------------------- exact_riemann.jl */
+
+static inline double snd(double rho, double p, double g) { return sqrt(g * p / rho); }
+
+/* _pressure_fn, src/exact_riemann.jl:11-23 */
+static void pressure_fn(double p, double rhoK, double pK, double cK, double g, double *f,
+                        double *df)
+{
+    if (p > pK) {
+        double AK = 2.0 / ((g + 1.0) * rhoK);
+        double BK = (g - 1.0) / (g + 1.0) * pK;
+        *f = (p - pK) * sqrt(AK / (p + BK));
+        *df = sqrt(AK / (BK + p)) * (1.0 - (p - pK) / (2.0 * (BK + p)));
+    } else {
+        *f = 2.0 * cK / (g - 1.0) * (pow(p / pK, (g - 1.0) / (2.0 * g)) - 1.0);
+        *df = 1.0 / (rhoK * cK) * pow(p / pK, -(g + 1.0) / (2.0 * g));
+    }
+}
+
+/* _star_state, src/exact_riemann.jl:25-48; WL/WR are (rho, u, p) */
+void vo_exact_riemann_star(const double *WL, const double *WR, double g, double *pu)
+{
+    const double tol = 1e-12;
+    double rhoL = WL[0], uL = WL[1], pL = WL[2];
+    double rhoR = WR[0], uR = WR[1], pR = WR[2];
+    double cL = snd(rhoL, pL, g), cR = snd(rhoR, pR, g);
+    double p = fmax(tol, 0.5 * (pL + pR));
+    for (int it = 0; it < 100; ++it) {
+        double fL, dfL, fR, dfR;
+        pressure_fn(p, rhoL, pL, cL, g, &fL, &dfL);
+        pressure_fn(p, rhoR, pR, cR, g, &fR, &dfR);
+        double f = fL + fR + (uR - uL);
+        double p_new = fmax(tol, p - f / (dfL + dfR));
+        if (fabs(p_new - p) / (0.5 * (p_new + p)) < tol) {
+            p = p_new;
+            break;
+        }
+        p = p_new;
+    }
+    double fL, fR, dummy;
+    pressure_fn(p, rhoL, pL, cL, g, &fL, &dummy);
+    pressure_fn(p, rhoR, pR, cR, g, &fR, &dummy);
+    pu[0] = p;
+    pu[1] = 0.5 * (uL + uR) + 0.5 * (fR - fL);
+}
+
+/* exact_riemann_sample, src/exact_riemann.jl:56-120 */
+void vo_exact_riemann_sample(const double *WL, const double *WR, double g, double s,
+                             double *out)
+{
+    double rhoL = WL[0], uL = WL[1], pL = WL[2];
+    double rhoR = WR[0], uR = WR[1], pR = WR[2];
+    double cL = snd(rhoL, pL, g), cR = snd(rhoR, pR, g);
+    double pu[2];
+    vo_exact_riemann_star(WL, WR, g, pu);
+    double pstar = pu[0], ustar = pu[1];
+    double gm = (g - 1.0) / (g + 1.0);
+    if (s <= ustar) {
+        if (pstar > pL) {
+            double SL = uL - cL * sqrt((g + 1.0) / (2.0 * g) * pstar / pL + (g - 1.0) / (2.0 * g));
+            if (s <= SL) {
+                out[0] = rhoL; out[1] = uL; out[2] = pL;
+            } else {
+                out[0] = rhoL * (pstar / pL + gm) / (gm * pstar / pL + 1.0);
+                out[1] = ustar; out[2] = pstar;
+            }
+        } else {
+            double SHL = uL - cL;
+            double cstar = cL * pow(pstar / pL, (g - 1.0) / (2.0 * g));
+            double STL = ustar - cstar;
+            if (s <= SHL) {
+                out[0] = rhoL; out[1] = uL; out[2] = pL;
+            } else if (s >= STL) {
+                out[0] = rhoL * pow(pstar / pL, 1.0 / g);
+                out[1] = ustar; out[2] = pstar;
+            } else {
+                double u = 2.0 / (g + 1.0) * (cL + (g - 1.0) / 2.0 * uL + s);
+                double c = 2.0 / (g + 1.0) * (cL + (g - 1.0) / 2.0 * (uL - s));
+                out[0] = rhoL * pow(c / cL, 2.0 / (g - 1.0));
+                out[1] = u;
+                out[2] = pL * pow(c / cL, 2.0 * g / (g - 1.0));
+            }
+        }
+    } else {
+        if (pstar > pR) {
+            double SR = uR + cR * sqrt((g + 1.0) / (2.0 * g) * pstar / pR + (g - 1.0) / (2.0 * g));
+            if (s >= SR) {
+                out[0] = rhoR; out[1] = uR; out[2] = pR;
+            } else {
+                out[0] = rhoR * (pstar / pR + gm) / (gm * pstar / pR + 1.0);
+                out[1] = ustar; out[2] = pstar;
+            }
+        } else {
+            double SHR = uR + cR;
+            double cstar = cR * pow(pstar / pR, (g - 1.0) / (2.0 * g));
+            double STR = ustar + cstar;
+            if (s >= SHR) {
+                out[0] = rhoR; out[1] = uR; out[2] = pR;
+            } else if (s <= STR) {
+                out[0] = rhoR * pow(pstar / pR, 1.0 / g);
+                out[1] = ustar; out[2] = pstar;
+            } else {
+                double u = 2.0 / (g + 1.0) * (-cR + (g - 1.0) / 2.0 * uR + s);
+                double c = 2.0 / (g + 1.0) * (cR - (g - 1.0) / 2.0 * (uR - s));
+                out[0] = rhoR * pow(c / cR, 2.0 / (g - 1.0));
+                out[1] = u;
+                out[2] = pR * pow(c / cR, 2.0 * g / (g - 1.0));
+            }
+        }
+    }
+}

@@ -1,0 +1,76 @@
+/*
+ * vespa_oracle.h -- CPU oracle for the Vespa.jl finite-volume hydro step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  The oracle is the checker: tests/, the smoke()
+ * hook and bench.py's CPU-baseline leg may call it; the product library
+ * (libvespa_b200.so) never links, loads or calls it.
+ *
+ * Parity status: the restatement is pinned against the known-answer tests the
+ * reference keeps for this path (test/test_sod.jl:32-43 Sod vs the exact
+ * Riemann solution and conservation; test/test_boundary_flux.jl:35 boundary
+ * flux identity) and against Toro's published star state for the Sod problem.
+ * The reference itself (Julia) cannot run in this container, so bit-level
+ * agreement with the reference's own outputs is unpinned.
+ *
+ * Layout conventions shared with the product library:
+ *   - state: structure of arrays, U[k * ncell + lin], k = 0..4 for
+ *     (rho, mx, my, mz, E), lin = i + n0*(j + n1*kz) (x fastest, column-major
+ *     like Julia's CartesianIndices);
+ *   - face batches: 5 doubles per face contiguous (Julia's Vector{NTuple{5}}
+ *     reinterpreted as a 5 x nf column-major matrix);
+ *   - axes are 1-based (1=x, 2=y, 3=z) as in the reference.
+ */
+#ifndef VESPA_ORACLE_H
+#define VESPA_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { VO_BC_OUTFLOW = 0, VO_BC_PERIODIC = 1, VO_BC_REFLECTING = 2 };
+
+typedef struct {
+    int32_t ndim;
+    int32_t bc_lo[3];
+    int32_t bc_hi[3];
+    int32_t reserved;
+    int64_t dims[3];
+    double lo[3];
+    double hi[3];
+    double gamma;
+    double cfl;
+    double aexp;
+} vo_grid;
+
+/* per-cell / per-face kernels (src/eos.jl, src/reconstruct.jl, src/riemann.jl) */
+void vo_cons2prim(const double *U, double gamma, double *W);
+void vo_prim2cons(const double *W, double gamma, double *U);
+double vo_minmod(double a, double b);
+void vo_hllc_flux(const double *WL, const double *WR, double gamma, int dim, double *F);
+void vo_compute_face_fluxes(int64_t nf, const double *WL, const double *WR,
+                            const int32_t *axis, double gamma, double *F);
+
+/* uniform-grid driver (src/driver.jl + lib/RefMesh/src/RefMesh.jl) */
+int64_t vo_ncell(const vo_grid *g);
+double vo_compute_dt(const vo_grid *g, const double *U);
+void vo_accumulate_flux(const vo_grid *g, const double *U, double *acc,
+                        double *bflux, double bscale);
+void vo_accumulate_flux_gather(const vo_grid *g, const double *U, double *acc, int nthreads);
+void vo_step(const vo_grid *g, double *U, double *u0, double *acc, double dt,
+             double *bflux, int mode, int nthreads);
+int64_t vo_evolve(const vo_grid *g, double *U, double *u0, double *acc, double tfinal,
+                  int64_t max_steps, double *t, int mode, int nthreads);
+void vo_conserved_totals(const vo_grid *g, const double *U, double *out);
+int64_t vo_bflux_size(const vo_grid *g);
+
+/* exact Riemann solver (src/exact_riemann.jl) */
+void vo_exact_riemann_star(const double *WL, const double *WR, double gamma, double *pu);
+void vo_exact_riemann_sample(const double *WL, const double *WR, double gamma, double s,
+                             double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

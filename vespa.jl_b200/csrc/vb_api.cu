@@ -1,0 +1,632 @@
+// vb_api.cu -- the extern "C" entry points of libvespa_b200 (include/vespa_b200.h).
+//
+// Host-side runtime: contexts (device + stream + scratch), device-resident
+// uniform grids with their control block, the stepping loop that keeps dt on
+// the device, and error reporting.  No C++ exception crosses the ABI.
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/vespa_b200.h"
+#include "vb_launch.h"
+
+struct vb_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t launches = 0;
+    void *scratch = nullptr;  // vb_hllc_faces staging (device)
+    size_t scratch_bytes = 0;
+    cudaEvent_t marks[16] = {};
+};
+
+struct vb_grid {
+    vb_ctx *ctx = nullptr;
+    vb::Geom g{};
+    int precision = VB_FP64;
+    double *U = nullptr;   // state (and u0: the stage-2 update runs in place)
+    double *U1 = nullptr;  // stage-1 state
+    vb::Ctrl *ctrl = nullptr;   // device control block
+    vb::Ctrl *hctrl = nullptr;  // pinned host mirror
+    double *partials = nullptr;
+    double *totals = nullptr;
+    double *htot = nullptr;     // pinned
+    double *bflux = nullptr;
+    int64_t bflux_n = 0;
+    bool bflux_on = false;
+    bool invdt_valid = false;   // ctrl->invdt_bits holds the CFL max of the current state
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define VB_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(e_ == cudaErrorMemoryAllocation ? VB_ENOMEM : VB_ECUDA,            \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+#define VB_CHECK_LAUNCH(ctx, n)                                                            \
+    do {                                                                                   \
+        int n_ = (n);                                                                      \
+        if (n_ < 0) return fail(VB_EINVAL, "invalid launch configuration");               \
+        (ctx)->launches += n_;                                                             \
+        cudaError_t e_ = cudaGetLastError();                                               \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(VB_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+int use(vb_ctx *ctx)
+{
+    if (!ctx) return fail(VB_EINVAL, "null context");
+    VB_CUDA(cudaSetDevice(ctx->device));
+    return VB_OK;
+}
+
+int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout)
+{
+    double *bf = gr->bflux_on ? gr->bflux : nullptr;
+    int n = gr->precision == VB_MIXED
+                ? vb::launch_stage_mixed(gr->g, st, Uin, U0, Uout, gr->ctrl, bf, gr->ctx->stream)
+                : vb::launch_stage_fp64(gr->g, st, Uin, U0, Uout, gr->ctrl, bf, gr->ctx->stream);
+    VB_CHECK_LAUNCH(gr->ctx, n);
+    return VB_OK;
+}
+
+// One RK2 step whose dt is already in the control block.
+int rk2(vb_grid *gr)
+{
+    int rc = stage(gr, 1, gr->U, gr->U, gr->U1);
+    if (rc) return rc;
+    rc = stage(gr, 2, gr->U1, gr->U, gr->U);
+    if (rc) return rc;
+    gr->invdt_valid = true;
+    return VB_OK;
+}
+
+int pull_ctrl(vb_grid *gr)
+{
+    VB_CUDA(cudaMemcpyAsync(gr->hctrl, gr->ctrl, sizeof(vb::Ctrl), cudaMemcpyDeviceToHost,
+                            gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    return VB_OK;
+}
+
+int ensure_cfl(vb_grid *gr)
+{
+    if (gr->invdt_valid) return VB_OK;
+    VB_CHECK_LAUNCH(gr->ctx, vb::launch_cfl(gr->g, gr->U, gr->ctrl, gr->ctx->stream));
+    gr->invdt_valid = true;
+    return VB_OK;
+}
+
+// Queue `count` CFL-limited steps (each: finalize dt, stage 1, stage 2).
+int queue_steps(vb_grid *gr, int64_t count)
+{
+    for (int64_t i = 0; i < count; ++i) {
+        VB_CHECK_LAUNCH(gr->ctx, vb::launch_finalize_cfl(gr->g, gr->ctrl, gr->ctx->stream));
+        int rc = rk2(gr);
+        if (rc) return rc;
+    }
+    return VB_OK;
+}
+
+// Host-side write of control fields (stream-ordered through a tiny copy).
+int push_ctrl(vb_grid *gr)
+{
+    VB_CUDA(cudaMemcpyAsync(gr->ctrl, gr->hctrl, sizeof(vb::Ctrl), cudaMemcpyHostToDevice,
+                            gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    return VB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vb_abi_version(void) { return VB_ABI_VERSION; }
+
+int vb_last_error(char *buf, size_t len)
+{
+    if (buf && len) {
+        size_t n = g_err.size() < len - 1 ? g_err.size() : len - 1;
+        std::memcpy(buf, g_err.data(), n);
+        buf[n] = '\0';
+    }
+    return (int)g_err.size();
+}
+
+int vb_ctx_create(int device, vb_ctx **out)
+{
+    if (!out) return fail(VB_EINVAL, "null output pointer");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(VB_ECUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return fail(VB_EINVAL, "device index out of range");
+    VB_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    VB_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10 || prop.minor != 0)
+        return fail(VB_ENOTSUP, std::string("libvespa_b200 is built for sm_100a; device is ") +
+                                    prop.name + " (sm_" + std::to_string(prop.major) +
+                                    std::to_string(prop.minor) + ")");
+    vb_ctx *ctx = new (std::nothrow) vb_ctx();
+    if (!ctx) return fail(VB_ENOMEM, "host allocation failed");
+    ctx->device = device;
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return fail(VB_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    *out = ctx;
+    return VB_OK;
+}
+
+int vb_ctx_destroy(vb_ctx *ctx)
+{
+    if (!ctx) return VB_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    for (cudaEvent_t &e : ctx->marks)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return VB_OK;
+}
+
+int vb_ctx_synchronize(vb_ctx *ctx)
+{
+    int rc = use(ctx);
+    if (rc) return rc;
+    VB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return VB_OK;
+}
+
+int vb_ctx_stream(vb_ctx *ctx, void **stream)
+{
+    if (!ctx || !stream) return fail(VB_EINVAL, "null argument");
+    *stream = (void *)ctx->stream;
+    return VB_OK;
+}
+
+int vb_ctx_launch_count(vb_ctx *ctx, int64_t *count)
+{
+    if (!ctx || !count) return fail(VB_EINVAL, "null argument");
+    *count = ctx->launches;
+    return VB_OK;
+}
+
+int vb_ctx_mark(vb_ctx *ctx, int slot)
+{
+    int rc = use(ctx);
+    if (rc) return rc;
+    if (slot < 0 || slot >= 16) return fail(VB_EINVAL, "slot must be in 0..15");
+    if (!ctx->marks[slot]) VB_CUDA(cudaEventCreate(&ctx->marks[slot]));
+    VB_CUDA(cudaEventRecord(ctx->marks[slot], ctx->stream));
+    return VB_OK;
+}
+
+int vb_ctx_elapsed_ms(vb_ctx *ctx, int a, int b, float *ms)
+{
+    int rc = use(ctx);
+    if (rc) return rc;
+    if (!ms || a < 0 || a >= 16 || b < 0 || b >= 16 || !ctx->marks[a] || !ctx->marks[b])
+        return fail(VB_EINVAL, "unrecorded mark or null output");
+    VB_CUDA(cudaEventSynchronize(ctx->marks[b]));
+    VB_CUDA(cudaEventElapsedTime(ms, ctx->marks[a], ctx->marks[b]));
+    return VB_OK;
+}
+
+int vb_hllc_faces_device_async(vb_ctx *ctx, int64_t nf, const double *dWL, const double *dWR,
+                               const int32_t *daxis, double gamma, double *dF)
+{
+    int rc = use(ctx);
+    if (rc) return rc;
+    if (nf < 0) return fail(VB_EINVAL, "nf < 0");
+    if (nf == 0) return VB_OK;
+    if (!dWL || !dWR || !daxis || !dF) return fail(VB_EINVAL, "null buffer");
+    if (!(gamma > 1.0)) return fail(VB_EINVAL, "gamma must exceed 1");
+    VB_CHECK_LAUNCH(ctx, vb::launch_hllc_faces(nf, dWL, dWR, daxis, gamma, dF, ctx->stream));
+    return VB_OK;
+}
+
+int vb_hllc_faces(vb_ctx *ctx, int64_t nf, const double *WL, const double *WR,
+                  const int32_t *axis, double gamma, double *F)
+{
+    int rc = use(ctx);
+    if (rc) return rc;
+    if (nf < 0) return fail(VB_EINVAL, "nf < 0");
+    if (nf == 0) return VB_OK;  // the reference returns F untouched for nf == 0
+    if (!WL || !WR || !axis || !F) return fail(VB_EINVAL, "null buffer");
+    for (int64_t f = 0; f < nf; ++f)
+        if (axis[f] < 1 || axis[f] > 3) return fail(VB_EINVAL, "axis entries must be 1, 2 or 3");
+    const size_t bw = sizeof(double) * 5 * (size_t)nf;
+    const size_t ba = sizeof(int32_t) * (size_t)nf;
+    const size_t need = 3 * bw + ((ba + 255) & ~(size_t)255);
+    if (need > ctx->scratch_bytes) {
+        if (ctx->scratch) cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+        VB_CUDA(cudaMalloc(&ctx->scratch, need));
+        ctx->scratch_bytes = need;
+    }
+    char *base = (char *)ctx->scratch;
+    double *dWL = (double *)base;
+    double *dWR = (double *)(base + bw);
+    double *dF = (double *)(base + 2 * bw);
+    int32_t *dax = (int32_t *)(base + 3 * bw);
+    VB_CUDA(cudaMemcpyAsync(dWL, WL, bw, cudaMemcpyHostToDevice, ctx->stream));
+    VB_CUDA(cudaMemcpyAsync(dWR, WR, bw, cudaMemcpyHostToDevice, ctx->stream));
+    VB_CUDA(cudaMemcpyAsync(dax, axis, ba, cudaMemcpyHostToDevice, ctx->stream));
+    VB_CHECK_LAUNCH(ctx, vb::launch_hllc_faces(nf, dWL, dWR, dax, gamma, dF, ctx->stream));
+    VB_CUDA(cudaMemcpyAsync(F, dF, bw, cudaMemcpyDeviceToHost, ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return VB_OK;
+}
+
+int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid **out)
+{
+    if (!out) return fail(VB_EINVAL, "null output pointer");
+    *out = nullptr;
+    int rc = use(ctx);
+    if (rc) return rc;
+    if (!d) return fail(VB_EINVAL, "null problem descriptor");
+    if (d->ndim < 1 || d->ndim > 3) return fail(VB_EINVAL, "ndim must be 1, 2 or 3");
+    if (precision != VB_FP64 && precision != VB_MIXED) return fail(VB_EINVAL, "unknown precision");
+    // Problem validation, src/problem.jl:39-46
+    if (!(d->gamma > 1.0)) return fail(VB_EINVAL, "gamma must exceed 1");
+    if (!(d->cfl > 0.0 && d->cfl <= 1.0)) return fail(VB_EINVAL, "cfl must be in (0, 1]");
+    if (!(d->aexp > 0.0)) return fail(VB_EINVAL, "aexp must be positive");
+    if (d->flags != 0) return fail(VB_EINVAL, "flags must be 0");
+    vb::Geom g{};
+    g.nd = d->ndim;
+    int64_t s = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (a < d->ndim) {
+            if (d->dims[a] < 1) return fail(VB_EINVAL, "all dims must be positive");
+            if (!(d->hi[a] > d->lo[a])) return fail(VB_EINVAL, "domain must have hi > lo");
+            for (int side = 0; side < 2; ++side) {
+                int bc = side ? d->bc_hi[a] : d->bc_lo[a];
+                if (bc < VB_BC_OUTFLOW || bc > VB_BC_REFLECTING)
+                    return fail(VB_EINVAL, "unknown boundary condition");
+            }
+            if ((d->bc_lo[a] == VB_BC_PERIODIC) != (d->bc_hi[a] == VB_BC_PERIODIC))
+                return fail(VB_EINVAL, "a periodic axis must be periodic on both sides");
+            g.n[a] = d->dims[a];
+            g.bc_lo[a] = d->bc_lo[a];
+            g.bc_hi[a] = d->bc_hi[a];
+        } else {
+            g.n[a] = 1;
+            g.bc_lo[a] = g.bc_hi[a] = VB_BC_PERIODIC;
+        }
+        g.stride[a] = s;
+        if (s > INT64_MAX / g.n[a]) return fail(VB_EINVAL, "cell count overflows");
+        s *= g.n[a];
+    }
+    g.ncell = s;
+    // _width, face_area, cell_volume (lib/RefMesh/src/RefMesh.jl:122-142)
+    for (int a = 0; a < g.nd; ++a) g.w[a] = (d->hi[a] - d->lo[a]) / (double)d->dims[a];
+    for (int a = 0; a < g.nd; ++a) {
+        double ar = 1.0;
+        for (int e = 0; e < g.nd; ++e)
+            if (e != a) ar *= g.w[e];
+        g.area[a] = ar;
+    }
+    double v = g.w[0];
+    for (int a = 1; a < g.nd; ++a) v = v * g.w[a];
+    g.vol = v;
+    g.gamma = d->gamma;
+    g.cfl = d->cfl;
+    g.aexp = d->aexp;
+
+    vb_grid *gr = new (std::nothrow) vb_grid();
+    if (!gr) return fail(VB_ENOMEM, "host allocation failed");
+    gr->ctx = ctx;
+    gr->g = g;
+    gr->precision = precision;
+    const size_t bytes = sizeof(double) * 5 * (size_t)g.ncell;
+    auto cleanup = [&](int code, const std::string &msg) {
+        vb_grid_destroy(gr);
+        return fail(code, msg);
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&gr->U, bytes)) != cudaSuccess ||
+        (e = cudaMalloc(&gr->U1, bytes)) != cudaSuccess ||
+        (e = cudaMalloc(&gr->ctrl, sizeof(vb::Ctrl))) != cudaSuccess ||
+        (e = cudaMalloc(&gr->partials, sizeof(double) * 5 * vb::TOTALS_PARTS)) != cudaSuccess ||
+        (e = cudaMalloc(&gr->totals, sizeof(double) * 5)) != cudaSuccess ||
+        (e = cudaMallocHost(&gr->hctrl, sizeof(vb::Ctrl))) != cudaSuccess ||
+        (e = cudaMallocHost(&gr->htot, sizeof(double) * 5)) != cudaSuccess)
+        return cleanup(VB_ENOMEM, std::string("grid allocation: ") + cudaGetErrorString(e));
+    std::memset(gr->hctrl, 0, sizeof(vb::Ctrl));
+    gr->hctrl->tfinal = INFINITY;
+    gr->hctrl->step_limit = LLONG_MAX;
+    if ((e = cudaMemsetAsync(gr->U, 0, bytes, ctx->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(gr->U1, 0, bytes, ctx->stream)) != cudaSuccess)
+        return cleanup(VB_ECUDA, cudaGetErrorString(e));
+    rc = push_ctrl(gr);
+    if (rc) {
+        std::string m = g_err;
+        return cleanup(rc, m);
+    }
+    *out = gr;
+    return VB_OK;
+}
+
+int vb_grid_destroy(vb_grid *gr)
+{
+    if (!gr) return VB_OK;
+    if (gr->ctx) {
+        cudaSetDevice(gr->ctx->device);
+        cudaStreamSynchronize(gr->ctx->stream);
+    }
+    cudaFree(gr->U);
+    cudaFree(gr->U1);
+    cudaFree(gr->ctrl);
+    cudaFree(gr->partials);
+    cudaFree(gr->totals);
+    cudaFree(gr->bflux);
+    cudaFreeHost(gr->hctrl);
+    cudaFreeHost(gr->htot);
+    delete gr;
+    return VB_OK;
+}
+
+int vb_grid_ncell(const vb_grid *gr, int64_t *n)
+{
+    if (!gr || !n) return fail(VB_EINVAL, "null argument");
+    *n = gr->g.ncell;
+    return VB_OK;
+}
+
+int vb_grid_upload(vb_grid *gr, const double *U)
+{
+    if (!gr || !U) return fail(VB_EINVAL, "null argument");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    VB_CUDA(cudaMemcpyAsync(gr->U, U, sizeof(double) * 5 * (size_t)gr->g.ncell,
+                            cudaMemcpyHostToDevice, gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    gr->invdt_valid = false;
+    return VB_OK;
+}
+
+int vb_grid_download(vb_grid *gr, double *U)
+{
+    if (!gr || !U) return fail(VB_EINVAL, "null argument");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    VB_CUDA(cudaMemcpyAsync(U, gr->U, sizeof(double) * 5 * (size_t)gr->g.ncell,
+                            cudaMemcpyDeviceToHost, gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    return VB_OK;
+}
+
+int vb_grid_device_state(vb_grid *gr, double **dU)
+{
+    if (!gr || !dU) return fail(VB_EINVAL, "null argument");
+    *dU = gr->U;
+    gr->invdt_valid = false;  // the caller may write through the pointer
+    return VB_OK;
+}
+
+int vb_grid_set_time(vb_grid *gr, double t, int64_t step)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    rc = pull_ctrl(gr);
+    if (rc) return rc;
+    gr->hctrl->t = t;
+    gr->hctrl->step = step;
+    return push_ctrl(gr);
+}
+
+int vb_grid_get_time(vb_grid *gr, double *t, int64_t *step)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    rc = pull_ctrl(gr);
+    if (rc) return rc;
+    if (t) *t = gr->hctrl->t;
+    if (step) *step = gr->hctrl->step;
+    return VB_OK;
+}
+
+int vb_compute_dt(vb_grid *gr, double *dt)
+{
+    if (!gr || !dt) return fail(VB_EINVAL, "null argument");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    VB_CHECK_LAUNCH(gr->ctx, vb::launch_cfl(gr->g, gr->U, gr->ctrl, gr->ctx->stream));
+    gr->invdt_valid = true;
+    rc = pull_ctrl(gr);
+    if (rc) return rc;
+    unsigned long long bits = gr->hctrl->invdt_bits;
+    double invdt;
+    std::memcpy(&invdt, &bits, sizeof invdt);
+    if (std::isnan(invdt)) {
+        *dt = NAN;
+        return fail(VB_ENONFINITE, "non-finite or negative density/pressure in the state");
+    }
+    *dt = invdt == 0.0 ? INFINITY : gr->g.cfl / invdt;
+    return VB_OK;
+}
+
+int vb_step(vb_grid *gr, double dt)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    if (!std::isfinite(dt)) return fail(VB_EINVAL, "dt must be finite");
+    VB_CHECK_LAUNCH(gr->ctx, vb::launch_set_dt(gr->g, gr->ctrl, dt, gr->ctx->stream));
+    rc = rk2(gr);
+    if (rc) return rc;
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    return VB_OK;
+}
+
+int vb_run_steps_async(vb_grid *gr, int64_t nsteps)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    if (nsteps < 0) return fail(VB_EINVAL, "nsteps < 0");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    rc = ensure_cfl(gr);
+    if (rc) return rc;
+    return queue_steps(gr, nsteps);
+}
+
+int vb_evolve(vb_grid *gr, double tfinal, int64_t max_steps, double *t, int64_t *nsteps)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    rc = pull_ctrl(gr);
+    if (rc) return rc;
+    const long long step0 = gr->hctrl->step;
+    gr->hctrl->tfinal = tfinal;
+    gr->hctrl->step_limit = max_steps < 0 ? LLONG_MAX : step0 + max_steps;
+    gr->hctrl->flags = 0;
+    gr->hctrl->active = 1;
+    rc = push_ctrl(gr);
+    if (rc) return rc;
+    rc = ensure_cfl(gr);
+    if (rc) return rc;
+    // chunks of steps between host checks of the control block
+    int64_t chunk = 8;
+    int status = VB_OK;
+    for (;;) {
+        rc = queue_steps(gr, chunk);
+        if (rc) return rc;
+        rc = pull_ctrl(gr);
+        if (rc) return rc;
+        if (gr->hctrl->flags & vb::CTRL_F_NONFINITE) {
+            status = fail(VB_ENONFINITE, "non-finite dt: NaN or negative density/pressure");
+            break;
+        }
+        if (!gr->hctrl->active) break;
+        if (chunk < 64) chunk *= 2;
+    }
+    if (t) *t = gr->hctrl->t;
+    if (nsteps) *nsteps = gr->hctrl->step - step0;
+    gr->hctrl->tfinal = INFINITY;
+    gr->hctrl->step_limit = LLONG_MAX;
+    gr->hctrl->active = 0;
+    rc = push_ctrl(gr);
+    return status ? status : rc;
+}
+
+int vb_conserved_totals(vb_grid *gr, double out[5])
+{
+    if (!gr || !out) return fail(VB_EINVAL, "null argument");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    VB_CHECK_LAUNCH(gr->ctx, vb::launch_totals(gr->g, gr->U, gr->partials, vb::TOTALS_PARTS,
+                                               gr->totals, gr->ctx->stream));
+    VB_CUDA(cudaMemcpyAsync(gr->htot, gr->totals, sizeof(double) * 5, cudaMemcpyDeviceToHost,
+                            gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    std::memcpy(out, gr->htot, sizeof(double) * 5);
+    return VB_OK;
+}
+
+int vb_grid_profile_step(vb_grid *gr, int nsteps, double *ms_fin, double *ms_s1, double *ms_s2)
+{
+    if (!gr || nsteps <= 0) return fail(VB_EINVAL, "bad argument");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    rc = ensure_cfl(gr);
+    if (rc) return rc;
+    cudaEvent_t ev[4];
+    for (auto &e : ev) VB_CUDA(cudaEventCreate(&e));
+    double acc[3] = {0, 0, 0};
+    cudaStream_t s = gr->ctx->stream;
+    for (int i = 0; i < nsteps && rc == VB_OK; ++i) {
+        cudaEventRecord(ev[0], s);
+        VB_CHECK_LAUNCH(gr->ctx, vb::launch_finalize_cfl(gr->g, gr->ctrl, s));
+        cudaEventRecord(ev[1], s);
+        rc = stage(gr, 1, gr->U, gr->U, gr->U1);
+        cudaEventRecord(ev[2], s);
+        if (rc == VB_OK) rc = stage(gr, 2, gr->U1, gr->U, gr->U);
+        cudaEventRecord(ev[3], s);
+        cudaEventSynchronize(ev[3]);
+        float m;
+        for (int k = 0; k < 3; ++k) {
+            cudaEventElapsedTime(&m, ev[k], ev[k + 1]);
+            acc[k] += m;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    if (ms_fin) *ms_fin = acc[0] / nsteps;
+    if (ms_s1) *ms_s1 = acc[1] / nsteps;
+    if (ms_s2) *ms_s2 = acc[2] / nsteps;
+    return VB_OK;
+}
+
+int vb_bflux_size(const vb_grid *gr, int64_t *n)
+{
+    if (!gr || !n) return fail(VB_EINVAL, "null argument");
+    int64_t s = 0;
+    for (int a = 0; a < gr->g.nd; ++a) s += 2 * 5 * (gr->g.ncell / gr->g.n[a]);
+    *n = s;
+    return VB_OK;
+}
+
+int vb_bflux_enable(vb_grid *gr, int enable)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    if (enable && !gr->bflux) {
+        int64_t n = 0;
+        vb_bflux_size(gr, &n);
+        VB_CUDA(cudaMalloc(&gr->bflux, sizeof(double) * (size_t)n));
+        gr->bflux_n = n;
+        VB_CUDA(cudaMemsetAsync(gr->bflux, 0, sizeof(double) * (size_t)n, gr->ctx->stream));
+        VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    }
+    gr->bflux_on = enable != 0;
+    return VB_OK;
+}
+
+int vb_bflux_read(vb_grid *gr, double *out, int64_t n)
+{
+    if (!gr || !out) return fail(VB_EINVAL, "null argument");
+    if (!gr->bflux) return fail(VB_EINVAL, "boundary-flux register not enabled");
+    if (n != gr->bflux_n) return fail(VB_EINVAL, "size mismatch (see vb_bflux_size)");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    VB_CUDA(cudaMemcpyAsync(out, gr->bflux, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost,
+                            gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    return VB_OK;
+}
+
+int vb_bflux_clear(vb_grid *gr)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    if (!gr->bflux) return VB_OK;
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    VB_CUDA(cudaMemsetAsync(gr->bflux, 0, sizeof(double) * (size_t)gr->bflux_n, gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    return VB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+// vb_common.cuh -- device-side geometry, control block and small helpers
+// shared by every kernel translation unit of libvespa_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace vb {
+
+enum { BC_OUTFLOW = 0, BC_PERIODIC = 1, BC_REFLECTING = 2 };
+enum { PREC_FP64 = 0, PREC_MIXED = 1 };
+
+// Uniform-mesh geometry (lib/RefMesh/src/RefMesh.jl:122-142), passed by value
+// to kernels.  Unused axes have n = 1.
+struct Geom {
+    int nd;
+    int bc_lo[3];
+    int bc_hi[3];
+    int64_t n[3];
+    int64_t stride[3];
+    int64_t ncell;
+    double w[3];     // cell widths (hi - lo) / n
+    double area[3];  // face areas: product of the other axes' widths
+    double vol;      // cell volume: left-fold product of the widths
+    double gamma;
+    double cfl;
+    double aexp;
+};
+
+// Per-grid control block in device memory.  The stepping kernels read dt and
+// invV from here so a whole evolve! loop can run without host round trips.
+struct Ctrl {
+    double t;                       // simulation clock (sim.t)
+    double dt;                      // dt of the step in flight
+    double invV;                    // dt / (aexp * V)
+    double tfinal;                  // evolve target; +Inf for fixed-count runs
+    unsigned long long invdt_bits;  // running max of (|v_d| + c) / w_d (bit pattern)
+    long long step;                 // sim.step
+    long long step_limit;           // evolve: stop after this many steps
+    int active;                     // 1 while the step in flight must run
+    int flags;                      // error bits, CTRL_F_*
+};
+
+enum { CTRL_F_NONFINITE = 1 };
+
+// min/max: fmin/fmax (one instruction).  They differ from Julia's Base.min /
+// Base.max only in the sign of a zero result and in NaN handling.  Where they
+// are used (the HLLC wave speeds SL/SR, the pressure floor, the dt clip) a
+// zero's sign never reaches later arithmetic: SL and SR only feed the
+// SL >= 0 / SR <= 0 tests when they are zero.  NaN is caught separately by the
+// CFL reduction below.
+
+// NaN-propagating max used by the CFL reduction: any NaN wins.
+__device__ __forceinline__ double nan_max(double m, double x) { return (x > m || x != x) ? x : m; }
+
+// Non-negative doubles order like their unsigned bit patterns; a NaN (either
+// sign) has a larger pattern than +Inf, so a u64 max keeps NaN visible.
+__device__ __forceinline__ unsigned long long order_bits(double x)
+{
+    unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    // a negative NaN has the sign bit set: still larger than +Inf's pattern
+    return b;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide max folded into the control block's running max.  The read of
+// the current value skips atomics that cannot raise it (the value only grows).
+__device__ __forceinline__ void block_max_to(unsigned long long *dst, double v, double *smem32)
+{
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) smem32[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double x = lane < nw ? smem32[lane] : 0.0;
+        x = warp_max(x);
+        if (lane == 0) {
+            unsigned long long b = order_bits(x);
+            if (b > *((volatile unsigned long long *)dst)) atomicMax(dst, b);
+        }
+    }
+}
+
+}  // namespace vb

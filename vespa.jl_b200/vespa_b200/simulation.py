@@ -1,0 +1,236 @@
+"""Device-resident Simulation API (host side of the drop-in).
+
+Mirrors the reference's driver API on a device-resident uniform mesh:
+``Simulation`` (src/driver.jl:27-79), ``step!`` (333-359), ``compute_dt``
+(169-199), ``evolve!`` (483-508), ``conserved_totals``
+(src/diagnostics.jl:16-31), ``primitive_at`` / ``cell_samples`` /
+``dump_fields`` (diagnostics.jl:9-67).  Every call goes through the C ABI of
+libvespa_b200.so; the state never leaves the GPU unless the caller reads it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from collections import namedtuple
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _lib
+from .problem import IdealHydro, Problem, cons2prim, initial_state
+
+Totals = namedtuple("Totals", "mass momentum_x momentum_y momentum_z energy")
+
+PRECISIONS = {"fp64": _lib.FP64, "mixed": _lib.MIXED}
+
+
+class B200Mesh:
+    """A uniform mesh whose fields live in B200 device memory.
+
+    The device analogue of ``UniformMesh(dims, domain)``
+    (lib/RefMesh/src/RefMesh.jl:89-100): same geometry, same column-major
+    cell order, same boundary resolution."""
+
+    def __init__(self, dims, domain):
+        self.dims = tuple(int(n) for n in dims)
+        self.domain = tuple((float(a), float(b)) for a, b in domain)
+        if len(self.dims) != len(self.domain) or not 1 <= len(self.dims) <= 3:
+            raise ValueError("B200Mesh supports rank 1-3 with one (lo, hi) pair per axis")
+
+    def rank(self) -> int:
+        return len(self.dims)
+
+    def n_cells(self) -> int:
+        return int(np.prod(self.dims))
+
+    def cell_width(self):
+        return tuple((b - a) / n for (a, b), n in zip(self.domain, self.dims))
+
+    def cell_volume(self) -> float:
+        w = self.cell_width()
+        v = w[0]
+        for x in w[1:]:
+            v = v * x
+        return v
+
+
+class Simulation:
+    """Bind a Problem to a B200Mesh, allocate the device state and set the
+    initial conditions (src/driver.jl:62-79).
+
+    ``precision`` is ``"fp64"`` (bit-identical to the reference's float64
+    arithmetic) or ``"mixed"`` (float32 reconstruction and HLLC, float64 state,
+    pressure recovery, accumulation and reductions)."""
+
+    def __init__(self, backend: B200Mesh, problem: Problem, *, precision: str = "fp64",
+                 ctx: Optional[_lib.Context] = None, initial: Optional[np.ndarray] = None):
+        if tuple(backend.dims) != tuple(problem.dims):
+            raise ValueError("mesh dims do not match the problem")
+        self.backend = backend
+        self.problem = problem
+        self.model = IdealHydro(problem.gamma)
+        self.gamma = problem.gamma
+        self.precision = precision
+        self.ctx = ctx or _lib.default_context()
+        desc = _lib.ProblemDesc()
+        desc.ndim = backend.rank()
+        for d, ((lo, hi), (blo, bhi)) in enumerate(zip(backend.domain, problem.bc_pairs())):
+            desc.dims[d] = backend.dims[d]
+            desc.lo[d] = lo
+            desc.hi[d] = hi
+            desc.bc_lo[d] = blo
+            desc.bc_hi[d] = bhi
+        desc.gamma = problem.gamma
+        desc.cfl = problem.cfl
+        desc.aexp = 1.0
+        desc.flags = 0
+        h = C.c_void_p()
+        _lib.call("vb_grid_create", self.ctx.handle, C.byref(desc), PRECISIONS[precision],
+                  C.byref(h))
+        self.handle = h
+        self.ncell = backend.n_cells()
+        U = initial if initial is not None else initial_state(problem)
+        self.upload(U)
+
+    # -- lifetime --
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().vb_grid_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state I/O (the `sv` views) --
+    def upload(self, U: np.ndarray) -> None:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.shape != (5, self.ncell):
+            raise ValueError(f"state must have shape (5, {self.ncell})")
+        _lib.call("vb_grid_upload", self.handle, _lib.dptr(U))
+
+    def state(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((5, self.ncell))
+        _lib.call("vb_grid_download", self.handle, _lib.dptr(out))
+        return out
+
+    def device_state_ptr(self) -> int:
+        p = C.c_void_p()
+        _lib.call("vb_grid_device_state", self.handle, C.byref(p))
+        return p.value
+
+    # -- clock --
+    @property
+    def t(self) -> float:
+        t = C.c_double()
+        _lib.call("vb_grid_get_time", self.handle, C.byref(t), None)
+        return t.value
+
+    @property
+    def step(self) -> int:
+        n = C.c_int64()
+        _lib.call("vb_grid_get_time", self.handle, None, C.byref(n))
+        return n.value
+
+    def set_time(self, t: float, step: int = 0) -> None:
+        _lib.call("vb_grid_set_time", self.handle, float(t), int(step))
+
+    def profile_step(self, nsteps: int = 5) -> dict:
+        """Mean device milliseconds of each kernel of a CFL step (advances the state)."""
+        fin, s1, s2 = C.c_double(), C.c_double(), C.c_double()
+        _lib.call("vb_grid_profile_step", self.handle, int(nsteps), C.byref(fin), C.byref(s1),
+                  C.byref(s2))
+        return {"ms_finalize": fin.value, "ms_stage1": s1.value, "ms_stage2": s2.value}
+
+    # -- boundary-flux register --
+    def bflux_enable(self, on: bool = True) -> None:
+        _lib.call("vb_bflux_enable", self.handle, 1 if on else 0)
+
+    def bflux_clear(self) -> None:
+        _lib.call("vb_bflux_clear", self.handle)
+
+    def bflux_read(self) -> np.ndarray:
+        n = C.c_int64()
+        _lib.call("vb_bflux_size", self.handle, C.byref(n))
+        out = np.empty(n.value)
+        _lib.call("vb_bflux_read", self.handle, _lib.dptr(out), n.value)
+        return out
+
+
+def compute_dt(sim: Simulation) -> float:
+    """compute_dt(sim) (src/driver.jl:169-199)."""
+    dt = C.c_double()
+    _lib.call("vb_compute_dt", sim.handle, C.byref(dt))
+    return dt.value
+
+
+def step(sim: Simulation, dt: float) -> Simulation:
+    """step!(sim, dt) (src/driver.jl:333-359): one SSP-RK2 step."""
+    _lib.call("vb_step", sim.handle, float(dt))
+    return sim
+
+
+def evolve(sim: Simulation, *, tfinal: Optional[float] = None, max_steps: int = -1,
+           callback: Optional[Callable] = None, callback_every: int = 1) -> Simulation:
+    """evolve!(sim) (src/driver.jl:483-508): integrate to problem.tfinal.
+
+    The dt loop runs on the device.  ``callback(sim, stage)`` is called with
+    ``"init"`` before the first step and ``"step"`` after every
+    ``callback_every`` steps, as in the reference."""
+    tf = sim.problem.tfinal if tfinal is None else float(tfinal)
+    t = C.c_double()
+    n = C.c_int64()
+    if callback is None:
+        _lib.call("vb_evolve", sim.handle, tf, int(max_steps), C.byref(t), C.byref(n))
+        return sim
+    callback(sim, "init")
+    done = 0
+    every = max(1, int(callback_every))
+    while max_steps < 0 or done < max_steps:
+        chunk = every if max_steps < 0 else min(every, max_steps - done)
+        _lib.call("vb_evolve", sim.handle, tf, chunk, C.byref(t), C.byref(n))
+        done += n.value
+        if n.value == 0:
+            break
+        if n.value == chunk and callback_every > 0:
+            callback(sim, "step")
+        if n.value < chunk:
+            break
+    return sim
+
+
+def run_steps_async(sim: Simulation, nsteps: int) -> None:
+    """Queue `nsteps` CFL-limited RK2 steps on the context stream (no final time)."""
+    _lib.call("vb_run_steps_async", sim.handle, int(nsteps))
+
+
+def conserved_totals(sim: Simulation) -> Totals:
+    """conserved_totals(sim) (src/diagnostics.jl:16-31)."""
+    out = np.empty(5)
+    _lib.call("vb_conserved_totals", sim.handle, _lib.dptr(out))
+    return Totals(*[float(v) for v in out])
+
+
+def primitive_state(sim: Simulation) -> np.ndarray:
+    return cons2prim(sim.state(), sim.gamma)
+
+
+def primitive_at(sim: Simulation, cell: int) -> tuple:
+    """primitive_at(sim, cell) (src/diagnostics.jl:9)."""
+    return tuple(float(v) for v in primitive_state(sim)[:, int(cell)])
+
+
+def cell_samples(sim: Simulation):
+    """cell_samples(sim) (src/diagnostics.jl:40-48): (centres, primitives)."""
+    return sim.problem.cell_centers(), primitive_state(sim)
+
+
+def dump_fields(sim: Simulation) -> dict:
+    """dump_fields(sim) (src/diagnostics.jl:57-67), 1D only."""
+    if sim.backend.rank() != 1:
+        raise ValueError("dump_fields currently supports 1D; use cell_samples for ND")
+    (x,), W = cell_samples(sim)
+    return {"x": x, "density": W[0], "velocity_x": W[1], "pressure": W[4]}
