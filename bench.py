@@ -271,7 +271,8 @@ def run_ours(args, ranks: Ranks):
             clocks = sampler.stop()
         ranks.barrier()
         ms_max = ranks.max(ms)
-        out[prec] = {"ms": ms_max, "launches": launches, **sim.profile_step(5)}
+        out[prec] = {"ms": ms_max, "launches": launches, "kernel": sim.kernel,
+                     **sim.profile_step(5)}
         sim.close()
 
     # end to end through the public API: pinned host state in, K steps, state out
@@ -319,7 +320,7 @@ def run_ours(args, ranks: Ranks):
         "data": DATA,
         "config": {"workload": f"3D {n}^3 periodic PLM/minmod+HLLC SSP-RK2, gamma 5/3, CFL 0.4, "
                                "dt recomputed on device each step",
-                   "cells_per_gpu": cells, "precision": "mixed",
+                   "cells_per_gpu": cells, "precision": "mixed", "kernel": mixed["kernel"],
                    "l2": "inputs larger than L2 (671 MB per state buffer)",
                    "parallelism": f"one independent instance per GPU x{ranks.world}"},
         "fp64": {"value": round(fp64_value, 1), "unit": UNIT,

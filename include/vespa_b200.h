@@ -110,6 +110,16 @@ int vb_grid_upload(vb_grid *grid, const double *U);
 int vb_grid_download(vb_grid *grid, double *U);
 /* Device pointer of the state (5*ncell float64), valid until vb_grid_destroy. */
 int vb_grid_device_state(vb_grid *grid, double **dU);
+/* Kernel selection and tuning knobs (no counterpart in the reference, whose
+ * per-face loop has no launch shape).  VB_OPT_KERNEL: VB_KERNEL_AUTO picks the
+ * tiled 3D kernel when the grid allows it (nx, ny multiples of 16, nz >= 2),
+ * VB_KERNEL_CELL forces the cell-centric kernel, VB_KERNEL_TILED requires the
+ * tiled one.  VB_OPT_TILE_KZ: z planes per tiled work item.  Results do not
+ * depend on either knob. */
+enum { VB_OPT_KERNEL = 1, VB_OPT_TILE_KZ = 2 };
+enum { VB_KERNEL_AUTO = 0, VB_KERNEL_CELL = 1, VB_KERNEL_TILED = 2 };
+int vb_grid_set_option(vb_grid *grid, int option, int64_t value);
+int vb_grid_get_option(const vb_grid *grid, int option, int64_t *value);
 /* Simulation clock (sim.t, sim.step). */
 int vb_grid_set_time(vb_grid *grid, double t, int64_t step);
 int vb_grid_get_time(vb_grid *grid, double *t, int64_t *step);

@@ -3,6 +3,8 @@
 // Host-side runtime: contexts (device + stream + scratch), device-resident
 // uniform grids with their control block, the stepping loop that keeps dt on
 // the device, and error reporting.  No C++ exception crosses the ABI.
+#include <cudaTypedefs.h>
+
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -36,6 +38,9 @@ struct vb_grid {
     int64_t bflux_n = 0;
     bool bflux_on = false;
     bool invdt_valid = false;   // ctrl->invdt_bits holds the CFL max of the current state
+    bool tiled = false;         // the tiled 3D kernels apply to this grid
+    int kz = 64;                // z planes per tiled work item
+    vb::TiledMaps maps_U{}, maps_U1{};  // TMA descriptors of the two stage inputs
 };
 
 namespace {
@@ -73,9 +78,63 @@ int use(vb_ctx *ctx)
     return VB_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry-point lookup (no
+// link-time dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// 4-D (x, y, z, field) float64 tensor map over a state buffer with box
+// (bx, by, 1, 5).  Out-of-range coordinates read zeros.
+int encode_state_map(CUtensorMap *m, const double *base, const vb::Geom &g, uint32_t bx,
+                     uint32_t by)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc) return fail(VB_ENOTSUP, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[4] = {(cuuint64_t)g.n[0], (cuuint64_t)g.n[1], (cuuint64_t)g.n[2], 5};
+    cuuint64_t strides[3] = {(cuuint64_t)g.n[0] * 8, (cuuint64_t)(g.n[0] * g.n[1]) * 8,
+                             (cuuint64_t)g.ncell * 8};
+    cuuint32_t box[4] = {bx, by, 1, 5};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(VB_ECUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return VB_OK;
+}
+
+int encode_maps(vb::TiledMaps *m, const double *base, const vb::Geom &g)
+{
+    int rc = encode_state_map(&m->in_int, base, g, 16, 16);
+    if (!rc) rc = encode_state_map(&m->in_xs, base, g, 2, 16);
+    if (!rc) rc = encode_state_map(&m->in_ys, base, g, 16, 2);
+    return rc;
+}
+
 int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout)
 {
     double *bf = gr->bflux_on ? gr->bflux : nullptr;
+    if (gr->tiled && !bf) {
+        const vb::TiledMaps &m = (Uin == gr->U) ? gr->maps_U : gr->maps_U1;
+        int n = gr->precision == VB_MIXED
+                    ? vb::launch_stage_tiled3d_mixed(m, gr->g, gr->kz, st, Uin, U0, Uout, gr->ctrl,
+                                                     gr->ctx->stream)
+                    : vb::launch_stage_tiled3d_fp64(m, gr->g, gr->kz, st, Uin, U0, Uout, gr->ctrl,
+                                                    gr->ctx->stream);
+        VB_CHECK_LAUNCH(gr->ctx, n);
+        return VB_OK;
+    }
     int n = gr->precision == VB_MIXED
                 ? vb::launch_stage_mixed(gr->g, st, Uin, U0, Uout, gr->ctrl, bf, gr->ctx->stream)
                 : vb::launch_stage_fp64(gr->g, st, Uin, U0, Uout, gr->ctrl, bf, gr->ctx->stream);
@@ -319,6 +378,7 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
     g.ncell = s;
     // _width, face_area, cell_volume (lib/RefMesh/src/RefMesh.jl:122-142)
     for (int a = 0; a < g.nd; ++a) g.w[a] = (d->hi[a] - d->lo[a]) / (double)d->dims[a];
+    for (int a = 0; a < 3; ++a) g.invw[a] = a < g.nd ? 1.0 / g.w[a] : 0.0;
     for (int a = 0; a < g.nd; ++a) {
         double ar = 1.0;
         for (int e = 0; e < g.nd; ++e)
@@ -362,8 +422,61 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
         std::string m = g_err;
         return cleanup(rc, m);
     }
+    if (vb::tiled3d_supported(g)) {
+        rc = encode_maps(&gr->maps_U, gr->U, g);
+        if (!rc) rc = encode_maps(&gr->maps_U1, gr->U1, g);
+        if (rc) {
+            std::string m = g_err;
+            return cleanup(rc, m);
+        }
+        gr->tiled = true;
+        gr->kz = g.n[2] >= 128 ? 64 : (int)((g.n[2] + 1) / 2);
+    }
     *out = gr;
     return VB_OK;
+}
+
+int vb_grid_set_option(vb_grid *gr, int option, int64_t value)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    switch (option) {
+    case VB_OPT_KERNEL:
+        if (value == VB_KERNEL_CELL) {
+            gr->tiled = false;
+        } else if (value == VB_KERNEL_AUTO || value == VB_KERNEL_TILED) {
+            if (!vb::tiled3d_supported(gr->g)) {
+                if (value == VB_KERNEL_TILED)
+                    return fail(VB_ENOTSUP, "tiled kernel needs a 3D grid with nx, ny multiples of 16");
+                gr->tiled = false;
+                return VB_OK;
+            }
+            if (!gr->maps_U.in_int.opaque[0] && !gr->maps_U.in_int.opaque[1]) {
+                int rc = encode_maps(&gr->maps_U, gr->U, gr->g);
+                if (!rc) rc = encode_maps(&gr->maps_U1, gr->U1, gr->g);
+                if (rc) return rc;
+            }
+            gr->tiled = true;
+        } else {
+            return fail(VB_EINVAL, "unknown kernel selector");
+        }
+        return VB_OK;
+    case VB_OPT_TILE_KZ:
+        if (value < 1 || value > gr->g.n[2]) return fail(VB_EINVAL, "kz must be in 1..nz");
+        gr->kz = (int)value;
+        return VB_OK;
+    default:
+        return fail(VB_EINVAL, "unknown option");
+    }
+}
+
+int vb_grid_get_option(const vb_grid *gr, int option, int64_t *value)
+{
+    if (!gr || !value) return fail(VB_EINVAL, "null argument");
+    switch (option) {
+    case VB_OPT_KERNEL: *value = gr->tiled ? VB_KERNEL_TILED : VB_KERNEL_CELL; return VB_OK;
+    case VB_OPT_TILE_KZ: *value = gr->kz; return VB_OK;
+    default: return fail(VB_EINVAL, "unknown option");
+    }
 }
 
 int vb_grid_destroy(vb_grid *gr)
@@ -476,7 +589,10 @@ int vb_step(vb_grid *gr, double dt)
     VB_CHECK_LAUNCH(gr->ctx, vb::launch_set_dt(gr->g, gr->ctrl, dt, gr->ctx->stream));
     rc = rk2(gr);
     if (rc) return rc;
-    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    rc = pull_ctrl(gr);
+    if (rc) return rc;
+    if (gr->hctrl->flags & vb::CTRL_F_TIMEOUT)
+        return fail(VB_ETIMEOUT, "a bounded device wait (TMA stage load) gave up");
     return VB_OK;
 }
 
@@ -517,6 +633,10 @@ int vb_evolve(vb_grid *gr, double tfinal, int64_t max_steps, double *t, int64_t 
         if (rc) return rc;
         if (gr->hctrl->flags & vb::CTRL_F_NONFINITE) {
             status = fail(VB_ENONFINITE, "non-finite dt: NaN or negative density/pressure");
+            break;
+        }
+        if (gr->hctrl->flags & vb::CTRL_F_TIMEOUT) {
+            status = fail(VB_ETIMEOUT, "a bounded device wait (TMA stage load) gave up");
             break;
         }
         if (!gr->hctrl->active) break;

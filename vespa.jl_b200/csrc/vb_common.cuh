@@ -21,6 +21,7 @@ struct Geom {
     int64_t stride[3];
     int64_t ncell;
     double w[3];     // cell widths (hi - lo) / n
+    double invw[3];  // 1 / w (VB_MIXED CFL term only)
     double area[3];  // face areas: product of the other axes' widths
     double vol;      // cell volume: left-fold product of the widths
     double gamma;
@@ -40,9 +41,10 @@ struct Ctrl {
     long long step_limit;           // evolve: stop after this many steps
     int active;                     // 1 while the step in flight must run
     int flags;                      // error bits, CTRL_F_*
+    unsigned int work[2];           // work-queue cursors of the two stage kernels
 };
 
-enum { CTRL_F_NONFINITE = 1 };
+enum { CTRL_F_NONFINITE = 1, CTRL_F_TIMEOUT = 2 };
 
 // min/max: fmin/fmax (one instruction).  They differ from Julia's Base.min /
 // Base.max only in the sign of a zero result and in NaN handling.  Where they

@@ -8,6 +8,7 @@
 //   - batched HLLC face kernel (the compute_face_fluxes! drop-in)
 #include "vb_launch.h"
 #include "vb_stage_generic.cuh"
+#include "vb_stage_tiled3d.cuh"
 
 namespace vb {
 
@@ -64,6 +65,7 @@ __global__ void k_finalize_cfl(Geom g, Ctrl *ctrl)
     ctrl->invV = dt / (g.aexp * g.vol);
     ctrl->active = 1;
     ctrl->invdt_bits = 0ull;
+    ctrl->work[0] = ctrl->work[1] = 0u;
 }
 
 // step!(sim, dt) with a caller-chosen dt.
@@ -73,6 +75,7 @@ __global__ void k_set_dt(Geom g, Ctrl *ctrl, double dt)
     ctrl->invV = dt / (g.aexp * g.vol);
     ctrl->active = 1;
     ctrl->invdt_bits = 0ull;
+    ctrl->work[0] = ctrl->work[1] = 0u;
 }
 
 // conserved_totals (src/diagnostics.jl:16-31): fixed grid of TOTALS_PARTS
@@ -153,6 +156,13 @@ int launch_stage_fp64(const Geom &g, int stage, const double *Uin, const double 
     case 32: return launch_generic<3, 2>(g, Uin, U0, Uout, ctrl, bflux, s);
     default: return -1;
     }
+}
+
+int launch_stage_tiled3d_fp64(const TiledMaps &m, const Geom &g, int kz, int stage,
+                              const double *Uin, const double *U0, double *Uout, Ctrl *ctrl,
+                              cudaStream_t s)
+{
+    return launch_tiled3d<double, 2>(m, g, kz, stage, Uin, U0, Uout, ctrl, s);
 }
 
 static unsigned grid_for(int64_t n, int bs, int maxb)

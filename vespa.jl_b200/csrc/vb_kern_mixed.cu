@@ -3,6 +3,7 @@
 // accumulation and CFL reduction; float32 reconstruction and HLLC.
 #include "vb_launch.h"
 #include "vb_stage_generic.cuh"
+#include "vb_stage_tiled3d.cuh"
 
 namespace vb {
 
@@ -20,6 +21,13 @@ int launch_generic(const Geom &g, const double *Uin, const double *U0, double *U
 }
 
 }  // namespace
+
+int launch_stage_tiled3d_mixed(const TiledMaps &m, const Geom &g, int kz, int stage,
+                               const double *Uin, const double *U0, double *Uout, Ctrl *ctrl,
+                               cudaStream_t s)
+{
+    return launch_tiled3d<float, 3>(m, g, kz, stage, Uin, U0, Uout, ctrl, s);
+}
 
 int launch_stage_mixed(const Geom &g, int stage, const double *Uin, const double *U0,
                        double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s)

@@ -8,6 +8,7 @@
 #pragma once
 
 #include "vb_common.cuh"
+#include "vb_tma.cuh"
 
 namespace vb {
 
@@ -86,20 +87,24 @@ __device__ __forceinline__ void hllc_flux(const T WL[5], const T WR[5], double g
     // SL >= 0 -> FL;  SR <= 0 -> FR;  else the star flux of the side picked by
     // the sign of S*.  Each side's quantities are the same expressions as the
     // reference's prim2cons / euler_flux, evaluated for that side only.
-    const T *W;
+    bool left, star;
     T SK, Sstar = T(0);
-    bool star;
     if (SL >= T(0)) {
-        W = WL; SK = SL; star = false;
+        left = true; SK = SL; star = false;
     } else if (SR <= T(0)) {
-        W = WR; SK = SR; star = false;
+        left = false; SK = SR; star = false;
     } else {
         Sstar = (pR - pL + rhoL * unL * (SL - unL) - rhoR * unR * (SR - unR)) /
                 (rhoL * (SL - unL) - rhoR * (SR - unR));
-        if (Sstar >= T(0)) { W = WL; SK = SL; } else { W = WR; SK = SR; }
+        left = Sstar >= T(0);
+        SK = left ? SL : SR;
         star = true;
     }
-    const T rho = W[0], vx = W[1], vy = W[2], vz = W[3], p = W[4];
+    // value selects (not a pointer to one side) keep both states in registers
+    const T rho = left ? WL[0] : WR[0], vx = left ? WL[1] : WR[1];
+    const T vy = left ? WL[2] : WR[2], vz = left ? WL[3] : WR[3];
+    const T p = left ? WL[4] : WR[4];
+    const T W[5] = {rho, vx, vy, vz, p};
     const T un = W[DIM];
     const T E = total_energy<T>(W, g);
     // euler_flux (riemann.jl:9-20); the +0 on tangential momentum is omitted
@@ -126,6 +131,97 @@ __device__ __forceinline__ void hllc_flux(const T WL[5], const T WR[5], double g
                      factor * Estar};
 #pragma unroll
     for (int k = 0; k < 5; ++k) F[k] = Fk[k] + SK * (Us[k] - Uk[k]);
+}
+
+// PLM face value w + h*s (src/driver.jl:227-233).  In float the product-add
+// is an explicit fused multiply-add so every call site rounds identically (a
+// face evaluated from both neighbouring cells must give one value); in the
+// float64 unit (-fmad=false) it is a separately rounded product and sum, as
+// in the reference.
+__device__ __forceinline__ double face_val(double w, double h, double s) { return w + h * s; }
+__device__ __forceinline__ float face_val(float w, float h, float s) { return __fmaf_rn(h, s, w); }
+
+// The same Riemann solve behind one call for every face of the cell-centric
+// kernel: in float, a non-inlined body guarantees identical instructions for
+// the two evaluations of each interior face (flux conservation to the bit).
+template <typename T, int DIM>
+__device__ __noinline__ void hllc_flux_shared(const T *WL, const T *WR, double gamma, T *F)
+{
+    T l[5], r[5], f[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        l[k] = WL[k];
+        r[k] = WR[k];
+    }
+    hllc_flux<T, DIM>(l, r, gamma, f);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) F[k] = f[k];
+}
+
+template <typename T, int DIM>
+__device__ __forceinline__ void hllc_face(const T WL[5], const T WR[5], double gamma, T F[5])
+{
+    if constexpr (sizeof(T) == 4)
+        hllc_flux_shared<T, DIM>(WL, WR, gamma, F);
+    else
+        hllc_flux<T, DIM>(WL, WR, gamma, F);
+}
+
+// Float32 HLLC for VB_MIXED: the same algebra as hllc_flux (Davis speeds,
+// contact speed S*, star flux F + SK (U* - U)) with approximate reciprocals
+// and square roots (rcp.approx / sqrt.approx, ~1 ulp) and contracted
+// multiply-adds.  ig1 = 1 / (gamma - 1).  Used where each face is evaluated
+// exactly once, so conservation does not depend on rounding.
+template <int DIM>
+__device__ __forceinline__ void hllc_flux_fast(const float WL[5], const float WR[5], float g,
+                                               float ig1, float F[5])
+{
+    const float rhoL = WL[0], rhoR = WR[0];
+    const float pL = WL[4], pR = WR[4];
+    const float unL = WL[DIM], unR = WR[DIM];
+    const float irL = rcp_approx(rhoL), irR = rcp_approx(rhoR);
+    const float cL = sqrt_approx(g * pL * irL);
+    const float cR = sqrt_approx(g * pR * irR);
+    const float SL = fminf(unL - cL, unR - cR);
+    const float SR = fmaxf(unL + cL, unR + cR);
+    bool left, star;
+    float Sstar = 0.f;
+    if (SL >= 0.f) {
+        left = true; star = false;
+    } else if (SR <= 0.f) {
+        left = false; star = false;
+    } else {
+        const float aL = rhoL * (SL - unL), aR = rhoR * (SR - unR);
+        Sstar = (pR - pL + unL * aL - unR * aR) * rcp_approx(aL - aR);
+        left = Sstar >= 0.f;
+        star = true;
+    }
+    const float SK = left ? SL : SR, ir = left ? irL : irR;
+    const float rho = left ? WL[0] : WR[0], vx = left ? WL[1] : WR[1];
+    const float vy = left ? WL[2] : WR[2], vz = left ? WL[3] : WR[3];
+    const float p = left ? WL[4] : WR[4];
+    const float un = DIM == 1 ? vx : (DIM == 2 ? vy : vz);
+    const float E = p * ig1 + 0.5f * rho * (vx * vx + vy * vy + vz * vz);
+    const float mun = rho * un;
+    F[0] = mun;
+    F[1] = mun * vx;
+    F[2] = mun * vy;
+    F[3] = mun * vz;
+    F[DIM] += p;
+    F[4] = (E + p) * un;
+    if (!star) return;
+    const float a = SK - un;
+    const float ra = rho * a;                 // rho (SK - un)
+    const float factor = ra * rcp_approx(SK - Sstar);
+    const float Estar = E * ir + (Sstar - un) * (Sstar + p * rcp_approx(ra));
+    const float vs[3] = {vx, vy, vz};
+    F[0] += SK * (factor - rho);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float us = (d == DIM - 1) ? factor * Sstar : factor * vs[d];
+        F[1 + d] += SK * (us - rho * vs[d]);
+    }
+    F[4] += SK * (factor * Estar - E);
 }
 
 // Runtime-axis dispatch for the batched face kernel.

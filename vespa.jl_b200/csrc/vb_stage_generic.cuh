@@ -78,8 +78,8 @@ __device__ __forceinline__ void axis_faces(const Geom &g, const double *__restri
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
         const T s = limited_slope<T>(Wlo[k], Wc[k], Whi[k]);
-        fhi[k] = Wc[k] + T(0.5) * s;
-        flo[k] = Wc[k] + T(-0.5) * s;
+        fhi[k] = face_val(Wc[k], T(0.5), s);
+        flo[k] = face_val(Wc[k], T(-0.5), s);
     }
 
     // hi face: (cell, hi neighbour) or the hi domain boundary
@@ -90,13 +90,13 @@ __device__ __forceinline__ void axis_faces(const Geom &g, const double *__restri
         if (nhi2 >= 0) load_prim<T>(g, U, nhi2, Whi2); else ghost_state<T>(Whi, g.bc_hi[AX], AX, Whi2);
         T WR[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) WR[k] = Whi[k] + T(-0.5) * limited_slope<T>(Wc[k], Whi[k], Whi2[k]);
-        hllc_flux<T, AX + 1>(fhi, WR, g.gamma, out.hi);
+        for (int k = 0; k < 5; ++k) WR[k] = face_val(Whi[k], T(-0.5), limited_slope<T>(Wc[k], Whi[k], Whi2[k]));
+        hllc_face<T, AX + 1>(fhi, WR, g.gamma, out.hi);
         out.hi_bnd = false;
     } else {
         T Wg[5];
         ghost_state<T>(fhi, g.bc_hi[AX], AX, Wg);
-        hllc_flux<T, AX + 1>(fhi, Wg, g.gamma, out.hi);
+        hllc_face<T, AX + 1>(fhi, Wg, g.gamma, out.hi);
         out.hi_bnd = true;
     }
 
@@ -108,14 +108,14 @@ __device__ __forceinline__ void axis_faces(const Geom &g, const double *__restri
         if (nlo2 >= 0) load_prim<T>(g, U, nlo2, Wlo2); else ghost_state<T>(Wlo, g.bc_lo[AX], AX, Wlo2);
         T WL[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k) WL[k] = Wlo[k] + T(0.5) * limited_slope<T>(Wlo2[k], Wlo[k], Wc[k]);
-        hllc_flux<T, AX + 1>(WL, flo, g.gamma, out.lo);
+        for (int k = 0; k < 5; ++k) WL[k] = face_val(Wlo[k], T(0.5), limited_slope<T>(Wlo2[k], Wlo[k], Wc[k]));
+        hllc_face<T, AX + 1>(WL, flo, g.gamma, out.lo);
         out.cat = nlo < lin ? LO_BEFORE : (nlo == lin ? LO_SELF : LO_AFTER);
         out.lo_bnd = false;
     } else {
         T Wg[5];
         ghost_state<T>(flo, g.bc_lo[AX], AX, Wg);
-        hllc_flux<T, AX + 1>(Wg, flo, g.gamma, out.lo);
+        hllc_face<T, AX + 1>(Wg, flo, g.gamma, out.lo);
         out.cat = LO_SELF;
         out.lo_bnd = true;
     }

@@ -18,6 +18,8 @@ STATUS_NAMES = {0: "VB_OK", 1: "VB_EINVAL", 2: "VB_ECUDA", 3: "VB_ENOMEM", 4: "V
                 5: "VB_ETIMEOUT", 6: "VB_ENOTSUP"}
 BC_OUTFLOW, BC_PERIODIC, BC_REFLECTING = 0, 1, 2
 FP64, MIXED = 0, 1
+OPT_KERNEL, OPT_TILE_KZ = 1, 2
+KERNELS = {"auto": 0, "cell": 1, "tiled": 2}
 
 
 class VespaB200Error(RuntimeError):
@@ -65,6 +67,8 @@ SIGNATURES = {
     "vb_grid_upload": [_VP, _DP],
     "vb_grid_download": [_VP, _DP],
     "vb_grid_device_state": [_VP, C.POINTER(_VP)],
+    "vb_grid_set_option": [_VP, C.c_int, C.c_int64],
+    "vb_grid_get_option": [_VP, C.c_int, _I64P],
     "vb_grid_set_time": [_VP, C.c_double, C.c_int64],
     "vb_grid_get_time": [_VP, _DP, _I64P],
     "vb_compute_dt": [_VP, _DP],

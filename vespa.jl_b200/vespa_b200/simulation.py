@@ -138,6 +138,19 @@ class Simulation:
     def set_time(self, t: float, step: int = 0) -> None:
         _lib.call("vb_grid_set_time", self.handle, float(t), int(step))
 
+    # -- kernel selection / tuning (results do not depend on these) --
+    def set_kernel(self, kind: str = "auto", kz: Optional[int] = None) -> None:
+        """kind: "auto", "cell" (cell-centric kernel) or "tiled" (tiled 3D kernel)."""
+        _lib.call("vb_grid_set_option", self.handle, _lib.OPT_KERNEL, _lib.KERNELS[kind])
+        if kz is not None:
+            _lib.call("vb_grid_set_option", self.handle, _lib.OPT_TILE_KZ, int(kz))
+
+    @property
+    def kernel(self) -> str:
+        v = C.c_int64()
+        _lib.call("vb_grid_get_option", self.handle, _lib.OPT_KERNEL, C.byref(v))
+        return {1: "cell", 2: "tiled"}[v.value]
+
     def profile_step(self, nsteps: int = 5) -> dict:
         """Mean device milliseconds of each kernel of a CFL step (advances the state)."""
         fin, s1, s2 = C.c_double(), C.c_double(), C.c_double()
