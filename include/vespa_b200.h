@@ -100,6 +100,22 @@ int vb_hllc_faces(vb_ctx *ctx, int64_t nf, const double *WL, const double *WR,
 int vb_hllc_faces_device_async(vb_ctx *ctx, int64_t nf, const double *dWL, const double *dWR,
                                const int32_t *daxis, double gamma, double *dF);
 
+/* No counterpart in the reference.  vb_hllc_faces without any device
+ * allocation, for callers that own all of the GPU's memory (a pool allocator
+ * that must not see foreign cudaMalloc/cudaFree, which synchronise the device
+ * and fragment the pool, or memory reserved up front).  The host arrays are
+ * staged in a fixed array compiled into the library, so at most
+ * VB_NOALLOC_MAX_FACES faces per call (larger nf returns VB_EINVAL); every
+ * GPU that loads the library holds that array (about 7.75 MiB) until exit.
+ * Runs on the calling thread's current device and `stream` (a cudaStream_t,
+ * NULL for the default stream) and returns after the results are in F.
+ * The first call on a device looks up the array's device address; make that
+ * call before any stream capture.  All calls share the array: calls whose
+ * work overlaps on the GPU race and must be serialised by the caller. */
+#define VB_NOALLOC_MAX_FACES 65536
+int vb_hllc_faces_noalloc(int64_t nf, const double *WL, const double *WR, const int32_t *axis,
+                          double gamma, double *F, void *stream);
+
 /* Device-resident uniform grid: Simulation(UniformMesh, prob) state, u0 and
  * stage buffers (src/driver.jl:27-79).  precision is VB_FP64 or VB_MIXED. */
 int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *desc, int precision, vb_grid **out);

@@ -191,6 +191,8 @@ int push_ctrl(vb_grid *gr)
 
 }  // namespace
 
+void vb::set_last_error(const char *msg) { g_err = msg; }
+
 extern "C" {
 
 int vb_abi_version(void) { return VB_ABI_VERSION; }

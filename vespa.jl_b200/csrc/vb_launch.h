@@ -49,4 +49,7 @@ int launch_stage_mixed(const Geom &g, int stage, const double *Uin, const double
 
 constexpr int TOTALS_PARTS = 1024;  // fixed partial count: deterministic sum order
 
+// vb_api.cu: record the calling thread's message for vb_last_error.
+void set_last_error(const char *msg);
+
 }  // namespace vb

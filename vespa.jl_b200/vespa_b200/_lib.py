@@ -61,6 +61,7 @@ SIGNATURES = {
     "vb_ctx_elapsed_ms": [_VP, C.c_int, C.c_int, C.POINTER(C.c_float)],
     "vb_hllc_faces": [_VP, C.c_int64, _DP, _DP, _I32P, C.c_double, _DP],
     "vb_hllc_faces_device_async": [_VP, C.c_int64, _VP, _VP, _VP, C.c_double, _VP],
+    "vb_hllc_faces_noalloc": [C.c_int64, _DP, _DP, _I32P, C.c_double, _DP, _VP],
     "vb_grid_create": [_VP, C.POINTER(ProblemDesc), C.c_int, C.POINTER(_VP)],
     "vb_grid_destroy": [_VP],
     "vb_grid_ncell": [_VP, _I64P],
