@@ -432,7 +432,7 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
             return cleanup(rc, m);
         }
         gr->tiled = true;
-        gr->kz = g.n[2] >= 128 ? 64 : (int)((g.n[2] + 1) / 2);
+        gr->kz = g.n[2] >= 64 ? 32 : (int)((g.n[2] + 1) / 2);
     }
     *out = gr;
     return VB_OK;

@@ -3,7 +3,7 @@
 // accumulation and CFL reduction; float32 reconstruction and HLLC.
 #include "vb_launch.h"
 #include "vb_stage_generic.cuh"
-#include "vb_stage_tiled3d.cuh"
+#include "vb_stage_tiled3d_mixed.cuh"
 
 namespace vb {
 
@@ -26,7 +26,7 @@ int launch_stage_tiled3d_mixed(const TiledMaps &m, const Geom &g, int kz, int st
                                const double *Uin, const double *U0, double *Uout, Ctrl *ctrl,
                                cudaStream_t s)
 {
-    return launch_tiled3d<float, 3>(m, g, kz, stage, Uin, U0, Uout, ctrl, s);
+    return launch_tiled3d_mixed<2>(m, g, kz, stage, Uin, U0, Uout, ctrl, s);
 }
 
 int launch_stage_mixed(const Geom &g, int stage, const double *Uin, const double *U0,

@@ -61,8 +61,8 @@ struct Smem {
     T sx[5][NT], sy[5][NT];   // x / y slopes of the interior cells
     T sxh[5][2 * TY];         // x slopes of the cells just outside x (lx = -1, TX)
     T syh[5][2 * TX];         // y slopes of the cells just outside y (ly = -1, TY)
-    T fx[5][TY * (TX + 1)];   // x-face fluxes, face fx between lx = fx-1 and fx
-    T fy[5][(TY + 1) * TX];   // y-face fluxes
+    double fx[5][TY * (TX + 1)];  // x-face area * flux, face fx between lx = fx-1 and fx
+    double fy[5][(TY + 1) * TX];  // y-face area * flux
     uint64_t bar[NS];
 };
 
@@ -88,6 +88,17 @@ __device__ __forceinline__ int lo_class(int64_t c, int64_t n, bool periodic)
 __device__ __forceinline__ void prefetch_l1(const void *p)
 {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// compute_dt's per-cell term of a new state, exactly as src/driver.jl:178-185
+__device__ __forceinline__ double cfl_term_exact(const double un[5], const Geom &g, double m)
+{
+    double W[5];
+    cons2prim(un, g.gamma, W);
+    const double cs = sound_speed(W, g.gamma);
+    m = nan_max(m, (fabs(W[1]) + cs) / g.w[0]);
+    m = nan_max(m, (fabs(W[2]) + cs) / g.w[1]);
+    return nan_max(m, (fabs(W[3]) + cs) / g.w[2]);
 }
 
 // Persistent: a grid of (2 x SMs) blocks pulls work items (a column tile and a
@@ -243,6 +254,7 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
     const int gx = x0 + tx, gy = y0 + ty;
     const int cx = lo_class(gx, nx, perx), cy = lo_class(gy, ny, pery);
     const int bx_lo = g.bc_lo[0], bx_hi = g.bc_hi[0], by_lo = g.bc_lo[1], by_hi = g.bc_hi[1];
+    double unp[5];  // previous plane's new state: its CFL term is folded one plane later
 
     for (int k = k0; k < k1; ++k) {
         const int q = k - k0 + 4;        // staged index of plane k + 2
@@ -256,6 +268,8 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
             }
         }
         consume(q, Wz2, true);
+        if constexpr (STAGE == 2)
+            if (k > k0) invdt = cfl_term_exact(unp, g, invdt);  // overlaps the cons2prim chain
 #pragma unroll
         for (int f = 0; f < 5; ++f) S.wi[f][t] = Wz0[f];
         __syncthreads();  // (1) plane k primitives complete; stage buffer q consumed
@@ -309,30 +323,30 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
                 }
             }
         }
-        // ---- z face k+1/2 from the own column (registers) ----
+        __syncthreads();  // (2) slopes ready
+
+        // ---- z face k+1/2 from the own column (registers), in the same phase
+        //      as the x/y faces so the independent solves can overlap ----
         T Fzhi[5], hz1[5];
         {
+            T zr[5];  // right state of the z face
             const bool plane_k1 = perz || k + 1 < nz;   // plane k+1 exists
             if (plane_k1) {
                 const bool gh = !perz && k + 2 >= nz;
-                T loz1[5];
 #pragma unroll
                 for (int f = 0; f < 5; ++f) {
                     const T wr = gh ? ((bz_hi == BC_REFLECTING && f == 3) ? -Wz1[f] : Wz1[f]) : Wz2[f];
                     const T s = limited_slope<T>(Wz0[f], Wz1[f], wr);
-                    loz1[f] = face_val(Wz1[f], mhalf, s);
+                    zr[f] = face_val(Wz1[f], mhalf, s);
                     hz1[f] = face_val(Wz1[f], half, s);
                 }
-                tiled_hllc<T, 3>(hz, loz1, gamma, Fzhi);
             } else {
-                T gst[5];
-                ghost_state<T>(hz, bz_hi, 2, gst);
-                tiled_hllc<T, 3>(hz, gst, gamma, Fzhi);
+                ghost_state<T>(hz, bz_hi, 2, zr);
 #pragma unroll
                 for (int f = 0; f < 5; ++f) hz1[f] = hz[f];
             }
+            tiled_hllc<T, 3>(hz, zr, gamma, Fzhi);
         }
-        __syncthreads();  // (2) slopes ready
 
         // ---- x and y faces: each thread its lo faces; 32 threads the hi edges ----
         {
@@ -352,7 +366,7 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
             }
             tiled_hllc<T, 1>(WL, WR, gamma, F);
 #pragma unroll
-            for (int f = 0; f < 5; ++f) S.fx[f][ty * (TX + 1) + tx] = F[f];
+            for (int f = 0; f < 5; ++f) S.fx[f][ty * (TX + 1) + tx] = ax * double(F[f]);
             // y face fy = ty in column tx: between ly = ty-1 and ty
 #pragma unroll
             for (int f = 0; f < 5; ++f) WR[f] = face_val(S.wi[f][t], mhalf, S.sy[f][t]);
@@ -368,7 +382,7 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
             }
             tiled_hllc<T, 2>(WL, WR, gamma, F);
 #pragma unroll
-            for (int f = 0; f < 5; ++f) S.fy[f][ty * TX + tx] = F[f];
+            for (int f = 0; f < 5; ++f) S.fy[f][ty * TX + tx] = ay * double(F[f]);
         }
         if (t >= 224) {
             const int j = t - 224;
@@ -386,7 +400,7 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
                 }
                 tiled_hllc<T, 1>(WL, WR, gamma, F);
 #pragma unroll
-                for (int f = 0; f < 5; ++f) S.fx[f][j * (TX + 1) + TX] = F[f];
+                for (int f = 0; f < 5; ++f) S.fx[f][j * (TX + 1) + TX] = ax * double(F[f]);
             } else {       // y face fy = TY in column i
                 const int i = j - 16;
                 const int c = (TY - 1) * TX + i;
@@ -401,34 +415,41 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
                 }
                 tiled_hllc<T, 2>(WL, WR, gamma, F);
 #pragma unroll
-                for (int f = 0; f < 5; ++f) S.fy[f][TY * TX + i] = F[f];
+                for (int f = 0; f < 5; ++f) S.fy[f][TY * TX + i] = ay * double(F[f]);
             }
         }
         __syncthreads();  // (3) fluxes ready
 
         // ---- flux divergence in the reference's order, then the stage update ----
         const int cz = lo_class(k, nz, perz);
+        const bool interior = cx == LO_BEFORE && cy == LO_BEFORE && cz == LO_BEFORE;
         double un[5];
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
-            const double fxl = double(S.fx[f][ty * (TX + 1) + tx]);
-            const double fxh = double(S.fx[f][ty * (TX + 1) + tx + 1]);
-            const double fyl = double(S.fy[f][ty * TX + tx]);
-            const double fyh = double(S.fy[f][(ty + 1) * TX + tx]);
-            const double fzl = double(Fzlo[f]), fzh = double(Fzhi[f]);
+            // area * flux per face; a lo contribution adds (-area) * F, which is
+            // exactly -(area * F)
+            const double gxl = S.fx[f][ty * (TX + 1) + tx];
+            const double gxh = S.fx[f][ty * (TX + 1) + tx + 1];
+            const double gyl = S.fy[f][ty * TX + tx];
+            const double gyh = S.fy[f][(ty + 1) * TX + tx];
+            const double gzl = az * double(Fzlo[f]), gzh = az * double(Fzhi[f]);
             double a = 0.0;
-            if (cz == LO_BEFORE) a += (-az) * fzl;
-            if (cy == LO_BEFORE) a += (-ay) * fyl;
-            if (cx == LO_BEFORE) a += (-ax) * fxl;
-            a += ax * fxh;
-            if (cx == LO_SELF) a += (-ax) * fxl;
-            a += ay * fyh;
-            if (cy == LO_SELF) a += (-ay) * fyl;
-            a += az * fzh;
-            if (cz == LO_SELF) a += (-az) * fzl;
-            if (cx == LO_AFTER) a += (-ax) * fxl;
-            if (cy == LO_AFTER) a += (-ay) * fyl;
-            if (cz == LO_AFTER) a += (-az) * fzl;
+            if (interior) {
+                a = a - gzl - gyl - gxl + gxh + gyh + gzh;
+            } else {
+                if (cz == LO_BEFORE) a -= gzl;
+                if (cy == LO_BEFORE) a -= gyl;
+                if (cx == LO_BEFORE) a -= gxl;
+                a += gxh;
+                if (cx == LO_SELF) a -= gxl;
+                a += gyh;
+                if (cy == LO_SELF) a -= gyl;
+                a += gzh;
+                if (cz == LO_SELF) a -= gzl;
+                if (cx == LO_AFTER) a -= gxl;
+                if (cy == LO_AFTER) a -= gyl;
+                if (cz == LO_AFTER) a -= gzl;
+            }
             const int64_t i = (int64_t)f * g.ncell + lin;
             if constexpr (STAGE == 1) {
                 un[f] = __ldg(Uin + i) - invV * a;
@@ -437,25 +458,9 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
             }
             Uout[i] = un[f];
         }
-        if constexpr (STAGE == 2 && sizeof(T) == 8) {
-            // compute_dt's term, exactly as src/driver.jl:178-185
-            double W[5];
-            cons2prim(un, gamma, W);
-            const double cs = sound_speed(W, gamma);
-            invdt = nan_max(invdt, (fabs(W[1]) + cs) / g.w[0]);
-            invdt = nan_max(invdt, (fabs(W[2]) + cs) / g.w[1]);
-            invdt = nan_max(invdt, (fabs(W[3]) + cs) / g.w[2]);
-        } else if constexpr (STAGE == 2) {
-            // VB_MIXED: the same float64 CFL term with 1/rho and 1/w reused
-            // (within an ulp of the divisions above)
-            const double inv = 1.0 / un[0];
-            const double vx = un[1] * inv, vy = un[2] * inv, vz = un[3] * inv;
-            const double kin = 0.5 * un[0] * (vx * vx + vy * vy + vz * vz);
-            const double p = fmax((gamma - 1.0) * (un[4] - kin), 1e-12 * kin);
-            const double cs = sqrt(gamma * p * inv);
-            invdt = nan_max(invdt, (fabs(vx) + cs) * g.invw[0]);
-            invdt = nan_max(invdt, (fabs(vy) + cs) * g.invw[1]);
-            invdt = nan_max(invdt, (fabs(vz) + cs) * g.invw[2]);
+        if constexpr (STAGE == 2) {
+#pragma unroll
+            for (int f = 0; f < 5; ++f) unp[f] = un[f];
         }
         // ---- advance the column registers ----
 #pragma unroll
@@ -466,6 +471,7 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
             Fzlo[f] = Fzhi[f];
         }
     }
+    if constexpr (STAGE == 2) invdt = cfl_term_exact(unp, g, invdt);  // the item's last plane
     qb += nplanes;
     }  // work items
 

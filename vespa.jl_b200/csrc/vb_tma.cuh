@@ -84,6 +84,16 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// Per-thread asynchronous 8-byte global -> shared copies (cp.async), waited
+// for by the issuing thread only.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Fast single-precision helpers for the VB_MIXED Riemann solver.
 __device__ __forceinline__ float rcp_approx(float x)
 {
