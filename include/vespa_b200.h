@@ -136,6 +136,14 @@ enum { VB_OPT_KERNEL = 1, VB_OPT_TILE_KZ = 2 };
 enum { VB_KERNEL_AUTO = 0, VB_KERNEL_CELL = 1, VB_KERNEL_TILED = 2 };
 int vb_grid_set_option(vb_grid *grid, int option, int64_t value);
 int vb_grid_get_option(const vb_grid *grid, int option, int64_t *value);
+/* Autotuner (no counterpart in the reference): times the tiled kernel's
+ * z-chunk candidates (16 .. 128 planes) on this grid for nsteps CFL steps
+ * each, keeps the fastest, and restores the state and clock.  The choice is
+ * cached for the process per (device, dims, boundaries, precision) and later
+ * grids of the same kind start from it.  Allocates one state-sized scratch
+ * buffer for the duration of the call.  No-op (returns the current kz) when
+ * the grid uses the cell-centric kernel. */
+int vb_grid_autotune(vb_grid *grid, int nsteps, int64_t *best_kz, double *best_ms_per_step);
 /* Simulation clock (sim.t, sim.step). */
 int vb_grid_set_time(vb_grid *grid, double t, int64_t step);
 int vb_grid_get_time(vb_grid *grid, double *t, int64_t *step);
@@ -158,6 +166,28 @@ int vb_conserved_totals(vb_grid *grid, double out[5]);
  * (dt finalisation, stage 1, stage 2) in milliseconds. */
 int vb_grid_profile_step(vb_grid *grid, int nsteps, double *ms_finalize, double *ms_stage1,
                          double *ms_stage2);
+
+/* Batch of independent uniform 3D problems stepped together (no counterpart
+ * in the reference, which steps one Simulation at a time).  Every box keeps
+ * its own state, clock and CFL dt (the per-box step is evolve!'s, src/driver.jl:
+ * 483-508); one persistent kernel launch per RK2 stage covers the column
+ * tiles of all boxes through one work queue (largest boxes first), and
+ * vb_batch_run_steps replays the steps as a CUDA graph.  Each box must take
+ * the tiled kernel: nx and ny multiples of 16, nz >= 2. */
+typedef struct vb_batch vb_batch;
+int vb_batch_create(vb_ctx *ctx, int nbox, const vb_problem_desc *descs, int precision,
+                    vb_batch **out);
+int vb_batch_destroy(vb_batch *batch);
+/* Cells of box `box`, or of all boxes when box = -1. */
+int vb_batch_ncell(const vb_batch *batch, int box, int64_t *ncell);
+int vb_batch_upload(vb_batch *batch, int box, const double *U);
+int vb_batch_download(vb_batch *batch, int box, double *U);
+/* nsteps CFL-limited SSP-RK2 steps of every box; returns when done. */
+int vb_batch_run_steps(vb_batch *batch, int64_t nsteps);
+/* The same, queued on the context's stream without waiting. */
+int vb_batch_run_steps_async(vb_batch *batch, int64_t nsteps);
+int vb_batch_get_time(vb_batch *batch, int box, double *t, int64_t *step);
+int vb_batch_conserved_totals(vb_batch *batch, int box, double out[5]);
 
 /* Boundary-flux register (BoundaryFluxRegister, src/reflux.jl:113-132): while
  * enabled, every domain-boundary face accumulates (0.5*dt*F)*area per RK2

@@ -234,6 +234,25 @@ def test_tiled_kernel_bit_identical_to_oracle(vb, oracle, dims, bclo, bchi, kz):
     assert_bit_identical(sim.state(), U)
 
 
+def test_autotune_restores_state_and_keeps_results(vb):
+    prob = P.smooth_random_problem((64, 48, 80), seed=31)
+    U0 = P.initial_state(prob)
+    a = make_sim(prob, U0)
+    kz, ms = a.autotune(nsteps=2)
+    assert kz in (16, 24, 32, 48, 64) and ms > 0
+    assert a.kz == kz
+    assert a.step == 0 and a.t == 0.0
+    assert_bit_identical(a.state(), U0)
+    # the chunking changes the schedule, never the float64 result
+    b = make_sim(prob, U0)
+    b.set_kernel("tiled", kz=7)
+    vb.evolve(a, tfinal=math.inf, max_steps=4)
+    vb.evolve(b, tfinal=math.inf, max_steps=4)
+    assert_bit_identical(a.state(), b.state())
+    c = make_sim(prob, U0)  # a new grid of the same kind starts from the tuned kz
+    assert c.kz == kz
+
+
 def test_tiled_equals_cell_kernel_on_sharp_data(vb):
     """A strong planar discontinuity (all HLLC branches, both star sides) on
     outflow walls: tiled and cell-centric float64 kernels agree to the bit."""

@@ -8,20 +8,15 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 
-#include "../../include/vespa_b200.h"
-#include "vb_launch.h"
+#include "vb_internal.h"
 
-struct vb_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int64_t launches = 0;
-    void *scratch = nullptr;  // vb_hllc_faces staging (device)
-    size_t scratch_bytes = 0;
-    cudaEvent_t marks[16] = {};
-};
+using vb::detail::fail;
+using vb::detail::use;
 
 struct vb_grid {
     vb_ctx *ctx = nullptr;
@@ -41,11 +36,16 @@ struct vb_grid {
     bool tiled = false;         // the tiled 3D kernels apply to this grid
     int kz = 64;                // z planes per tiled work item
     vb::TiledMaps maps_U{}, maps_U1{};  // TMA descriptors of the two stage inputs
+    vb::BoxDesc box{};                  // the tiled kernels' box descriptor (passed by value)
+    int box_kz = 0;                     // kz the descriptor was written with
 };
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
+
+namespace vb {
+namespace detail {
 
 int fail(int code, const std::string &msg)
 {
@@ -53,30 +53,17 @@ int fail(int code, const std::string &msg)
     return code;
 }
 
-#define VB_CUDA(call)                                                                      \
-    do {                                                                                   \
-        cudaError_t e_ = (call);                                                           \
-        if (e_ != cudaSuccess)                                                             \
-            return fail(e_ == cudaErrorMemoryAllocation ? VB_ENOMEM : VB_ECUDA,            \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
-    } while (0)
-
-#define VB_CHECK_LAUNCH(ctx, n)                                                            \
-    do {                                                                                   \
-        int n_ = (n);                                                                      \
-        if (n_ < 0) return fail(VB_EINVAL, "invalid launch configuration");               \
-        (ctx)->launches += n_;                                                             \
-        cudaError_t e_ = cudaGetLastError();                                               \
-        if (e_ != cudaSuccess)                                                             \
-            return fail(VB_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
-    } while (0)
-
 int use(vb_ctx *ctx)
 {
     if (!ctx) return fail(VB_EINVAL, "null context");
     VB_CUDA(cudaSetDevice(ctx->device));
     return VB_OK;
 }
+
+}  // namespace detail
+}  // namespace vb
+
+namespace {
 
 // cuTensorMapEncodeTiled through the runtime's driver entry-point lookup (no
 // link-time dependency on libcuda).
@@ -114,6 +101,24 @@ int encode_state_map(CUtensorMap *m, const double *base, const vb::Geom &g, uint
     return VB_OK;
 }
 
+// Autotuned z-chunk per (device, dims, boundaries, precision), process-wide.
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune_kz;
+
+std::string tune_key(int device, const vb::Geom &g, int precision)
+{
+    std::string k = std::to_string(device) + ":" + std::to_string(precision);
+    for (int a = 0; a < 3; ++a)
+        k += ":" + std::to_string(g.n[a]) + "/" + std::to_string(g.bc_lo[a]) +
+             std::to_string(g.bc_hi[a]);
+    return k;
+}
+
+}  // namespace
+
+namespace vb {
+namespace detail {
+
 int encode_maps(vb::TiledMaps *m, const double *base, const vb::Geom &g)
 {
     int rc = encode_state_map(&m->in_int, base, g, 16, 16);
@@ -122,16 +127,123 @@ int encode_maps(vb::TiledMaps *m, const double *base, const vb::Geom &g)
     return rc;
 }
 
+int default_kz(const vb::Geom &g) { return g.n[2] >= 64 ? 32 : (int)((g.n[2] + 1) / 2); }
+
+// Geometry of a descriptor, validated as Problem is (src/problem.jl:39-46),
+// and RefMesh's derived widths, areas and volume (lib/RefMesh/src/RefMesh.jl:
+// 122-142).
+int make_geom(const vb_problem_desc *d, vb::Geom *out)
+{
+    if (!d) return fail(VB_EINVAL, "null problem descriptor");
+    if (d->ndim < 1 || d->ndim > 3) return fail(VB_EINVAL, "ndim must be 1, 2 or 3");
+    if (!(d->gamma > 1.0)) return fail(VB_EINVAL, "gamma must exceed 1");
+    if (!(d->cfl > 0.0 && d->cfl <= 1.0)) return fail(VB_EINVAL, "cfl must be in (0, 1]");
+    if (!(d->aexp > 0.0)) return fail(VB_EINVAL, "aexp must be positive");
+    if (d->flags != 0) return fail(VB_EINVAL, "flags must be 0");
+    vb::Geom g{};
+    g.nd = d->ndim;
+    int64_t s = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (a < d->ndim) {
+            if (d->dims[a] < 1) return fail(VB_EINVAL, "all dims must be positive");
+            if (!(d->hi[a] > d->lo[a])) return fail(VB_EINVAL, "domain must have hi > lo");
+            for (int side = 0; side < 2; ++side) {
+                int bc = side ? d->bc_hi[a] : d->bc_lo[a];
+                if (bc < VB_BC_OUTFLOW || bc > VB_BC_REFLECTING)
+                    return fail(VB_EINVAL, "unknown boundary condition");
+            }
+            if ((d->bc_lo[a] == VB_BC_PERIODIC) != (d->bc_hi[a] == VB_BC_PERIODIC))
+                return fail(VB_EINVAL, "a periodic axis must be periodic on both sides");
+            g.n[a] = d->dims[a];
+            g.bc_lo[a] = d->bc_lo[a];
+            g.bc_hi[a] = d->bc_hi[a];
+        } else {
+            g.n[a] = 1;
+            g.bc_lo[a] = g.bc_hi[a] = VB_BC_PERIODIC;
+        }
+        g.stride[a] = s;
+        if (s > INT64_MAX / g.n[a]) return fail(VB_EINVAL, "cell count overflows");
+        s *= g.n[a];
+    }
+    g.ncell = s;
+    for (int a = 0; a < g.nd; ++a) g.w[a] = (d->hi[a] - d->lo[a]) / (double)d->dims[a];
+    for (int a = 0; a < 3; ++a) g.invw[a] = a < g.nd ? 1.0 / g.w[a] : 0.0;
+    for (int a = 0; a < g.nd; ++a) {
+        double ar = 1.0;
+        for (int e = 0; e < g.nd; ++e)
+            if (e != a) ar *= g.w[e];
+        g.area[a] = ar;
+    }
+    double v = g.w[0];
+    for (int a = 1; a < g.nd; ++a) v = v * g.w[a];
+    g.vol = v;
+    g.gamma = d->gamma;
+    g.cfl = d->cfl;
+    g.aexp = d->aexp;
+    *out = g;
+    return VB_OK;
+}
+
+// Box-table entry of a tiled grid (host side).
+vb::BoxDesc make_box(const vb::TiledMaps &mU, const vb::TiledMaps &mU1, const vb::Geom &g,
+                     double *U, double *U1, vb::Ctrl *ctrl, int kz, int item0)
+{
+    vb::BoxDesc b;
+    std::memset(&b, 0, sizeof b);
+    b.map[0][0] = mU.in_int;
+    b.map[0][1] = mU.in_xs;
+    b.map[0][2] = mU.in_ys;
+    b.map[1][0] = mU1.in_int;
+    b.map[1][1] = mU1.in_xs;
+    b.map[1][2] = mU1.in_ys;
+    b.g = g;
+    b.U = U;
+    b.U1 = U1;
+    b.ctrl = ctrl;
+    b.kz = kz;
+    b.ntx = (int)(g.n[0] / 16);
+    b.ntiles = (int)((g.n[0] / 16) * (g.n[1] / 16));
+    b.item0 = item0;
+    return b;
+}
+
+int64_t box_items(const vb::Geom &g, int kz)
+{
+    return (g.n[0] / 16) * (g.n[1] / 16) * ((g.n[2] + kz - 1) / kz);
+}
+
+}  // namespace detail
+}  // namespace vb
+
+namespace {
+
+using vb::detail::box_items;
+using vb::detail::encode_maps;
+using vb::detail::make_box;
+
+// Refresh the grid's box descriptor after kz (or the maps) changed.
+int sync_box(vb_grid *gr)
+{
+    if (gr->box_kz == gr->kz) return VB_OK;
+    gr->box = make_box(gr->maps_U, gr->maps_U1, gr->g, gr->U, gr->U1, gr->ctrl, gr->kz, 0);
+    gr->box_kz = gr->kz;
+    return VB_OK;
+}
+
 int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout)
 {
     double *bf = gr->bflux_on ? gr->bflux : nullptr;
     if (gr->tiled && !bf) {
-        const vb::TiledMaps &m = (Uin == gr->U) ? gr->maps_U : gr->maps_U1;
+        int rc = sync_box(gr);
+        if (rc) return rc;
+        const int64_t items = box_items(gr->g, gr->kz);
+        if (items > 0x7fffffff) return fail(VB_ENOTSUP, "too many tiled work items");
+        unsigned int *work = gr->ctrl->work;  // device address of the cursors
         int n = gr->precision == VB_MIXED
-                    ? vb::launch_stage_tiled3d_mixed(m, gr->g, gr->kz, st, Uin, U0, Uout, gr->ctrl,
-                                                     gr->ctx->stream)
-                    : vb::launch_stage_tiled3d_fp64(m, gr->g, gr->kz, st, Uin, U0, Uout, gr->ctrl,
-                                                    gr->ctx->stream);
+                    ? vb::launch_stage_tiled3d_mixed(&gr->box, nullptr, nullptr, (int)items, work,
+                                                     st, gr->ctx->stream)
+                    : vb::launch_stage_tiled3d_fp64(&gr->box, nullptr, nullptr, (int)items, work,
+                                                    st, gr->ctx->stream);
         VB_CHECK_LAUNCH(gr->ctx, n);
         return VB_OK;
     }
@@ -149,6 +261,7 @@ int rk2(vb_grid *gr)
     if (rc) return rc;
     rc = stage(gr, 2, gr->U1, gr->U, gr->U);
     if (rc) return rc;
+    VB_CHECK_LAUNCH(gr->ctx, vb::launch_advance(gr->ctrl, gr->ctx->stream));
     gr->invdt_valid = true;
     return VB_OK;
 }
@@ -344,55 +457,10 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
     *out = nullptr;
     int rc = use(ctx);
     if (rc) return rc;
-    if (!d) return fail(VB_EINVAL, "null problem descriptor");
-    if (d->ndim < 1 || d->ndim > 3) return fail(VB_EINVAL, "ndim must be 1, 2 or 3");
     if (precision != VB_FP64 && precision != VB_MIXED) return fail(VB_EINVAL, "unknown precision");
-    // Problem validation, src/problem.jl:39-46
-    if (!(d->gamma > 1.0)) return fail(VB_EINVAL, "gamma must exceed 1");
-    if (!(d->cfl > 0.0 && d->cfl <= 1.0)) return fail(VB_EINVAL, "cfl must be in (0, 1]");
-    if (!(d->aexp > 0.0)) return fail(VB_EINVAL, "aexp must be positive");
-    if (d->flags != 0) return fail(VB_EINVAL, "flags must be 0");
     vb::Geom g{};
-    g.nd = d->ndim;
-    int64_t s = 1;
-    for (int a = 0; a < 3; ++a) {
-        if (a < d->ndim) {
-            if (d->dims[a] < 1) return fail(VB_EINVAL, "all dims must be positive");
-            if (!(d->hi[a] > d->lo[a])) return fail(VB_EINVAL, "domain must have hi > lo");
-            for (int side = 0; side < 2; ++side) {
-                int bc = side ? d->bc_hi[a] : d->bc_lo[a];
-                if (bc < VB_BC_OUTFLOW || bc > VB_BC_REFLECTING)
-                    return fail(VB_EINVAL, "unknown boundary condition");
-            }
-            if ((d->bc_lo[a] == VB_BC_PERIODIC) != (d->bc_hi[a] == VB_BC_PERIODIC))
-                return fail(VB_EINVAL, "a periodic axis must be periodic on both sides");
-            g.n[a] = d->dims[a];
-            g.bc_lo[a] = d->bc_lo[a];
-            g.bc_hi[a] = d->bc_hi[a];
-        } else {
-            g.n[a] = 1;
-            g.bc_lo[a] = g.bc_hi[a] = VB_BC_PERIODIC;
-        }
-        g.stride[a] = s;
-        if (s > INT64_MAX / g.n[a]) return fail(VB_EINVAL, "cell count overflows");
-        s *= g.n[a];
-    }
-    g.ncell = s;
-    // _width, face_area, cell_volume (lib/RefMesh/src/RefMesh.jl:122-142)
-    for (int a = 0; a < g.nd; ++a) g.w[a] = (d->hi[a] - d->lo[a]) / (double)d->dims[a];
-    for (int a = 0; a < 3; ++a) g.invw[a] = a < g.nd ? 1.0 / g.w[a] : 0.0;
-    for (int a = 0; a < g.nd; ++a) {
-        double ar = 1.0;
-        for (int e = 0; e < g.nd; ++e)
-            if (e != a) ar *= g.w[e];
-        g.area[a] = ar;
-    }
-    double v = g.w[0];
-    for (int a = 1; a < g.nd; ++a) v = v * g.w[a];
-    g.vol = v;
-    g.gamma = d->gamma;
-    g.cfl = d->cfl;
-    g.aexp = d->aexp;
+    rc = vb::detail::make_geom(d, &g);
+    if (rc) return rc;
 
     vb_grid *gr = new (std::nothrow) vb_grid();
     if (!gr) return fail(VB_ENOMEM, "host allocation failed");
@@ -432,9 +500,76 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
             return cleanup(rc, m);
         }
         gr->tiled = true;
-        gr->kz = g.n[2] >= 64 ? 32 : (int)((g.n[2] + 1) / 2);
+        gr->kz = vb::detail::default_kz(g);
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_kz.find(tune_key(ctx->device, g, precision));
+        if (it != g_tune_kz.end()) gr->kz = it->second;
     }
     *out = gr;
+    return VB_OK;
+}
+
+int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
+{
+    if (!gr || nsteps < 1) return fail(VB_EINVAL, "bad argument");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    if (!gr->tiled || gr->bflux_on) {
+        if (best_kz) *best_kz = gr->kz;
+        if (best_ms) *best_ms = 0.0;
+        return VB_OK;
+    }
+    const size_t bytes = sizeof(double) * 5 * (size_t)gr->g.ncell;
+    double *save = nullptr;
+    VB_CUDA(cudaMalloc(&save, bytes));
+    cudaStream_t s = gr->ctx->stream;
+    rc = pull_ctrl(gr);
+    vb::Ctrl ctrl0 = *gr->hctrl;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int best = gr->kz;
+    float best_t = INFINITY;
+    if (!rc && (cudaMemcpyAsync(save, gr->U, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+                cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = fail(VB_ECUDA, "autotune setup failed");
+    const int cand[] = {16, 24, 32, 48, 64, 96, 128};
+    for (int kz : cand) {
+        if (rc) break;
+        if (kz > gr->g.n[2]) continue;
+        gr->kz = kz;
+        rc = ensure_cfl(gr);
+        if (!rc) rc = queue_steps(gr, 1);  // warm-up
+        if (rc) break;
+        cudaEventRecord(e0, s);
+        rc = queue_steps(gr, nsteps);
+        cudaEventRecord(e1, s);
+        if (rc) break;
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = fail(VB_ECUDA, "autotune timing failed");
+            break;
+        }
+        if (ms < best_t) {
+            best_t = ms;
+            best = kz;
+        }
+    }
+    // restore the state and the clock whatever happened
+    cudaMemcpyAsync(gr->U, save, bytes, cudaMemcpyDeviceToDevice, s);
+    *gr->hctrl = ctrl0;
+    int rc2 = push_ctrl(gr);
+    cudaFree(save);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    gr->invdt_valid = false;
+    gr->kz = best;
+    if (rc) return rc;
+    if (rc2) return rc2;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_kz[tune_key(gr->ctx->device, gr->g, gr->precision)] = best;
+    }
+    if (best_kz) *best_kz = best;
+    if (best_ms) *best_ms = best_t / nsteps;
     return VB_OK;
 }
 

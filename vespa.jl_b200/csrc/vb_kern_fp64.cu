@@ -158,11 +158,83 @@ int launch_stage_fp64(const Geom &g, int stage, const double *Uin, const double 
     }
 }
 
-int launch_stage_tiled3d_fp64(const TiledMaps &m, const Geom &g, int kz, int stage,
-                              const double *Uin, const double *U0, double *Uout, Ctrl *ctrl,
-                              cudaStream_t s)
+int launch_stage_tiled3d_fp64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
+                              int nitems, unsigned int *work, int stage, cudaStream_t s)
 {
-    return launch_tiled3d<double, 2>(m, g, kz, stage, Uin, U0, Uout, ctrl, s);
+    return launch_tiled3d<double, 2>(hbox, boxes, item_box, nitems, work, stage, s);
+}
+
+namespace {
+
+// evolve!'s loop head for every box of a table (one thread per box); thread 0
+// of block 0 also rewinds the shared work cursors.
+__global__ void k_finalize_boxes(const BoxDesc *boxes, int nbox, unsigned int *work)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b == 0) work[0] = work[1] = 0u;
+    if (b >= nbox) return;
+    const Geom &g = boxes[b].g;
+    Ctrl *ctrl = boxes[b].ctrl;
+    const double t = ctrl->t;
+    if (!(t < ctrl->tfinal * (1.0 - 1e-12)) || ctrl->step >= ctrl->step_limit) {
+        ctrl->active = 0;
+        return;
+    }
+    const double invdt = __longlong_as_double((long long)ctrl->invdt_bits);
+    double dt = (invdt == 0.0) ? (double)INFINITY : g.cfl / invdt;
+    dt = fmin(dt, ctrl->tfinal - t);
+    if (invdt != invdt || !(dt < (double)INFINITY)) {
+        ctrl->flags |= CTRL_F_NONFINITE;
+        ctrl->active = 0;
+        return;
+    }
+    ctrl->dt = dt;
+    ctrl->invV = dt / (g.aexp * g.vol);
+    ctrl->active = 1;
+    ctrl->invdt_bits = 0ull;
+    ctrl->work[0] = ctrl->work[1] = 0u;
+}
+
+// step!'s clock advance (src/driver.jl:353-356) after stage 2.
+__global__ void k_advance_boxes(const BoxDesc *boxes, int nbox)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nbox) return;
+    Ctrl *ctrl = boxes[b].ctrl;
+    if (ctrl->active) {
+        ctrl->t = ctrl->t + ctrl->dt;
+        ctrl->step = ctrl->step + 1;
+    }
+}
+
+__global__ void k_advance(Ctrl *ctrl)
+{
+    if (ctrl->active) {
+        ctrl->t = ctrl->t + ctrl->dt;
+        ctrl->step = ctrl->step + 1;
+    }
+}
+
+}  // namespace
+
+int launch_finalize_boxes(const BoxDesc *boxes, int nbox, unsigned int *work, cudaStream_t s)
+{
+    if (nbox <= 0) return -1;
+    k_finalize_boxes<<<(nbox + 127) / 128, 128, 0, s>>>(boxes, nbox, work);
+    return 1;
+}
+
+int launch_advance_boxes(const BoxDesc *boxes, int nbox, cudaStream_t s)
+{
+    if (nbox <= 0) return -1;
+    k_advance_boxes<<<(nbox + 127) / 128, 128, 0, s>>>(boxes, nbox);
+    return 1;
+}
+
+int launch_advance(Ctrl *ctrl, cudaStream_t s)
+{
+    k_advance<<<1, 1, 0, s>>>(ctrl);
+    return 1;
 }
 
 static unsigned grid_for(int64_t n, int bs, int maxb)

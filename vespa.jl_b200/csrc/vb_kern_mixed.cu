@@ -22,11 +22,10 @@ int launch_generic(const Geom &g, const double *Uin, const double *U0, double *U
 
 }  // namespace
 
-int launch_stage_tiled3d_mixed(const TiledMaps &m, const Geom &g, int kz, int stage,
-                               const double *Uin, const double *U0, double *Uout, Ctrl *ctrl,
-                               cudaStream_t s)
+int launch_stage_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
+                               int nitems, unsigned int *work, int stage, cudaStream_t s)
 {
-    return launch_tiled3d_mixed<2>(m, g, kz, stage, Uin, U0, Uout, ctrl, s);
+    return launch_tiled3d_mixed<2>(hbox, boxes, item_box, nitems, work, stage, s);
 }
 
 int launch_stage_mixed(const Geom &g, int stage, const double *Uin, const double *U0,

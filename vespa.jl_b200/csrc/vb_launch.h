@@ -17,6 +17,21 @@ struct TiledMaps {
     CUtensorMap in_int, in_xs, in_ys;
 };
 
+// One box of a tiled launch, in device memory: the tensor maps of its two
+// stage inputs, its geometry, state buffers and control block, and where its
+// work items start in the launch's global item numbering.  A single grid is a
+// one-box table; a batch of independent problems is a table of many.
+struct alignas(64) BoxDesc {
+    CUtensorMap map[2][3];  // [stage-1 input U, stage-2 input U1][interior, x strip, y strip]
+    Geom g;
+    double *U, *U1;
+    Ctrl *ctrl;
+    int kz;       // z planes per work item
+    int ntx;      // column tiles along x
+    int ntiles;   // column tiles per plane
+    int item0;    // first global work item of this box
+};
+
 // Tiled 3D path applicability: 16 x 16 column tiles, at least two planes,
 // periodic axes periodic on both sides (checked at grid creation).
 inline bool tiled3d_supported(const Geom &g)
@@ -36,14 +51,20 @@ int launch_totals(const Geom &g, const double *U, double *partials, int npart, d
 int launch_hllc_faces(int64_t nf, const double *WL, const double *WR, const int32_t *axis,
                       double gamma, double *F, cudaStream_t s);
 
-int launch_stage_tiled3d_fp64(const TiledMaps &m, const Geom &g, int kz, int stage,
-                              const double *Uin, const double *U0, double *Uout, Ctrl *ctrl,
-                              cudaStream_t s);
+// Tiled stage.  hbox (host pointer) set: a single box passed by value; else a
+// device box table `boxes` with `item_box` mapping each global work item to
+// its box.  `work` holds the two stage cursors (reset by the dt kernels).
+int launch_stage_tiled3d_fp64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
+                              int nitems, unsigned int *work, int stage, cudaStream_t s);
+// Per-box dt finalisation (evolve!'s loop head) and clock advance for a table.
+int launch_finalize_boxes(const BoxDesc *boxes, int nbox, unsigned int *work, cudaStream_t s);
+int launch_advance_boxes(const BoxDesc *boxes, int nbox, cudaStream_t s);
+// Clock advance of a single control block (t += dt, step += 1 while active).
+int launch_advance(Ctrl *ctrl, cudaStream_t s);
 
 // vb_kern_mixed.cu
-int launch_stage_tiled3d_mixed(const TiledMaps &m, const Geom &g, int kz, int stage,
-                               const double *Uin, const double *U0, double *Uout, Ctrl *ctrl,
-                               cudaStream_t s);
+int launch_stage_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
+                               int nitems, unsigned int *work, int stage, cudaStream_t s);
 int launch_stage_mixed(const Geom &g, int stage, const double *Uin, const double *U0,
                        double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s);
 

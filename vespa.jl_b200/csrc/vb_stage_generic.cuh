@@ -220,13 +220,7 @@ k_stage_generic(Geom g, const double *__restrict__ Uin, const double *U0, double
             for (int d = 0; d < ND; ++d) invdt = nan_max(invdt, (fabs(W[1 + d]) + cs) / g.w[d]);
         }
     }
-    if constexpr (STAGE == 2) {
-        block_max_to(&ctrl->invdt_bits, invdt, red);
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            ctrl->t = ctrl->t + ctrl->dt;
-            ctrl->step = ctrl->step + 1;
-        }
-    }
+    if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);
 }
 
 }  // namespace vb

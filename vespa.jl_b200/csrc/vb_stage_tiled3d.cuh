@@ -18,6 +18,8 @@
 // done here (the cell-centric kernel handles grids with bflux enabled).
 #pragma once
 
+#include <cstring>
+
 #include "vb_launch.h"
 #include "vb_stage_generic.cuh"
 
@@ -101,15 +103,28 @@ __device__ __forceinline__ double cfl_term_exact(const double un[5], const Geom 
     return nan_max(m, (fabs(W[3]) + cs) / g.w[2]);
 }
 
-// Persistent: a grid of (2 x SMs) blocks pulls work items (a column tile and a
-// z chunk; item = chunk * ntiles + tile, so concurrently processed items are
-// spatial neighbours and share halo planes in L2) from ctrl->work[STAGE-1].
-template <typename T, int NS, int STAGE>
+// Persistent: a grid of (2 x SMs) blocks pulls work items from work[STAGE-1].
+// An item is a column tile and a z chunk of one box (within a box, item =
+// chunk * ntiles + tile, so concurrently processed items are spatial
+// neighbours and share halo planes in L2).
+//
+// BATCH = false: one box, passed by value as a kernel parameter (its geometry
+// and tensor maps are then read from the constant bank); BATCH = true: the box
+// of each item is looked up in the device table.
+template <bool BATCH>
+__device__ __forceinline__ const BoxDesc &box_of(const BoxDesc &box0, const BoxDesc *boxes,
+                                                 const int *item_box, int item)
+{
+    if constexpr (BATCH)
+        return boxes[item_box[item]];
+    else
+        return box0;
+}
+
+template <typename T, int NS, int STAGE, bool BATCH>
 __global__ void __launch_bounds__(256, 2)
-k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
-                const __grid_constant__ CUtensorMap tm_xs,
-                const __grid_constant__ CUtensorMap tm_ys, Geom g, int kz, int nitems,
-                const double *__restrict__ Uin, const double *U0, double *Uout, Ctrl *ctrl)
+k_stage_tiled3d(const __grid_constant__ BoxDesc box0, const BoxDesc *__restrict__ boxes,
+                const int *__restrict__ item_box, int nitems, unsigned int *work)
 {
     using namespace t3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -117,16 +132,8 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
     __shared__ double red[32];
     __shared__ int item_sh;
 
-    if (!ctrl->active) return;
     const int t = threadIdx.x;
     const int tx = t & (TX - 1), ty = t >> 4;
-    const int ntx = (int)(g.n[0] / TX);
-    const int ntiles = ntx * (int)(g.n[1] / TY);
-    const int nx = (int)g.n[0], ny = (int)g.n[1], nz = (int)g.n[2];
-    const bool perx = g.bc_lo[0] == BC_PERIODIC, pery = g.bc_lo[1] == BC_PERIODIC;
-    const bool perz = g.bc_lo[2] == BC_PERIODIC;
-    const double gamma = g.gamma;
-    const double invV = ctrl->invV;
 
     if (t == 0) {
         for (int s = 0; s < NS; ++s) mbar_init(&S.bar[s], 1);
@@ -135,16 +142,34 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
     __syncthreads();
 
     bool timed_out = false;
-    double invdt = 0.0;
     int qb = 0;  // staged planes this block consumed before the current item
     for (;;) {
-    if (t == 0) item_sh = (int)atomicAdd(&ctrl->work[STAGE - 1], 1u);
+    if (t == 0) item_sh = (int)atomicAdd(&work[STAGE - 1], 1u);
     __syncthreads();
     const int item = item_sh;  // rewritten only after this item's barriers
     if (item >= nitems) break;
-    const int tile = item % ntiles;
+    const BoxDesc &B = box_of<BATCH>(box0, boxes, item_box, item);
+    Ctrl *ctrl = B.ctrl;
+    if (!ctrl->active) {  // uniform: the box is not stepping
+        __syncthreads();  // everyone has read item_sh before thread 0 rewrites it
+        continue;
+    }
+    const Geom &g = B.g;
+    const CUtensorMap *tm = B.map[STAGE - 1];
+    const double *__restrict__ Uin = STAGE == 1 ? B.U : B.U1;
+    const double *U0 = B.U;
+    double *Uout = STAGE == 1 ? B.U1 : B.U;
+    const int kz = B.kz, ntx = B.ntx, ntiles = B.ntiles;
+    const int nx = (int)g.n[0], ny = (int)g.n[1], nz = (int)g.n[2];
+    const bool perx = g.bc_lo[0] == BC_PERIODIC, pery = g.bc_lo[1] == BC_PERIODIC;
+    const bool perz = g.bc_lo[2] == BC_PERIODIC;
+    const double gamma = g.gamma;
+    const double invV = ctrl->invV;
+    double invdt = 0.0;
+    const int local = item - B.item0;
+    const int tile = local % ntiles;
     const int x0 = (tile % ntx) * TX, y0 = (tile / ntx) * TY;
-    const int k0 = (item / ntiles) * kz;
+    const int k0 = (local / ntiles) * kz;
     const int k1 = min(nz, k0 + kz);
     const int nplanes = (k1 - k0) + 4;  // planes k0-2 .. k1+1
     // tile edges that are domain boundaries (ghost states instead of halo data)
@@ -161,11 +186,11 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
         const int yl = (pery && y0 == 0) ? ny - 2 : y0 - 2;
         const int yh = (pery && y0 + TY == ny) ? 0 : y0 + TY;
         mbar_expect_tx(bar, PLANE_BYTES);
-        tma_load_4d(dst, &tm_int, x0, y0, z, 0, bar);
-        tma_load_4d(dst + U_XLO, &tm_xs, xl, y0, z, 0, bar);
-        tma_load_4d(dst + U_XHI, &tm_xs, xh, y0, z, 0, bar);
-        tma_load_4d(dst + U_YLO, &tm_ys, x0, yl, z, 0, bar);
-        tma_load_4d(dst + U_YHI, &tm_ys, x0, yh, z, 0, bar);
+        tma_load_4d(dst, &tm[0], x0, y0, z, 0, bar);
+        tma_load_4d(dst + U_XLO, &tm[1], xl, y0, z, 0, bar);
+        tma_load_4d(dst + U_XHI, &tm[1], xh, y0, z, 0, bar);
+        tma_load_4d(dst + U_YLO, &tm[2], x0, yl, z, 0, bar);
+        tma_load_4d(dst + U_YHI, &tm[2], x0, yh, z, 0, bar);
     };
     if (t == 0) {
         fence_proxy_async_smem();  // the previous item read these buffers
@@ -473,58 +498,61 @@ k_stage_tiled3d(const __grid_constant__ CUtensorMap tm_int,
     }
     if constexpr (STAGE == 2) invdt = cfl_term_exact(unp, g, invdt);  // the item's last plane
     qb += nplanes;
+    if (timed_out && t == 0) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
+    if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);  // this box's CFL max
     }  // work items
-
-    if (timed_out) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
-    if constexpr (STAGE == 2) {
-        block_max_to(&ctrl->invdt_bits, invdt, red);
-        if (blockIdx.x == 0 && t == 0) {
-            ctrl->t = ctrl->t + ctrl->dt;
-            ctrl->step = ctrl->step + 1;
-        }
-    }
 }
 
 }  // namespace vb
 
 namespace vb {
 
+// Resident blocks of a persistent kernel on the current device (all SMs), with
+// its dynamic shared memory opted in once.
+template <typename K>
+int persistent_blocks(K kernel1, K kernel2, size_t smem)
+{
+    if (cudaFuncSetAttribute(kernel1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(kernel2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+        return -1;
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel2, t3::NT, smem) != cudaSuccess ||
+        per_sm < 1)
+        return -1;
+    return sms * per_sm;
+}
+
 // Host-side launch of the persistent tiled 3D stage kernel: as many blocks as
-// can be resident (occupancy query), pulling (tile, z-chunk) items.
+// can be resident, pulling (box, tile, z-chunk) items.  hbox (host) set: one
+// box passed by value; else the device table `boxes` with `item_box`.
 template <typename T, int NS>
-int launch_tiled3d(const TiledMaps &m, const Geom &g, int kz, int stage, const double *Uin,
-                   const double *U0, double *Uout, Ctrl *ctrl, cudaStream_t s)
+int launch_tiled3d(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box, int nitems,
+                   unsigned int *work, int stage, cudaStream_t s)
 {
     const size_t smem = sizeof(t3::Smem<T, NS>);
-    static int resident = 0;  // blocks resident per device (all SMs)
-    if (!resident) {
-        if (cudaFuncSetAttribute(k_stage_tiled3d<T, NS, 1>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-            cudaFuncSetAttribute(k_stage_tiled3d<T, NS, 2>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return -1;
-        int dev = 0, sms = 0, per_sm = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_tiled3d<T, NS, 2>,
-                                                          t3::NT, smem) != cudaSuccess ||
-            per_sm < 1)
-            return -1;
-        resident = sms * per_sm;
-    }
-    if (kz <= 0) return -1;
-    const int ntiles = (int)((g.n[0] / t3::TX) * (g.n[1] / t3::TY));
-    const int nchunks = (int)((g.n[2] + kz - 1) / kz);
-    const int64_t items = (int64_t)ntiles * nchunks;
-    if (items > 0x7fffffff) return -1;
-    const int nitems = (int)items;
+    static int res1 = 0, resb = 0;
+    if (!res1) res1 = persistent_blocks(k_stage_tiled3d<T, NS, 1, false>,
+                                        k_stage_tiled3d<T, NS, 2, false>, smem);
+    if (!resb) resb = persistent_blocks(k_stage_tiled3d<T, NS, 1, true>,
+                                        k_stage_tiled3d<T, NS, 2, true>, smem);
+    const int resident = hbox ? res1 : resb;
+    if (resident <= 0 || nitems <= 0) return -1;
     const unsigned grid = (unsigned)(nitems < resident ? nitems : resident);
-    if (stage == 1)
-        k_stage_tiled3d<T, NS, 1><<<grid, t3::NT, smem, s>>>(m.in_int, m.in_xs, m.in_ys, g, kz,
-                                                             nitems, Uin, U0, Uout, ctrl);
+    BoxDesc box0;
+    if (hbox) box0 = *hbox;
+    else std::memset(&box0, 0, sizeof box0);
+    if (hbox && stage == 1)
+        k_stage_tiled3d<T, NS, 1, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (hbox)
+        k_stage_tiled3d<T, NS, 2, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (stage == 1)
+        k_stage_tiled3d<T, NS, 1, true><<<grid, t3::NT, smem, s>>>(box0, boxes, item_box, nitems, work);
     else
-        k_stage_tiled3d<T, NS, 2><<<grid, t3::NT, smem, s>>>(m.in_int, m.in_xs, m.in_ys, g, kz,
-                                                             nitems, Uin, U0, Uout, ctrl);
+        k_stage_tiled3d<T, NS, 2, true><<<grid, t3::NT, smem, s>>>(box0, boxes, item_box, nitems, work);
     return 1;
 }
 

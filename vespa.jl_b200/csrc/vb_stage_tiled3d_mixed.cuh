@@ -66,28 +66,46 @@ __device__ __forceinline__ float mm(float l, float c, float r)
     return fabsf(a) < fabsf(b) ? a : b;
 }
 
+// cons2prim for VB_MIXED (src/eos.jl:8-25): velocities and the
+// total-energy-minus-kinetic pressure recovery in float64, results rounded
+// to float32.  1/rho comes from a float32 reciprocal refined by two float64
+// Newton steps (relative error ~1e-16) instead of a float64 division.
+__device__ __forceinline__ void cons2prim_mixed(const double U[5], double g, float W[5])
+{
+    const double rho = U[0];
+    double inv = (double)rcp_approx((float)rho);
+    inv = inv * (2.0 - rho * inv);
+    inv = inv * (2.0 - rho * inv);
+    const double vx = U[1] * inv, vy = U[2] * inv, vz = U[3] * inv;
+    const double kinetic = 0.5 * rho * (vx * vx + vy * vy + vz * vz);
+    const double p = (g - 1.0) * (U[4] - kinetic);
+    W[0] = (float)rho;
+    W[1] = (float)vx;
+    W[2] = (float)vy;
+    W[3] = (float)vz;
+    W[4] = (float)fmax(p, 1e-12 * kinetic);
+}
+
 // VB_MIXED CFL term of a new float64 state: compute_dt's (|v_d| + c) / w_d
-// (src/driver.jl:178-185) with 1/rho and 1/w reused (within an ulp).
+// (src/driver.jl:178-185) from the mixed primitives, wave speeds in float32
+// (a dt estimate within float32 rounding of the float64 one), max in float64.
 __device__ __forceinline__ double cfl_term(const double un[5], const Geom &g, double m)
 {
-    const double inv = 1.0 / un[0];
-    const double vx = un[1] * inv, vy = un[2] * inv, vz = un[3] * inv;
-    const double kin = 0.5 * un[0] * (vx * vx + vy * vy + vz * vz);
-    const double p = fmax((g.gamma - 1.0) * (un[4] - kin), 1e-12 * kin);
-    const double cs = sqrt(g.gamma * p * inv);
-    m = nan_max(m, (fabs(vx) + cs) * g.invw[0]);
-    m = nan_max(m, (fabs(vy) + cs) * g.invw[1]);
-    return nan_max(m, (fabs(vz) + cs) * g.invw[2]);
+    float W[5];
+    cons2prim_mixed(un, g.gamma, W);
+    const float cs = sqrt_approx((float)g.gamma * W[4] * rcp_approx(W[0]));
+    const float t = fmaxf(fmaxf((fabsf(W[1]) + cs) * (float)g.invw[0],
+                                (fabsf(W[2]) + cs) * (float)g.invw[1]),
+                          (fabsf(W[3]) + cs) * (float)g.invw[2]);
+    return nan_max(m, (double)t);
 }
 
 }  // namespace t3m
 
-template <int NS, int STAGE>
+template <int NS, int STAGE, bool BATCH>
 __global__ void __launch_bounds__(256, 2)
-k_stage_tiled3d_mixed(const __grid_constant__ CUtensorMap tm_int,
-                      const __grid_constant__ CUtensorMap tm_xs,
-                      const __grid_constant__ CUtensorMap tm_ys, Geom g, int kz, int nitems,
-                      const double *__restrict__ Uin, const double *U0, double *Uout, Ctrl *ctrl)
+k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__restrict__ boxes,
+                      const int *__restrict__ item_box, int nitems, unsigned int *work)
 {
     using namespace t3;
     using namespace t3m;
@@ -96,11 +114,34 @@ k_stage_tiled3d_mixed(const __grid_constant__ CUtensorMap tm_int,
     __shared__ double red[32];
     __shared__ int item_sh;
 
-    if (!ctrl->active) return;
     const int t = threadIdx.x;
     const int tx = t & (TX - 1), ty = t >> 4;
-    const int ntx = (int)(g.n[0] / TX);
-    const int ntiles = ntx * (int)(g.n[1] / TY);
+
+    if (t == 0) {
+        for (int s = 0; s < NS; ++s) mbar_init(&S.bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    bool timed_out = false;
+    int qb = 0;
+    for (;;) {
+    if (t == 0) item_sh = (int)atomicAdd(&work[STAGE - 1], 1u);
+    __syncthreads();
+    const int item = item_sh;
+    if (item >= nitems) break;
+    const BoxDesc &B = box_of<BATCH>(box0, boxes, item_box, item);
+    Ctrl *ctrl = B.ctrl;
+    if (!ctrl->active) {  // uniform: the box is not stepping
+        __syncthreads();  // everyone has read item_sh before thread 0 rewrites it
+        continue;
+    }
+    const Geom &g = B.g;
+    const CUtensorMap *tm = B.map[STAGE - 1];
+    const double *__restrict__ Uin = STAGE == 1 ? B.U : B.U1;
+    const double *U0 = B.U;
+    double *Uout = STAGE == 1 ? B.U1 : B.U;
+    const int kz = B.kz, ntx = B.ntx, ntiles = B.ntiles;
     const int nx = (int)g.n[0], ny = (int)g.n[1], nz = (int)g.n[2];
     const bool perx = g.bc_lo[0] == BC_PERIODIC, pery = g.bc_lo[1] == BC_PERIODIC;
     const bool perz = g.bc_lo[2] == BC_PERIODIC;
@@ -110,24 +151,11 @@ k_stage_tiled3d_mixed(const __grid_constant__ CUtensorMap tm_int,
     const double ax = g.area[0], ay = g.area[1], az = g.area[2];
     const int bx_lo = g.bc_lo[0], bx_hi = g.bc_hi[0], by_lo = g.bc_lo[1], by_hi = g.bc_hi[1];
     const int bz_lo = g.bc_lo[2], bz_hi = g.bc_hi[2];
-
-    if (t == 0) {
-        for (int s = 0; s < NS; ++s) mbar_init(&S.bar[s], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    bool timed_out = false;
     double invdt = 0.0;
-    int qb = 0;
-    for (;;) {
-    if (t == 0) item_sh = (int)atomicAdd(&ctrl->work[STAGE - 1], 1u);
-    __syncthreads();
-    const int item = item_sh;
-    if (item >= nitems) break;
-    const int tile = item % ntiles;
+    const int local = item - B.item0;
+    const int tile = local % ntiles;
     const int x0 = (tile % ntx) * TX, y0 = (tile / ntx) * TY;
-    const int k0 = (item / ntiles) * kz;
+    const int k0 = (local / ntiles) * kz;
     const int k1 = min(nz, k0 + kz);
     const int nplanes = (k1 - k0) + 4;
     const bool xlo_bnd = !perx && x0 == 0, xhi_bnd = !perx && x0 + TX == nx;
@@ -143,11 +171,11 @@ k_stage_tiled3d_mixed(const __grid_constant__ CUtensorMap tm_int,
         const int yl = (pery && y0 == 0) ? ny - 2 : y0 - 2;
         const int yh = (pery && y0 + TY == ny) ? 0 : y0 + TY;
         mbar_expect_tx(bar, PLANE_BYTES);
-        tma_load_4d(dst, &tm_int, x0, y0, z, 0, bar);
-        tma_load_4d(dst + U_XLO, &tm_xs, xl, y0, z, 0, bar);
-        tma_load_4d(dst + U_XHI, &tm_xs, xh, y0, z, 0, bar);
-        tma_load_4d(dst + U_YLO, &tm_ys, x0, yl, z, 0, bar);
-        tma_load_4d(dst + U_YHI, &tm_ys, x0, yh, z, 0, bar);
+        tma_load_4d(dst, &tm[0], x0, y0, z, 0, bar);
+        tma_load_4d(dst + U_XLO, &tm[1], xl, y0, z, 0, bar);
+        tma_load_4d(dst + U_XHI, &tm[1], xh, y0, z, 0, bar);
+        tma_load_4d(dst + U_YLO, &tm[2], x0, yl, z, 0, bar);
+        tma_load_4d(dst + U_YHI, &tm[2], x0, yh, z, 0, bar);
     };
     if (t == 0) {
         fence_proxy_async_smem();
@@ -158,20 +186,19 @@ k_stage_tiled3d_mixed(const __grid_constant__ CUtensorMap tm_int,
         if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) timed_out = true;
         const double *u = S.u[b];
         {
-            double uu[5], w[5];
+            double uu[5];
 #pragma unroll
             for (int f = 0; f < 5; ++f) uu[f] = u[f * NT + t];
-            cons2prim(uu, gamma, w);
-#pragma unroll
-            for (int f = 0; f < 5; ++f) Wown[f] = (float)w[f];
+            cons2prim_mixed(uu, gamma, Wown);
         }
         if (halo && t < NH) {
-            double uu[5], w[5];
+            double uu[5];
+            float w[5];
 #pragma unroll
             for (int f = 0; f < 5; ++f) uu[f] = u[halo_uoff(t, f)];
-            cons2prim(uu, gamma, w);
+            cons2prim_mixed(uu, gamma, w);
 #pragma unroll
-            for (int f = 0; f < 5; ++f) S.w[HB + ((q % 3) * 5 + f) * NH + t] = (float)w[f];
+            for (int f = 0; f < 5; ++f) S.w[HB + ((q % 3) * 5 + f) * NH + t] = w[f];
         }
     };
     auto release = [&](int q) {
@@ -415,7 +442,10 @@ k_stage_tiled3d_mixed(const __grid_constant__ CUtensorMap tm_int,
             const double gxh = S.gx[f][ty * (TX + 1) + tx + 1];
             const double gyl = S.gy[f][ty * TX + tx];
             const double gyh = S.gy[f][(ty + 1) * TX + tx];
-            const double gzl = az * (double)Fzlo[f], gzh = az * (double)Fzhi[f];
+            // explicit roundings: the result must not depend on how the compiler
+            // contracts this code in each kernel instantiation
+            const double gzl = __dmul_rn(az, (double)Fzlo[f]);
+            const double gzh = __dmul_rn(az, (double)Fzhi[f]);
             double a = 0.0;
             if (interior) {
                 a = a - gzl - gyl - gxl + gxh + gyh + gzh;
@@ -435,9 +465,10 @@ k_stage_tiled3d_mixed(const __grid_constant__ CUtensorMap tm_int,
             }
             const int64_t i = (int64_t)f * g.ncell + lin;
             if constexpr (STAGE == 1) {
-                un[f] = S.ep[0][f][t] - invV * a;
+                un[f] = __fma_rn(-invV, a, S.ep[0][f][t]);
             } else {
-                un[f] = 0.5 * S.ep[1][f][t] + 0.5 * (S.ep[0][f][t] - invV * a);
+                un[f] = __fma_rn(0.5, S.ep[1][f][t],
+                                 __dmul_rn(0.5, __fma_rn(-invV, a, S.ep[0][f][t])));
             }
             Uout[i] = un[f];
         }
@@ -455,52 +486,35 @@ k_stage_tiled3d_mixed(const __grid_constant__ CUtensorMap tm_int,
     }
     if constexpr (STAGE == 2) invdt = cfl_term(unp, g, invdt);  // the item's last plane
     qb += nplanes;
+    if (timed_out && t == 0) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
+    if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);  // this box's CFL max
     }  // work items
-
-    if (timed_out) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
-    if constexpr (STAGE == 2) {
-        block_max_to(&ctrl->invdt_bits, invdt, red);
-        if (blockIdx.x == 0 && t == 0) {
-            ctrl->t = ctrl->t + ctrl->dt;
-            ctrl->step = ctrl->step + 1;
-        }
-    }
 }
 
 template <int NS>
-int launch_tiled3d_mixed(const TiledMaps &m, const Geom &g, int kz, int stage, const double *Uin,
-                         const double *U0, double *Uout, Ctrl *ctrl, cudaStream_t s)
+int launch_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
+                         int nitems, unsigned int *work, int stage, cudaStream_t s)
 {
     const size_t smem = sizeof(t3m::Smem<NS>);
-    static int resident = 0;
-    if (!resident) {
-        if (cudaFuncSetAttribute(k_stage_tiled3d_mixed<NS, 1>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-            cudaFuncSetAttribute(k_stage_tiled3d_mixed<NS, 2>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return -1;
-        int dev = 0, sms = 0, per_sm = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_tiled3d_mixed<NS, 2>,
-                                                          t3::NT, smem) != cudaSuccess ||
-            per_sm < 1)
-            return -1;
-        resident = sms * per_sm;
-    }
-    if (kz <= 0) return -1;
-    const int ntiles = (int)((g.n[0] / t3::TX) * (g.n[1] / t3::TY));
-    const int nchunks = (int)((g.n[2] + kz - 1) / kz);
-    const int64_t items = (int64_t)ntiles * nchunks;
-    if (items > 0x7fffffff) return -1;
-    const int nitems = (int)items;
+    static int res1 = 0, resb = 0;
+    if (!res1) res1 = persistent_blocks(k_stage_tiled3d_mixed<NS, 1, false>,
+                                        k_stage_tiled3d_mixed<NS, 2, false>, smem);
+    if (!resb) resb = persistent_blocks(k_stage_tiled3d_mixed<NS, 1, true>,
+                                        k_stage_tiled3d_mixed<NS, 2, true>, smem);
+    const int resident = hbox ? res1 : resb;
+    if (resident <= 0 || nitems <= 0) return -1;
     const unsigned grid = (unsigned)(nitems < resident ? nitems : resident);
-    if (stage == 1)
-        k_stage_tiled3d_mixed<NS, 1><<<grid, t3::NT, smem, s>>>(m.in_int, m.in_xs, m.in_ys, g, kz,
-                                                                nitems, Uin, U0, Uout, ctrl);
+    BoxDesc box0;
+    if (hbox) box0 = *hbox;
+    else std::memset(&box0, 0, sizeof box0);
+    if (hbox && stage == 1)
+        k_stage_tiled3d_mixed<NS, 1, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (hbox)
+        k_stage_tiled3d_mixed<NS, 2, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (stage == 1)
+        k_stage_tiled3d_mixed<NS, 1, true><<<grid, t3::NT, smem, s>>>(box0, boxes, item_box, nitems, work);
     else
-        k_stage_tiled3d_mixed<NS, 2><<<grid, t3::NT, smem, s>>>(m.in_int, m.in_xs, m.in_ys, g, kz,
-                                                                nitems, Uin, U0, Uout, ctrl);
+        k_stage_tiled3d_mixed<NS, 2, true><<<grid, t3::NT, smem, s>>>(box0, boxes, item_box, nitems, work);
     return 1;
 }
 

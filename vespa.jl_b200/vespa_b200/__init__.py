@@ -11,7 +11,7 @@ from .problem import (BC, IdealHydro, Outflow, Periodic, Problem, Reflecting, co
                       initial_primitive, initial_state, kelvin_helmholtz_problem, prim2cons,
                       riemann_box_problem, sedov_problem, smooth_random_problem,
                       sod_problem_defaults, uniform01)
-from .simulation import (B200Mesh, Simulation, Totals, cell_samples, compute_dt,
+from .simulation import (B200Mesh, Batch, Simulation, Totals, cell_samples, compute_dt,
                          conserved_totals, dump_fields, evolve, primitive_at, primitive_state,
                          run_steps_async, step)
 
@@ -22,6 +22,6 @@ __all__ = [
     "initial_primitive", "initial_state", "kelvin_helmholtz_problem", "prim2cons",
     "riemann_box_problem", "sedov_problem", "smooth_random_problem", "sod_problem_defaults",
     "uniform01",
-    "B200Mesh", "Simulation", "Totals", "cell_samples", "compute_dt", "conserved_totals",
+    "B200Mesh", "Batch", "Simulation", "Totals", "cell_samples", "compute_dt", "conserved_totals",
     "dump_fields", "evolve", "primitive_at", "primitive_state", "run_steps_async", "step",
 ]

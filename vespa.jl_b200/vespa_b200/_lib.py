@@ -70,6 +70,7 @@ SIGNATURES = {
     "vb_grid_device_state": [_VP, C.POINTER(_VP)],
     "vb_grid_set_option": [_VP, C.c_int, C.c_int64],
     "vb_grid_get_option": [_VP, C.c_int, _I64P],
+    "vb_grid_autotune": [_VP, C.c_int, _I64P, _DP],
     "vb_grid_set_time": [_VP, C.c_double, C.c_int64],
     "vb_grid_get_time": [_VP, _DP, _I64P],
     "vb_compute_dt": [_VP, _DP],
@@ -78,6 +79,15 @@ SIGNATURES = {
     "vb_run_steps_async": [_VP, C.c_int64],
     "vb_conserved_totals": [_VP, _DP],
     "vb_grid_profile_step": [_VP, C.c_int, _DP, _DP, _DP],
+    "vb_batch_create": [_VP, C.c_int, C.POINTER(ProblemDesc), C.c_int, C.POINTER(_VP)],
+    "vb_batch_destroy": [_VP],
+    "vb_batch_ncell": [_VP, C.c_int, _I64P],
+    "vb_batch_upload": [_VP, C.c_int, _DP],
+    "vb_batch_download": [_VP, C.c_int, _DP],
+    "vb_batch_run_steps": [_VP, C.c_int64],
+    "vb_batch_run_steps_async": [_VP, C.c_int64],
+    "vb_batch_get_time": [_VP, C.c_int, _DP, _I64P],
+    "vb_batch_conserved_totals": [_VP, C.c_int, _DP],
     "vb_bflux_enable": [_VP, C.c_int],
     "vb_bflux_size": [_VP, _I64P],
     "vb_bflux_read": [_VP, _DP, C.c_int64],

@@ -54,6 +54,92 @@ class B200Mesh:
         return v
 
 
+def problem_desc(problem: Problem) -> _lib.ProblemDesc:
+    """vb_problem_desc of a Problem on a uniform mesh."""
+    desc = _lib.ProblemDesc()
+    desc.ndim = problem.ndim
+    for d, ((lo, hi), (blo, bhi)) in enumerate(zip(problem.domain, problem.bc_pairs())):
+        desc.dims[d] = problem.dims[d]
+        desc.lo[d] = lo
+        desc.hi[d] = hi
+        desc.bc_lo[d] = blo
+        desc.bc_hi[d] = bhi
+    desc.gamma = problem.gamma
+    desc.cfl = problem.cfl
+    desc.aexp = 1.0
+    desc.flags = 0
+    return desc
+
+
+class Batch:
+    """Many independent 3D problems stepped together on one GPU.
+
+    One persistent kernel launch per RK2 stage covers every box's column
+    tiles; each box keeps its own clock and CFL dt; runs of steps replay a
+    CUDA graph.  Each problem needs nx, ny multiples of 16 and nz >= 2."""
+
+    def __init__(self, problems, *, precision: str = "fp64", ctx: Optional[_lib.Context] = None,
+                 initial=None):
+        self.problems = list(problems)
+        self.ctx = ctx or _lib.default_context()
+        descs = (_lib.ProblemDesc * len(self.problems))(*[problem_desc(p) for p in self.problems])
+        h = C.c_void_p()
+        _lib.call("vb_batch_create", self.ctx.handle, len(self.problems), descs,
+                  PRECISIONS[precision], C.byref(h))
+        self.handle = h
+        self.precision = precision
+        for i, p in enumerate(self.problems):
+            U = initial[i] if initial is not None else initial_state(p)
+            self.upload(i, U)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().vb_batch_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.problems)
+
+    def ncell(self, box: int = -1) -> int:
+        n = C.c_int64()
+        _lib.call("vb_batch_ncell", self.handle, int(box), C.byref(n))
+        return n.value
+
+    def upload(self, box: int, U) -> None:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.shape != (5, self.ncell(box)):
+            raise ValueError("state shape does not match the box")
+        _lib.call("vb_batch_upload", self.handle, int(box), _lib.dptr(U))
+
+    def state(self, box: int, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((5, self.ncell(box)))
+        _lib.call("vb_batch_download", self.handle, int(box), _lib.dptr(out))
+        return out
+
+    def run_steps(self, nsteps: int) -> None:
+        _lib.call("vb_batch_run_steps", self.handle, int(nsteps))
+
+    def run_steps_async(self, nsteps: int) -> None:
+        _lib.call("vb_batch_run_steps_async", self.handle, int(nsteps))
+
+    def time(self, box: int) -> tuple:
+        t, n = C.c_double(), C.c_int64()
+        _lib.call("vb_batch_get_time", self.handle, int(box), C.byref(t), C.byref(n))
+        return t.value, n.value
+
+    def conserved_totals(self, box: int) -> Totals:
+        out = np.empty(5)
+        _lib.call("vb_batch_conserved_totals", self.handle, int(box), _lib.dptr(out))
+        return Totals(*[float(v) for v in out])
+
+
 class Simulation:
     """Bind a Problem to a B200Mesh, allocate the device state and set the
     initial conditions (src/driver.jl:62-79).
@@ -72,18 +158,10 @@ class Simulation:
         self.gamma = problem.gamma
         self.precision = precision
         self.ctx = ctx or _lib.default_context()
-        desc = _lib.ProblemDesc()
-        desc.ndim = backend.rank()
-        for d, ((lo, hi), (blo, bhi)) in enumerate(zip(backend.domain, problem.bc_pairs())):
-            desc.dims[d] = backend.dims[d]
+        desc = problem_desc(problem)
+        for d, (lo, hi) in enumerate(backend.domain):
             desc.lo[d] = lo
             desc.hi[d] = hi
-            desc.bc_lo[d] = blo
-            desc.bc_hi[d] = bhi
-        desc.gamma = problem.gamma
-        desc.cfl = problem.cfl
-        desc.aexp = 1.0
-        desc.flags = 0
         h = C.c_void_p()
         _lib.call("vb_grid_create", self.ctx.handle, C.byref(desc), PRECISIONS[precision],
                   C.byref(h))
@@ -144,6 +222,19 @@ class Simulation:
         _lib.call("vb_grid_set_option", self.handle, _lib.OPT_KERNEL, _lib.KERNELS[kind])
         if kz is not None:
             _lib.call("vb_grid_set_option", self.handle, _lib.OPT_TILE_KZ, int(kz))
+
+    def autotune(self, nsteps: int = 3) -> tuple:
+        """Pick the fastest z-chunk for the tiled kernel on this grid (state and
+        clock are restored).  Returns (kz, ms_per_step)."""
+        kz, ms = C.c_int64(), C.c_double()
+        _lib.call("vb_grid_autotune", self.handle, int(nsteps), C.byref(kz), C.byref(ms))
+        return kz.value, ms.value
+
+    @property
+    def kz(self) -> int:
+        v = C.c_int64()
+        _lib.call("vb_grid_get_option", self.handle, _lib.OPT_TILE_KZ, C.byref(v))
+        return v.value
 
     @property
     def kernel(self) -> str:
