@@ -145,15 +145,22 @@ def measured_hbm():
 
 
 def ncu_traffic(kernel: str, cells: int):
-    """Per-launch DRAM traffic of `kernel` scaled to `cells`, from the committed
-    ncu summary (profiles/traffic.json), or None."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    try:
-        with open(p) as f:
-            d = json.load(f)[kernel]
-        return float(d["bytes_per_cell"]) * cells
-    except (OSError, KeyError, ValueError):
-        return None
+    """Per-launch DRAM traffic of `kernel` scaled to `cells`: the
+    `traffic_bytes_per_cell <kernel> <B>` line of a committed ncu summary
+    under profiles/ (dram__bytes_read.sum + dram__bytes_write.sum of one
+    captured launch divided by its cells), or None."""
+    import glob
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        try:
+            with open(p) as f:
+                for ln in f:
+                    parts = ln.split()
+                    if len(parts) == 3 and parts[0] == "traffic_bytes_per_cell" \
+                            and parts[1] == kernel:
+                        return round(float(parts[2]) * cells)
+        except (OSError, ValueError):
+            continue
+    return None
 
 
 # ----------------------------------------------------------------- CPU baseline
