@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256, help="cells per axis of the cube")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the KH 512^2 adjoint timing and finite-difference check")
     ap.add_argument("--workload", choices=["cube", "batch64"], default="cube",
                     help="cube: the 256^3 headline; batch64: 64 uneven Riemann boxes in one batch")
     return ap.parse_args()
@@ -322,6 +324,8 @@ def run_ours(args, ranks: Ranks):
                 "algorithmic_bytes_per_launch": bytes_launch,
                 "step_hbm_frac": round(200 * cells / (d["ms"] / K / 1e3) / 1e9 / hbm, 4)}
 
+    adjoint = None if args.no_adjoint else adjoint_section(ctx, ranks)
+
     cpu = None
     if ranks.world == 1 and ranks.rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cpu_threads())
@@ -357,9 +361,86 @@ def run_ours(args, ranks: Ranks):
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }
+    if adjoint:
+        line["adjoint"] = adjoint
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
+
+
+def adjoint_section(ctx, ranks: Ranks, n=512, nsteps=200, every=20, fd_cells=32, h_rel=1e-6):
+    """KH n^2 float64: forward evolve! of nsteps vs the checkpointed adjoint
+    (forward with checkpoints, reverse sweep = segment recompute + adjoint
+    stages), all timed with CUDA events; then d(int rho^2)/d rho_0 against
+    central differences of the forward path at fd_cells random cells (dt
+    sequence held fixed), on the KH state with a 1e-2 texture and as
+    specified (exactly uniform bands: limiter ties, no derivative there)."""
+    import numpy as np
+    import vespa_b200 as vb
+
+    def fd_check(sim, U0, grad, dts):
+        V = sim.backend.cell_volume()
+        errs = []
+        for c in np.random.default_rng(3).choice(sim.ncell, size=fd_cells, replace=False):
+            h = h_rel * U0[0, c]
+            Up = U0.copy(); Up[0, c] += h
+            Um = U0.copy(); Um[0, c] -= h
+            r = []
+            for Ux in (Up, Um):
+                sim.upload(Ux)
+                for dt in dts:
+                    vb.step(sim, float(dt))
+                r.append(sim.state()[0])
+            fd = float(np.sum((r[0] - r[1]) * (r[0] + r[1])) * V) / (2.0 * h)
+            errs.append(abs(fd - grad[0, c]) / abs(grad[0, c]))
+        errs = np.array(errs)
+        return {"cells": fd_cells, "h_rel": h_rel, "median_rel_err": float(np.median(errs)),
+                "max_rel_err": float(errs.max()), "frac_within_1e-6": float(np.mean(errs <= 1e-6))}
+
+    res = {}
+    for tex in (1e-2, 0.0):
+        prob = vb.kelvin_helmholtz_problem(n=n, texture=tex)
+        mesh = vb.B200Mesh(prob.dims, prob.domain)
+        sim = vb.Simulation(mesh, prob, precision="fp64", ctx=ctx)
+        U0 = sim.state()
+        fwd = []
+        for _ in range(3):
+            sim.upload(U0)
+            sim.set_time(0.0, 0)
+            ctx.mark(4)
+            vb.evolve(sim, max_steps=nsteps)
+            ctx.mark(5)
+            fwd.append(ctx.elapsed_ms(4, 5))
+        fwd_ms = ranks.max(min(fwd[1:]))
+        sim.upload(U0)
+        sim.set_time(0.0, 0)
+        adj = vb.Adjoint(sim, nsteps, every)
+        adj.forward(max_steps=nsteps)
+        lam = vb.rho2_seed(sim, sim.state())
+        dts = adj.dts()
+        adj.backward(lam)
+        grad = adj.backward(lam)
+        tm = adj.timing()
+        entry = {"texture": tex, "fd": fd_check(sim, U0, grad, dts)}
+        if tex > 0:
+            fwd_ckpt = ranks.max(tm["forward_ms"])
+            re_ms = ranks.max(tm["recompute_ms"])
+            adj_ms = ranks.max(tm["adjoint_ms"])
+            entry.update({
+                "forward_ms": round(fwd_ms, 3), "forward_with_checkpoints_ms": round(fwd_ckpt, 3),
+                "recompute_ms": round(re_ms, 3), "adjoint_stages_ms": round(adj_ms, 3),
+                "adj_step_over_fwd_step": round((re_ms + adj_ms) / fwd_ms, 3),
+                "adj_stages_over_fwd": round(adj_ms / fwd_ms, 3),
+                "gradient_over_forward": round((fwd_ckpt + re_ms + adj_ms) / fwd_ms, 3)})
+        res["textured" if tex > 0 else "as_specified"] = entry
+        adj.close()
+        sim.close()
+    return {"config": f"2D Kelvin-Helmholtz {n}^2 periodic, gamma 1.4, float64, {nsteps} "
+                      f"CFL-limited RK2 steps, checkpoints every {every}; J = int rho^2 at "
+                      "t_end, gradient w.r.t. the initial conserved density",
+            "adj_step": "reverse sweep per step (segment recompute + two adjoint stages) "
+                        "over the forward step (evolve!)",
+            **res}
 
 
 def run_batch64(args, ranks: Ranks):

@@ -199,6 +199,36 @@ int vb_bflux_size(const vb_grid *grid, int64_t *n);
 int vb_bflux_read(vb_grid *grid, double *out, int64_t n);
 int vb_bflux_clear(vb_grid *grid);
 
+/* Adjoint of the float64 SSP-RK2 step on a periodic grid (no counterpart in
+ * the reference, which has no adjoint; it differentiates the map that
+ * step!/evolve! apply, src/driver.jl:285-359,483-508).  Reverse mode, written
+ * by hand: HLLC, minmod and the pressure floor keep the branches the forward
+ * evaluation took, and each step's dt is held at its forward value.
+ *
+ * vb_adjoint_forward runs up to max_steps CFL-limited steps of the grid
+ * (like vb_evolve), keeping a copy of the state every checkpoint_every steps
+ * and every step's dt.  vb_adjoint_backward maps dJ/dU at the end of that run
+ * (host, the state layout) to dJ/dU at its start, recomputing each segment
+ * from its checkpoint.  Device memory: (ceil(max_steps/checkpoint_every) +
+ * 2*checkpoint_every + 2 + 2*ndim) states.  The grid must be VB_FP64 and
+ * periodic on every side (VB_ENOTSUP otherwise). */
+typedef struct vb_adjoint vb_adjoint;
+int vb_adjoint_create(vb_grid *grid, int64_t max_steps, int64_t checkpoint_every,
+                      vb_adjoint **out);
+int vb_adjoint_destroy(vb_adjoint *adj);
+int vb_adjoint_forward(vb_adjoint *adj, double tfinal, int64_t max_steps, double *t,
+                       int64_t *nsteps);
+int vb_adjoint_steps(const vb_adjoint *adj, int64_t *nsteps);
+/* dt of each recorded step; n must equal the recorded step count. */
+int vb_adjoint_dts(const vb_adjoint *adj, double *dts, int64_t n);
+int vb_adjoint_backward(vb_adjoint *adj, const double *lam_final, double *lam_init);
+/* One step from the grid's current state with the given dt (the grid is not
+ * advanced): lam_in = (dU^{n+1}/dU^n)^T lam_out. */
+int vb_adjoint_step(vb_adjoint *adj, double dt, const double *lam_out, double *lam_in);
+/* Device milliseconds of the last forward run, and of the last backward
+ * sweep's recompute and adjoint stages. */
+int vb_adjoint_timing(const vb_adjoint *adj, double ms[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,27 +18,6 @@
 using vb::detail::fail;
 using vb::detail::use;
 
-struct vb_grid {
-    vb_ctx *ctx = nullptr;
-    vb::Geom g{};
-    int precision = VB_FP64;
-    double *U = nullptr;   // state (and u0: the stage-2 update runs in place)
-    double *U1 = nullptr;  // stage-1 state
-    vb::Ctrl *ctrl = nullptr;   // device control block
-    vb::Ctrl *hctrl = nullptr;  // pinned host mirror
-    double *partials = nullptr;
-    double *totals = nullptr;
-    double *htot = nullptr;     // pinned
-    double *bflux = nullptr;
-    int64_t bflux_n = 0;
-    bool bflux_on = false;
-    bool invdt_valid = false;   // ctrl->invdt_bits holds the CFL max of the current state
-    bool tiled = false;         // the tiled 3D kernels apply to this grid
-    int kz = 64;                // z planes per tiled work item
-    vb::TiledMaps maps_U{}, maps_U1{};  // TMA descriptors of the two stage inputs
-    vb::BoxDesc box{};                  // the tiled kernels' box descriptor (passed by value)
-    int box_kz = 0;                     // kz the descriptor was written with
-};
 
 namespace {
 thread_local std::string g_err;
@@ -303,6 +282,11 @@ int push_ctrl(vb_grid *gr)
 }
 
 }  // namespace
+
+int vb::detail::grid_ensure_cfl(vb_grid *gr) { return ensure_cfl(gr); }
+int vb::detail::grid_rk2(vb_grid *gr) { return rk2(gr); }
+int vb::detail::grid_pull_ctrl(vb_grid *gr) { return pull_ctrl(gr); }
+int vb::detail::grid_push_ctrl(vb_grid *gr) { return push_ctrl(gr); }
 
 void vb::set_last_error(const char *msg) { g_err = msg; }
 

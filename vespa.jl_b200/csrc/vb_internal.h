@@ -16,6 +16,28 @@ struct vb_ctx {
     cudaEvent_t marks[16] = {};
 };
 
+struct vb_grid {
+    vb_ctx *ctx = nullptr;
+    vb::Geom g{};
+    int precision = VB_FP64;
+    double *U = nullptr;   // state (and u0: the stage-2 update runs in place)
+    double *U1 = nullptr;  // stage-1 state
+    vb::Ctrl *ctrl = nullptr;   // device control block
+    vb::Ctrl *hctrl = nullptr;  // pinned host mirror
+    double *partials = nullptr;
+    double *totals = nullptr;
+    double *htot = nullptr;     // pinned
+    double *bflux = nullptr;
+    int64_t bflux_n = 0;
+    bool bflux_on = false;
+    bool invdt_valid = false;   // ctrl->invdt_bits holds the CFL max of the current state
+    bool tiled = false;         // the tiled 3D kernels apply to this grid
+    int kz = 64;                // z planes per tiled work item
+    vb::TiledMaps maps_U{}, maps_U1{};  // TMA descriptors of the two stage inputs
+    vb::BoxDesc box{};                  // the tiled kernels' box descriptor (passed by value)
+    int box_kz = 0;                     // kz the descriptor was written with
+};
+
 namespace vb {
 namespace detail {
 
@@ -33,6 +55,12 @@ BoxDesc make_box(const TiledMaps &mU, const TiledMaps &mU1, const Geom &g, doubl
 int64_t box_items(const Geom &g, int kz);
 // default z-chunk of a tiled grid
 int default_kz(const Geom &g);
+
+// Grid stepping helpers shared with the adjoint (vb_api.cu).
+int grid_ensure_cfl(vb_grid *gr);   // CFL max of the current state, if stale
+int grid_rk2(vb_grid *gr);          // one RK2 step with dt already in the control block
+int grid_pull_ctrl(vb_grid *gr);    // device control block -> gr->hctrl (synchronous)
+int grid_push_ctrl(vb_grid *gr);    // gr->hctrl -> device control block (synchronous)
 
 }  // namespace detail
 }  // namespace vb

@@ -68,6 +68,15 @@ int launch_stage_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const 
 int launch_stage_mixed(const Geom &g, int stage, const double *Uin, const double *U0,
                        double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s);
 
+// vb_adjoint_kern.cu (periodic meshes, float64): one adjoint RK2 stage,
+//   out = 0.5*lam + (M ? M : 0) - invV * (dD/dU)^T mu,  mu = M ? M : 0.5*lam,
+// at the state U; gL/gR (2*nd*5*ncell doubles) and code (nd*ncell) are scratch.
+int launch_adj_stage(const Geom &g, const double *U, const double *lam, const double *M,
+                     double invV, double *gL, double *gR, uint16_t *code, double *out,
+                     cudaStream_t s);
+// dts[ctrl->step - step0] = ctrl->dt while the step in flight is active
+int launch_record_dt(const Ctrl *ctrl, double *dts, int64_t step0, int64_t cap, cudaStream_t s);
+
 constexpr int TOTALS_PARTS = 1024;  // fixed partial count: deterministic sum order
 
 // vb_api.cu: record the calling thread's message for vb_last_error.

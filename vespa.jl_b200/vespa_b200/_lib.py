@@ -92,6 +92,14 @@ SIGNATURES = {
     "vb_bflux_size": [_VP, _I64P],
     "vb_bflux_read": [_VP, _DP, C.c_int64],
     "vb_bflux_clear": [_VP],
+    "vb_adjoint_create": [_VP, C.c_int64, C.c_int64, C.POINTER(_VP)],
+    "vb_adjoint_destroy": [_VP],
+    "vb_adjoint_forward": [_VP, C.c_double, C.c_int64, _DP, _I64P],
+    "vb_adjoint_steps": [_VP, _I64P],
+    "vb_adjoint_dts": [_VP, _DP, C.c_int64],
+    "vb_adjoint_backward": [_VP, _DP, _DP],
+    "vb_adjoint_step": [_VP, C.c_double, _DP, _DP],
+    "vb_adjoint_timing": [_VP, _DP],
 }
 
 _lib = None

@@ -267,23 +267,34 @@ def smooth_random_problem(dims: Sequence[int], seed: int = DEFAULT_SEED, gamma: 
 
 
 def kelvin_helmholtz_problem(n: int = 512, seed: int = DEFAULT_SEED, tfinal: float = math.inf,
-                             cfl: float = 0.4) -> Problem:
+                             cfl: float = 0.4, texture: float = 0.0) -> Problem:
     """2D Kelvin-Helmholtz: rho=2, u_x=+0.5 in |y-0.5|<0.25, else rho=1,
-    u_x=-0.5; p=2.5; u_y = 0.01 sin(4 pi x) + 1e-3 * uniform[-1,1]; periodic."""
+    u_x=-0.5; p=2.5; u_y = 0.01 sin(4 pi x) + 1e-3 * uniform[-1,1]; periodic.
+
+    ``texture`` > 0 multiplies rho and p by (1 + texture*uniform[-1,1]) and
+    adds texture*uniform[-1,1] to u_x, cell by cell (seeded).  Without it the
+    bands are exactly uniform in rho, u_x and p, so the minmod limiter sits on
+    its kinks there and the step map has no derivative at that state; a
+    texture makes the state generic for finite-difference checks."""
     def init_prim(prob):
         x, y = prob.cell_centers()
         band = np.abs(y - 0.5) < 0.25
         W = np.empty((5, prob.ncell))
         W[0] = np.where(band, 2.0, 1.0)
         W[1] = np.where(band, 0.5, -0.5)
-        noise = 2.0 * uniform01(seed, 7, np.arange(prob.ncell, dtype=np.uint64)) - 1.0
+        cells = np.arange(prob.ncell, dtype=np.uint64)
+        noise = 2.0 * uniform01(seed, 7, cells) - 1.0
         W[2] = 0.01 * np.sin(4.0 * math.pi * x) + 1e-3 * noise
         W[3] = 0.0
         W[4] = 2.5
+        if texture > 0.0:
+            W[0] = W[0] * (1.0 + texture * (2.0 * uniform01(seed, 8, cells) - 1.0))
+            W[1] = W[1] + texture * (2.0 * uniform01(seed, 9, cells) - 1.0)
+            W[4] = W[4] * (1.0 + texture * (2.0 * uniform01(seed, 10, cells) - 1.0))
         return W
     return Problem(name="KelvinHelmholtz2D", dims=(n, n), domain=((0.0, 1.0), (0.0, 1.0)),
                    gamma=1.4, bcs=Periodic, init_prim=init_prim, tfinal=tfinal, cfl=cfl,
-                   meta={"seed": seed})
+                   meta={"seed": seed, "texture": texture})
 
 
 BOX_SIDES = (32, 48, 64, 96, 128, 192, 256)

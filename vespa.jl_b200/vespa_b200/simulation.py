@@ -10,6 +10,7 @@ libvespa_b200.so; the state never leaves the GPU unless the caller reads it.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import math
 from collections import namedtuple
 from typing import Callable, Optional
@@ -166,12 +167,15 @@ class Simulation:
         _lib.call("vb_grid_create", self.ctx.handle, C.byref(desc), PRECISIONS[precision],
                   C.byref(h))
         self.handle = h
+        self._dependents = weakref.WeakSet()  # adjoints bound to this grid
         self.ncell = backend.n_cells()
         U = initial if initial is not None else initial_state(problem)
         self.upload(U)
 
     # -- lifetime --
     def close(self):
+        for dep in list(getattr(self, "_dependents", ())):
+            dep.close()
         if getattr(self, "handle", None):
             _lib.load().vb_grid_destroy(self.handle)
             self.handle = C.c_void_p()
