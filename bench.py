@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256, help="cells per axis of the cube")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-amr", action="store_true",
+                    help="skip the Sedov 48^2 AMR run")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the KH 512^2 adjoint timing and finite-difference check")
     ap.add_argument("--workload", choices=["cube", "batch64"], default="cube",
@@ -325,6 +327,7 @@ def run_ours(args, ranks: Ranks):
                 "step_hbm_frac": round(200 * cells / (d["ms"] / K / 1e3) / 1e9 / hbm, 4)}
 
     adjoint = None if args.no_adjoint else adjoint_section(ctx, ranks)
+    amr = None if args.no_amr else amr_section(ctx, ranks)
 
     cpu = None
     if ranks.world == 1 and ranks.rank == 0 and not args.no_cpu_baseline:
@@ -363,6 +366,8 @@ def run_ours(args, ranks: Ranks):
     }
     if adjoint:
         line["adjoint"] = adjoint
+    if amr:
+        line["amr"] = amr
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -441,6 +446,66 @@ def adjoint_section(ctx, ranks: Ranks, n=512, nsteps=200, every=20, fd_cells=32,
             "adj_step": "reverse sweep per step (segment recompute + two adjoint stages) "
                         "over the forward step (evolve!)",
             **res}
+
+
+def amr_section(ctx, ranks: Ranks, cpu_steps=60):
+    """2D Sedov blast on the composite AMR mesh: 48^2 base, E = 1 in a 3-cell
+    hot spot, reflecting walls, regrid every 4 steps refining above a density
+    jump of 0.2 up to 4 levels, float64, to t = 0.05.  Single-rate (one global
+    dt) and subcycled (per-level dt with flux registers).  Device time of the
+    whole run (regrids, i.e. tag download, host tree/table rebuild and upload,
+    included); leaf-updates = sum over steps of the leaves stepped."""
+    import numpy as np
+    import vespa_b200 as vb
+    from vespa_b200 import amr as A
+    prob = vb.sedov_problem(n=48, r0=3.0 / 48, tfinal=0.05)
+    pol = A.RefinementPolicy(0.2, 4, 4)
+    out = {"config": "2D Sedov 48^2 base, r0 = 3 cells, gamma 1.4, reflecting, CFL 0.3, "
+                     "RefinementPolicy(refine_above=0.2, max_level=4, every=4), t_end = 0.05, float64"}
+    for sub in (False, True):
+        sim = A.AmrSimulation(A.AmrMesh(prob.dims, prob.domain), prob, ctx=ctx)
+        t0 = A.conserved_totals(sim)
+        ms = 0.0
+        updates = 0
+        regrid_ms = 0.0
+        while sim.t < prob.tfinal * (1 - 1e-12):
+            s0 = sim.step
+            ctx.mark(6)
+            A.evolve(sim, policy=pol, subcycle=sub, max_steps=4 if not sub else 1)
+            ctx.mark(7)
+            ms += ctx.elapsed_ms(6, 7)
+            regrid_ms += sim.regrid_ms()
+            if not sub:
+                updates += (sim.step - s0) * sim.nleaf
+        t1 = A.conserved_totals(sim)
+        entry = {"steps": sim.step, "leaves_final": sim.nleaf, "max_level": sim.max_level,
+                 "faces_final": sim.nface, "ms": round(ranks.max(ms), 3),
+                 "regrid_ms": round(regrid_ms, 3),
+                 "mass_drift_rel": abs(t1.mass - t0.mass) / t0.mass,
+                 "energy_drift_rel": abs(t1.energy - t0.energy) / t0.energy}
+        if not sub:
+            entry["leaf_updates"] = updates
+            entry["value"] = round(updates / (entry["ms"] / 1e3) / 1e6, 2)
+            entry["unit"] = "Mleaf-updates/s"
+        out["subcycled" if sub else "single_rate"] = entry
+        sim.close()
+    # the oracle on the first cpu_steps steps of the same run (host, 1 thread)
+    if ranks.rank == 0:
+        from oracle import oracle as O
+        ora = O.Amr(O.grid_from_problem(prob))
+        ora.set_state(vb.initial_state(prob))
+        upd, t_cpu, done = 0, 0.0, 0
+        while done < cpu_steps:
+            ts = time.perf_counter()
+            ora.evolve(prob.tfinal, max_steps=4, refine_above=0.2, max_level=4, every=4)
+            t_cpu += time.perf_counter() - ts
+            upd += 4 * ora.nleaf
+            done += 4
+        out["cpu_oracle"] = {"value": round(upd / t_cpu / 1e6, 3), "unit": "Mleaf-updates/s",
+                             "cores": 1, "kind": "port",
+                             "sample": f"first {cpu_steps} single-rate steps of the same run, "
+                                       "C oracle (serial, like the reference's loop)"}
+    return out
 
 
 def run_batch64(args, ranks: Ranks):

@@ -229,6 +229,50 @@ int vb_adjoint_step(vb_adjoint *adj, double dt, const double *lam_out, double *l
  * sweep's recompute and adjoint stages. */
 int vb_adjoint_timing(const vb_adjoint *adj, double ms[3]);
 
+/* Composite AMR mesh (lib/HGBackend/src/HGBackend.jl semantics): the base
+ * grid of `base` is a forest of root cells refined into a 2:1 face-balanced
+ * cell tree whose leaves are the cells; float64 only.  Leaves are ordered
+ * by root (column-major), then depth first with children x fastest; the state
+ * is five float64 fields of nleaf values in that order.  Faces follow the
+ * reference's emission rules (conforming faces from the hi side, coarse<->fine
+ * sub-faces from the fine side with the fine area), PLM uses the
+ * representative face neighbour (the first finer leaf when the neighbours are
+ * finer), regrid is refine-only on the density-gradient indicator with
+ * piecewise-constant prolongation (src/driver.jl:400-462), and the drivers
+ * are evolve! with a RefinementPolicy, single rate or subcycled with flux
+ * registers (src/driver.jl:483-605, src/reflux.jl:51-103). */
+typedef struct vb_amr vb_amr;
+int vb_amr_create(vb_ctx *ctx, const vb_problem_desc *base, vb_amr **out);
+int vb_amr_destroy(vb_amr *amr);
+int vb_amr_nleaf(const vb_amr *amr, int64_t *nleaf);
+int vb_amr_nface(const vb_amr *amr, int64_t *nface);
+/* level (0 = base) and integer coordinates at that level (3 per leaf) */
+int vb_amr_leaves(const vb_amr *amr, int32_t *level, int64_t *coords);
+int vb_amr_max_level(const vb_amr *amr, int32_t *level);
+int vb_amr_upload(vb_amr *amr, const double *U);
+int vb_amr_download(vb_amr *amr, double *U);
+int vb_amr_set_time(vb_amr *amr, double t, int64_t step);
+int vb_amr_get_time(const vb_amr *amr, double *t, int64_t *step);
+/* refine! of the given leaves (indices in the current order), with balance */
+int vb_amr_refine(vb_amr *amr, const int64_t *leaves, int64_t n);
+/* density_gradient_indicator of every leaf */
+int vb_amr_indicator(vb_amr *amr, double *out);
+/* regrid!: refine leaves below max_level whose indicator exceeds refine_above */
+int vb_amr_regrid(vb_amr *amr, double refine_above, int max_level, int64_t *ntagged);
+/* compute_dt over one level (level < 0: every leaf); +Inf for an empty level */
+int vb_amr_compute_dt(vb_amr *amr, int level, double *dt);
+/* step!(sim, dt): one single-rate SSP-RK2 step, advances the clock */
+int vb_amr_step(vb_amr *amr, double dt);
+/* step!(sim, dt; level): only that level's leaves, clock unchanged */
+int vb_amr_step_level(vb_amr *amr, double dt, int level);
+/* evolve! with RefinementPolicy(refine_above, max_level, every); every <= 0
+ * disables regrid; subcycle != 0 selects evolve_level! with flux registers. */
+int vb_amr_evolve(vb_amr *amr, double tfinal, int64_t max_steps, double refine_above,
+                  int max_level, int every, int subcycle, double *t, int64_t *nsteps);
+/* device milliseconds spent in regrids during the last vb_amr_evolve */
+int vb_amr_regrid_ms(const vb_amr *amr, double *ms);
+int vb_amr_conserved_totals(vb_amr *amr, double out[5]);
+
 #ifdef __cplusplus
 }
 #endif

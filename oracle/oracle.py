@@ -74,6 +74,33 @@ def lib():
         L.vo_bflux_size.restype = C.c_int64
         L.vo_exact_riemann_star.argtypes = [dp, dp, C.c_double, dp]
         L.vo_exact_riemann_sample.argtypes = [dp, dp, C.c_double, C.c_double, dp]
+        vp = C.c_void_p
+        i64 = C.c_int64
+        L.vo_amr_create.argtypes = [gp]
+        L.vo_amr_create.restype = vp
+        L.vo_amr_destroy.argtypes = [vp]
+        L.vo_amr_nleaf.argtypes = [vp]
+        L.vo_amr_nleaf.restype = i64
+        L.vo_amr_leaves.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
+        L.vo_amr_set_state.argtypes = [vp, dp]
+        L.vo_amr_get_state.argtypes = [vp, dp]
+        L.vo_amr_set_time.argtypes = [vp, C.c_double, i64]
+        L.vo_amr_time.argtypes = [vp]
+        L.vo_amr_time.restype = C.c_double
+        L.vo_amr_steps.argtypes = [vp]
+        L.vo_amr_steps.restype = i64
+        L.vo_amr_max_level.argtypes = [vp]
+        L.vo_amr_refine.argtypes = [vp, C.POINTER(C.c_int64), i64]
+        L.vo_amr_refine.restype = i64
+        L.vo_amr_indicator.argtypes = [vp, dp]
+        L.vo_amr_regrid.argtypes = [vp, C.c_double, C.c_int]
+        L.vo_amr_regrid.restype = i64
+        L.vo_amr_compute_dt.argtypes = [vp, C.c_int]
+        L.vo_amr_compute_dt.restype = C.c_double
+        L.vo_amr_step.argtypes = [vp, C.c_double, C.c_int]
+        L.vo_amr_evolve.argtypes = [vp, C.c_double, i64, C.c_double, C.c_int, C.c_int, C.c_int]
+        L.vo_amr_evolve.restype = i64
+        L.vo_amr_totals.argtypes = [vp, dp]
         _lib = L
     return _lib
 
@@ -207,3 +234,87 @@ def exact_riemann_sample(WL, WR, gamma, s):
     out = np.empty(3)
     lib().vo_exact_riemann_sample(_dp(WL), _dp(WR), gamma, float(s), _dp(out))
     return out
+
+
+class Amr:
+    """The AMR restatement (vespa_oracle_amr.c): a composite leaf-only mesh
+    over a base grid, with the reference's face rules, regrid and drivers.
+    The state is a (5, nleaf) float64 array in leaf order."""
+
+    def __init__(self, g: VoGrid):
+        self.h = lib().vo_amr_create(C.byref(g))
+
+    def close(self):
+        if self.h:
+            lib().vo_amr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nleaf(self) -> int:
+        return int(lib().vo_amr_nleaf(self.h))
+
+    def leaves(self):
+        n = self.nleaf
+        lev = np.empty(n, dtype=np.int32)
+        cx = np.empty((n, 3), dtype=np.int64)
+        lib().vo_amr_leaves(self.h, lev.ctypes.data_as(C.POINTER(C.c_int32)),
+                            cx.ctypes.data_as(C.POINTER(C.c_int64)))
+        return lev, cx
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        assert U.shape == (5, self.nleaf)
+        lib().vo_amr_set_state(self.h, _dp(U))
+
+    def state(self):
+        U = np.empty((5, self.nleaf))
+        lib().vo_amr_get_state(self.h, _dp(U))
+        return U
+
+    def set_time(self, t, step=0):
+        lib().vo_amr_set_time(self.h, float(t), int(step))
+
+    @property
+    def t(self):
+        return float(lib().vo_amr_time(self.h))
+
+    @property
+    def step_count(self):
+        return int(lib().vo_amr_steps(self.h))
+
+    @property
+    def max_level(self):
+        return int(lib().vo_amr_max_level(self.h))
+
+    def refine(self, leaves):
+        idx = np.ascontiguousarray(leaves, dtype=np.int64)
+        return int(lib().vo_amr_refine(self.h, idx.ctypes.data_as(C.POINTER(C.c_int64)), len(idx)))
+
+    def indicator(self):
+        out = np.empty(self.nleaf)
+        lib().vo_amr_indicator(self.h, _dp(out))
+        return out
+
+    def regrid(self, refine_above, max_level):
+        return int(lib().vo_amr_regrid(self.h, float(refine_above), int(max_level)))
+
+    def compute_dt(self, level=-1):
+        return float(lib().vo_amr_compute_dt(self.h, int(level)))
+
+    def step(self, dt, level=-1):
+        lib().vo_amr_step(self.h, float(dt), int(level))
+
+    def evolve(self, tfinal, max_steps=-1, refine_above=0.0, max_level=0, every=0, subcycle=False):
+        return int(lib().vo_amr_evolve(self.h, float(tfinal), int(max_steps), float(refine_above),
+                                       int(max_level), int(every), int(bool(subcycle))))
+
+    def totals(self):
+        out = np.empty(5)
+        lib().vo_amr_totals(self.h, _dp(out))
+        return out

@@ -70,6 +70,28 @@ void vo_exact_riemann_star(const double *WL, const double *WR, double gamma, dou
 void vo_exact_riemann_sample(const double *WL, const double *WR, double gamma, double s,
                              double *out);
 
+
+/* AMR (vespa_oracle_amr.c): composite leaf-only mesh over a base grid. */
+typedef struct vo_amr vo_amr;
+vo_amr *vo_amr_create(const vo_grid *g);
+void vo_amr_destroy(vo_amr *a);
+int64_t vo_amr_nleaf(const vo_amr *a);
+void vo_amr_leaves(const vo_amr *a, int32_t *level, int64_t *coords);
+void vo_amr_set_state(vo_amr *a, const double *U);
+void vo_amr_get_state(const vo_amr *a, double *U);
+void vo_amr_set_time(vo_amr *a, double t, int64_t step);
+double vo_amr_time(const vo_amr *a);
+int64_t vo_amr_steps(const vo_amr *a);
+int vo_amr_max_level(const vo_amr *a);
+int64_t vo_amr_refine(vo_amr *a, const int64_t *leaves, int64_t n);
+void vo_amr_indicator(const vo_amr *a, double *out);
+int64_t vo_amr_regrid(vo_amr *a, double refine_above, int max_level);
+double vo_amr_compute_dt(const vo_amr *a, int level);
+void vo_amr_step(vo_amr *a, double dt, int level);
+int64_t vo_amr_evolve(vo_amr *a, double tfinal, int64_t max_steps, double refine_above,
+                      int max_level, int every, int subcycle);
+void vo_amr_totals(const vo_amr *a, double *out);
+
 #ifdef __cplusplus
 }
 #endif

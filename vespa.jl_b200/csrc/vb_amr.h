@@ -1,0 +1,55 @@
+// vb_amr.h -- device view of the composite AMR mesh and the launchers of
+// vb_amr_kern.cu.  Not part of the public ABI.
+#pragma once
+
+#include "vb_launch.h"
+
+namespace vb {
+
+constexpr int AMR_MAX_LEVEL = 15;  // levels above the base grid
+
+// The mesh tables the kernels read (device pointers), by value per launch.
+struct AmrDev {
+    int nd;
+    int bc_lo[3], bc_hi[3];
+    double gamma, aexp;
+    int64_t cap;     // leaf capacity: field stride of U, reg, rep
+    int64_t fcap;    // face capacity: field stride of F
+    int nleaf, nface;
+    const int *lev;       // level of each leaf
+    const int *rep;       // [2*axis+side][cap]: representative neighbour, -1 boundary
+    const int *fL, *fR;   // face sides (-1: boundary ghost)
+    const int8_t *fax;    // face axis (0-based)
+    const double *farea;  // face area
+    const int *off;       // CSR offsets, nleaf+1
+    const int *ent;       // CSR entries: face*2 + (1 if the leaf is the face's right side)
+    double *reg;          // flux registers, [5][cap]
+    double vol[AMR_MAX_LEVEL + 1];
+    double w[AMR_MAX_LEVEL + 1][3];
+};
+
+// Per-stage parameters: dt, which level is updated (-1: all), active flux
+// registers (coarse level and signed scale), and whether the stage-2
+// epilogue folds the CFL maximum of every leaf.
+struct AmrStageArgs {
+    double dt;
+    int level;
+    int nreg;
+    int reg_level[2];
+    double reg_scale[2];
+    int cfl_all;
+};
+
+int launch_amr_stage(const AmrDev &m, int stage, const double *Uin, const double *U0,
+                     double *Uout, double *F, const AmrStageArgs &a, Ctrl *ctrl, cudaStream_t s);
+int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cudaStream_t s);
+int launch_amr_tag(const AmrDev &m, const double *U, double above, int max_level, uint8_t *tag,
+                   double *ind, cudaStream_t s);
+int launch_amr_prolong(int n, int64_t cap_old, int64_t cap_new, const int *src, const double *Uold,
+                       double *Unew, cudaStream_t s);
+int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s);
+int launch_amr_zero_reg(const AmrDev &m, int level, cudaStream_t s);
+int launch_amr_totals(const AmrDev &m, const double *U, double *partials, int npart, double *out,
+                      cudaStream_t s);
+
+}  // namespace vb

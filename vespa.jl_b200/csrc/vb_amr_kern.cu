@@ -1,0 +1,322 @@
+// vb_amr_kern.cu -- device kernels of the composite AMR mesh (float64, built
+// with -fmad=false: bit-identical to a serial evaluation in the reference's
+// order).
+//
+// The mesh is a table set rebuilt on the host after every regrid:
+//   - leaves in depth-first order with their level; per-level widths/volumes
+//   - rep[2*axis+side][leaf]: the representative face neighbour (PLM stencil
+//     and refinement indicator), -1 at a domain boundary
+//   - faces in the reference's emission order (HGBackend.jl:220-276):
+//     left leaf, right leaf (-1 = boundary ghost side), axis, area
+//   - per-leaf CSR of (face, sign) in emission order, so each leaf sums its
+//     flux contributions in exactly the reference's order
+// One RK2 stage is two launches: k_amr_faces (one thread per face: PLM face
+// states, HLLC) and k_amr_cells (one thread per leaf: ordered flux
+// divergence, flux-register capture, stage update, CFL maximum).
+#include "vb_amr.h"
+#include "vb_physics.cuh"
+
+namespace vb {
+
+namespace {
+
+__device__ __forceinline__ void amr_prim(const AmrDev &m, const double *__restrict__ U, int i,
+                                         double W[5])
+{
+    double u[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) u[k] = U[(int64_t)k * m.cap + i];
+    cons2prim(u, m.gamma, W);
+}
+
+// _face_value(sim, i, axis, side) with the slope from representatives
+__device__ __forceinline__ void amr_face_value(const AmrDev &m, const double *__restrict__ U, int i,
+                                               int ax, bool hi, double out[5])
+{
+    double Wc[5], Wl[5], Wr[5];
+    amr_prim(m, U, i, Wc);
+    const int jl = m.rep[(2 * ax) * m.cap + i];
+    const int jr = m.rep[(2 * ax + 1) * m.cap + i];
+    if (jl >= 0) amr_prim(m, U, jl, Wl); else ghost_state<double>(Wc, m.bc_lo[ax], ax, Wl);
+    if (jr >= 0) amr_prim(m, U, jr, Wr); else ghost_state<double>(Wc, m.bc_hi[ax], ax, Wr);
+    const double h = hi ? 0.5 : -0.5;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = face_val(Wc[k], h, limited_slope<double>(Wl[k], Wc[k], Wr[k]));
+}
+
+template <int DIM>
+__device__ __forceinline__ void amr_face(const AmrDev &m, const double *__restrict__ U, int f,
+                                         double *__restrict__ F)
+{
+    const int L = m.fL[f], R = m.fR[f];
+    constexpr int ax = DIM - 1;
+    double WL[5], WR[5], out[5];
+    if (L >= 0 && R >= 0) {
+        amr_face_value(m, U, L, ax, true, WL);
+        amr_face_value(m, U, R, ax, false, WR);
+    } else if (R < 0) {
+        amr_face_value(m, U, L, ax, true, WL);
+        ghost_state<double>(WL, m.bc_hi[ax], ax, WR);
+    } else {
+        amr_face_value(m, U, R, ax, false, WR);
+        ghost_state<double>(WR, m.bc_lo[ax], ax, WL);
+    }
+    hllc_flux<double, DIM>(WL, WR, m.gamma, out);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) F[(int64_t)k * m.fcap + f] = out[k];
+}
+
+__global__ void __launch_bounds__(256) k_amr_faces(AmrDev m, const double *__restrict__ U,
+                                                   double *__restrict__ F, const Ctrl *gate)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nface) return;
+    if (gate && !gate->active) return;
+    switch (m.fax[f]) {
+    case 0: amr_face<1>(m, U, f, F); break;
+    case 1: amr_face<2>(m, U, f, F); break;
+    default: amr_face<3>(m, U, f, F); break;
+    }
+}
+
+// One stage over the leaves.  `level` < 0 updates every leaf; otherwise only
+// that level (step!(sim, dt; level)), and stage 1 copies the other leaves into
+// Uout so stage 2 reads one consistent state.  Registers: up to two active
+// (coarse level, scale) pairs; a leaf at a register's coarse level adds
+// scale*F*area (sign by side) for each face to a leaf one level finer.
+template <int STAGE>
+__global__ void __launch_bounds__(256)
+k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *Uout,
+            const double *__restrict__ F, AmrStageArgs a, Ctrl *ctrl)
+{
+    __shared__ double red[32];
+    // a.dt < 0: dt from the control block, and nothing to do once inactive
+    double dt = a.dt;
+    if (dt < 0.0) {
+        if (!ctrl->active) return;
+        dt = ctrl->dt;
+    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double invdt = 0.0;
+    if (i < m.nleaf) {
+        const int li = m.lev[i];
+        const bool upd = a.level < 0 || li == a.level;
+        int rslot = -1;
+        for (int r = 0; r < a.nreg; ++r)
+            if (a.reg_level[r] == li) rslot = r;
+        if (upd || rslot >= 0) {
+            double acc[5] = {0, 0, 0, 0, 0}, rg[5];
+            const double rs = rslot >= 0 ? a.reg_scale[rslot] : 0.0;
+            if (rslot >= 0)
+#pragma unroll
+                for (int k = 0; k < 5; ++k) rg[k] = m.reg[(int64_t)k * m.cap + i];
+            const int e0 = m.off[i], e1 = m.off[i + 1];
+            for (int e = e0; e < e1; ++e) {
+                const int code = m.ent[e];
+                const int f = code >> 1;
+                const bool neg = code & 1;
+                const double ar = m.farea[f];
+                double Fk[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) Fk[k] = F[(int64_t)k * m.fcap + f];
+                const double s = neg ? -ar : ar;
+#pragma unroll
+                for (int k = 0; k < 5; ++k) acc[k] = acc[k] + s * Fk[k];
+                if (rslot >= 0) {
+                    const int other = neg ? m.fL[f] : m.fR[f];
+                    if (other >= 0 && m.lev[other] == li + 1) {
+                        const double ss = neg ? -rs : rs;
+#pragma unroll
+                        for (int k = 0; k < 5; ++k) rg[k] = rg[k] + ss * Fk[k] * ar;
+                    }
+                }
+            }
+            if (rslot >= 0)
+#pragma unroll
+                for (int k = 0; k < 5; ++k) m.reg[(int64_t)k * m.cap + i] = rg[k];
+            if (upd) {
+                const double invV = dt / (m.aexp * m.vol[li]);
+                double un[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) {
+                    const int64_t o = (int64_t)k * m.cap + i;
+                    if constexpr (STAGE == 1)
+                        un[k] = U0[o] - invV * acc[k];
+                    else
+                        un[k] = 0.5 * U0[o] + 0.5 * (Uin[o] - invV * acc[k]);
+                    Uout[o] = un[k];
+                }
+                if constexpr (STAGE == 2) {
+                    double W[5];
+                    cons2prim(un, m.gamma, W);
+                    const double c = sqrt(m.gamma * W[4] / W[0]);
+                    for (int d = 0; d < m.nd; ++d)
+                        invdt = nan_max(invdt, (fabs(W[1 + d]) + c) / m.w[li][d]);
+                }
+            }
+        }
+        if constexpr (STAGE == 1) {
+            if (!upd)
+#pragma unroll
+                for (int k = 0; k < 5; ++k) Uout[(int64_t)k * m.cap + i] = Uin[(int64_t)k * m.cap + i];
+        }
+    }
+    if constexpr (STAGE == 2)
+        if (a.cfl_all) block_max_to(&ctrl->invdt_bits, invdt, red);
+}
+
+// compute_dt(sim; level) maximum; level < 0: every leaf
+__global__ void __launch_bounds__(256) k_amr_cfl(AmrDev m, const double *__restrict__ U, int level,
+                                                 Ctrl *ctrl)
+{
+    __shared__ double red[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double invdt = 0.0;
+    if (i < m.nleaf && (level < 0 || m.lev[i] == level)) {
+        double W[5];
+        amr_prim(m, U, i, W);
+        const double c = sqrt(m.gamma * W[4] / W[0]);
+        for (int d = 0; d < m.nd; ++d)
+            invdt = nan_max(invdt, (fabs(W[1 + d]) + c) / m.w[m.lev[i]][d]);
+    }
+    block_max_to(&ctrl->invdt_bits, invdt, red);
+}
+
+// density_gradient_indicator (src/driver.jl:406-420) and the regrid! tag
+__global__ void __launch_bounds__(256) k_amr_tag(AmrDev m, const double *__restrict__ U,
+                                                 double above, int max_level, uint8_t *tag,
+                                                 double *ind)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nleaf) return;
+    double W[5], Wn[5];
+    amr_prim(m, U, i, W);
+    const double rc = W[0];
+    double g = 0.0;
+    for (int s = 0; s < 2 * m.nd; ++s) {
+        const int j = m.rep[s * m.cap + i];
+        if (j < 0) continue;
+        amr_prim(m, U, j, Wn);
+        const double rn = Wn[0];
+        g = fmax(g, fabs(rn - rc) / fmax(fmax(rc, rn), 2.220446049250313e-16));
+    }
+    if (ind) ind[i] = g;
+    tag[i] = (m.lev[i] < max_level && g > above) ? 1 : 0;
+}
+
+// new state from the old one after a regrid: every new leaf copies the cell
+// mean of the old leaf it came from (itself or its refined ancestor)
+__global__ void k_amr_prolong(int n, int64_t cap_old, int64_t cap_new, const int *__restrict__ src,
+                              const double *__restrict__ Uold, double *__restrict__ Unew)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = src[i];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) Unew[(int64_t)k * cap_new + i] = Uold[(int64_t)k * cap_old + s];
+}
+
+// _reflux_apply! (src/reflux.jl:91-101) for the leaves of one level
+__global__ void k_amr_reflux(AmrDev m, double *U, int level)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nleaf || m.lev[i] != level) return;
+    const double invV = 1.0 / m.vol[level];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int64_t o = (int64_t)k * m.cap + i;
+        U[o] = U[o] - invV * m.reg[o];
+        m.reg[o] = 0.0;
+    }
+}
+
+__global__ void k_amr_zero_reg(AmrDev m, int level)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nleaf || m.lev[i] != level) return;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) m.reg[(int64_t)k * m.cap + i] = 0.0;
+}
+
+// conserved_totals: fixed partition (deterministic), then one folding block
+__global__ void __launch_bounds__(256) k_amr_totals_part(AmrDev m, const double *__restrict__ U,
+                                                         double *partials)
+{
+    __shared__ double red[5][8];
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.nleaf; i += gridDim.x * blockDim.x) {
+        const double v = m.vol[m.lev[i]];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) s[k] += U[(int64_t)k * m.cap + i] * v;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const double v = warp_sum(s[k]);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double v = 0.0;
+        for (int w = 0; w < 8; ++w) v += red[threadIdx.x][w];
+        partials[blockIdx.x * 5 + threadIdx.x] = v;
+    }
+}
+
+}  // namespace
+
+static unsigned blocks(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs > 0 ? (n + bs - 1) / bs : 1); }
+
+int launch_amr_stage(const AmrDev &m, int stage, const double *Uin, const double *U0,
+                     double *Uout, double *F, const AmrStageArgs &a, Ctrl *ctrl, cudaStream_t s)
+{
+    if (m.nface > 0)
+        k_amr_faces<<<blocks(m.nface, 256), 256, 0, s>>>(m, Uin, F, a.dt < 0.0 ? ctrl : nullptr);
+    if (stage == 1)
+        k_amr_cells<1><<<blocks(m.nleaf, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
+    else
+        k_amr_cells<2><<<blocks(m.nleaf, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
+    return m.nface > 0 ? 2 : 1;
+}
+
+int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cudaStream_t s)
+{
+    k_amr_cfl<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, level, ctrl);
+    return 1;
+}
+
+int launch_amr_tag(const AmrDev &m, const double *U, double above, int max_level, uint8_t *tag,
+                   double *ind, cudaStream_t s)
+{
+    k_amr_tag<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, above, max_level, tag, ind);
+    return 1;
+}
+
+int launch_amr_prolong(int n, int64_t cap_old, int64_t cap_new, const int *src, const double *Uold,
+                       double *Unew, cudaStream_t s)
+{
+    if (n <= 0) return 0;
+    k_amr_prolong<<<blocks(n, 256), 256, 0, s>>>(n, cap_old, cap_new, src, Uold, Unew);
+    return 1;
+}
+
+int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s)
+{
+    k_amr_reflux<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, level);
+    return 1;
+}
+
+int launch_amr_zero_reg(const AmrDev &m, int level, cudaStream_t s)
+{
+    k_amr_zero_reg<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, level);
+    return 1;
+}
+
+int launch_amr_totals(const AmrDev &m, const double *U, double *partials, int npart, double *out,
+                      cudaStream_t s)
+{
+    k_amr_totals_part<<<npart, 256, 0, s>>>(m, U, partials);
+    return 1 + launch_totals_final(partials, npart, out, s);
+}
+
+}  // namespace vb

@@ -272,6 +272,12 @@ int launch_totals(const Geom &g, const double *U, double *partials, int npart, d
     return 2;
 }
 
+int launch_totals_final(const double *partials, int npart, double *out, cudaStream_t s)
+{
+    k_totals_final<<<1, 32, 0, s>>>(partials, npart, out);
+    return 1;
+}
+
 int launch_hllc_faces(int64_t nf, const double *WL, const double *WR, const int32_t *axis,
                       double gamma, double *F, cudaStream_t s)
 {

@@ -48,6 +48,8 @@ int launch_finalize_cfl(const Geom &g, Ctrl *ctrl, cudaStream_t s);
 int launch_set_dt(const Geom &g, Ctrl *ctrl, double dt, cudaStream_t s);
 int launch_totals(const Geom &g, const double *U, double *partials, int npart, double *out,
                   cudaStream_t s);
+// fold `npart` five-component partial sums in index order (one block)
+int launch_totals_final(const double *partials, int npart, double *out, cudaStream_t s);
 int launch_hllc_faces(int64_t nf, const double *WL, const double *WR, const int32_t *axis,
                       double gamma, double *F, cudaStream_t s);
 

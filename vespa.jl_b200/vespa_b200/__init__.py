@@ -6,6 +6,8 @@ reference's public names (Simulation, step!, evolve!, compute_dt,
 conserved_totals, compute_face_fluxes!).
 """
 from ._lib import Context, VespaB200Error, default_context, load
+from . import amr
+from .amr import AmrMesh, AmrSimulation, RefinementPolicy
 from .adjoint import Adjoint, EvolveFunction, evolve_with_adjoint, rho2_integral, rho2_seed
 from .flux import AbstractFluxBackend, B200Flux, compute_face_fluxes
 from .problem import (BC, IdealHydro, Outflow, Periodic, Problem, Reflecting, cons2prim,
@@ -18,6 +20,7 @@ from .simulation import (B200Mesh, Batch, Simulation, Totals, cell_samples, comp
 
 __all__ = [
     "Context", "VespaB200Error", "default_context", "load",
+    "amr", "AmrMesh", "AmrSimulation", "RefinementPolicy",
     "Adjoint", "EvolveFunction", "evolve_with_adjoint", "rho2_integral", "rho2_seed",
     "AbstractFluxBackend", "B200Flux", "compute_face_fluxes",
     "BC", "IdealHydro", "Outflow", "Periodic", "Problem", "Reflecting", "cons2prim",

@@ -100,6 +100,26 @@ SIGNATURES = {
     "vb_adjoint_backward": [_VP, _DP, _DP],
     "vb_adjoint_step": [_VP, C.c_double, _DP, _DP],
     "vb_adjoint_timing": [_VP, _DP],
+    "vb_amr_create": [_VP, C.POINTER(ProblemDesc), C.POINTER(_VP)],
+    "vb_amr_destroy": [_VP],
+    "vb_amr_nleaf": [_VP, _I64P],
+    "vb_amr_nface": [_VP, _I64P],
+    "vb_amr_leaves": [_VP, _I32P, _I64P],
+    "vb_amr_max_level": [_VP, _I32P],
+    "vb_amr_upload": [_VP, _DP],
+    "vb_amr_download": [_VP, _DP],
+    "vb_amr_set_time": [_VP, C.c_double, C.c_int64],
+    "vb_amr_get_time": [_VP, _DP, _I64P],
+    "vb_amr_refine": [_VP, _I64P, C.c_int64],
+    "vb_amr_indicator": [_VP, _DP],
+    "vb_amr_regrid": [_VP, C.c_double, C.c_int, _I64P],
+    "vb_amr_compute_dt": [_VP, C.c_int, _DP],
+    "vb_amr_step": [_VP, C.c_double],
+    "vb_amr_step_level": [_VP, C.c_double, C.c_int],
+    "vb_amr_evolve": [_VP, C.c_double, C.c_int64, C.c_double, C.c_int, C.c_int, C.c_int, _DP,
+                      _I64P],
+    "vb_amr_regrid_ms": [_VP, _DP],
+    "vb_amr_conserved_totals": [_VP, _DP],
 }
 
 _lib = None
