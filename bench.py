@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256, help="cells per axis of the cube")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plane", action="store_true",
+                    help="skip the 2D 4096^2 throughput run")
     ap.add_argument("--no-amr", action="store_true",
                     help="skip the Sedov 48^2 AMR run")
     ap.add_argument("--no-adjoint", action="store_true",
@@ -328,6 +330,7 @@ def run_ours(args, ranks: Ranks):
 
     adjoint = None if args.no_adjoint else adjoint_section(ctx, ranks)
     amr = None if args.no_amr else amr_section(ctx, ranks)
+    plane = None if args.no_plane else plane_section(ctx, ranks, K, W)
 
     cpu = None
     if ranks.world == 1 and ranks.rank == 0 and not args.no_cpu_baseline:
@@ -368,6 +371,8 @@ def run_ours(args, ranks: Ranks):
         line["adjoint"] = adjoint
     if amr:
         line["amr"] = amr
+    if plane:
+        line["plane2d"] = plane
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -446,6 +451,36 @@ def adjoint_section(ctx, ranks: Ranks, n=512, nsteps=200, every=20, fd_cells=32,
             "adj_step": "reverse sweep per step (segment recompute + two adjoint stages) "
                         "over the forward step (evolve!)",
             **res}
+
+
+def plane_section(ctx, ranks: Ranks, K: int, W: int, n=4096):
+    """2D 4096^2 periodic throughput (the reference's '2D uniform throughput
+    step' configuration, same generator as the cube), both precisions, tiled
+    2D kernel with the autotuned row chunk; K timed CFL steps after W warm-up."""
+    import vespa_b200 as vb
+    prob = vb.smooth_random_problem((n, n), seed=vb.problem.DEFAULT_SEED + ranks.rank)
+    U0 = vb.initial_state(prob)
+    mesh = vb.B200Mesh(prob.dims, prob.domain)
+    out = {"config": f"2D {n}^2 periodic, gamma 5/3, CFL 0.4, 5 float64 fields "
+                     "(z momentum stays 0), inputs larger than L2 (134 MB per buffer)"}
+    for prec in ("fp64", "mixed"):
+        sim = vb.Simulation(mesh, prob, precision=prec, ctx=ctx, initial=U0)
+        ky, _ = sim.autotune(3)
+        vb.run_steps_async(sim, W)
+        ctx.synchronize()
+        ranks.barrier()
+        ctx.mark(8)
+        vb.run_steps_async(sim, K)
+        ctx.mark(9)
+        ms = ranks.max(ctx.elapsed_ms(8, 9))
+        prof = sim.profile_step(3)
+        hbm, _ = measured_hbm()
+        s2 = 120 * n * n / (prof["ms_stage2"] / 1e3) / 1e9
+        out[prec] = {"value": round(n * n * ranks.world * K / (ms / 1e3) / 1e6, 1), "unit": UNIT,
+                     "ms_per_step": round(ms / K, 4), "kernel": sim.kernel, "row_chunk": ky,
+                     "stage2_hbm_frac": round(s2 / hbm, 4)}
+        sim.close()
+    return out
 
 
 def amr_section(ctx, ranks: Ranks, cpu_steps=60):

@@ -100,13 +100,23 @@ namespace detail {
 
 int encode_maps(vb::TiledMaps *m, const double *base, const vb::Geom &g)
 {
+    if (g.nd == 2) {  // 256-cell row segments and their 2-cell x halos
+        int rc = encode_state_map(&m->in_int, base, g, 256, 1);
+        if (!rc) rc = encode_state_map(&m->in_xs, base, g, 2, 1);
+        if (!rc) m->in_ys = m->in_xs;
+        return rc;
+    }
     int rc = encode_state_map(&m->in_int, base, g, 16, 16);
     if (!rc) rc = encode_state_map(&m->in_xs, base, g, 2, 16);
     if (!rc) rc = encode_state_map(&m->in_ys, base, g, 16, 2);
     return rc;
 }
 
-int default_kz(const vb::Geom &g) { return g.n[2] >= 64 ? 32 : (int)((g.n[2] + 1) / 2); }
+int default_kz(const vb::Geom &g)
+{
+    const int64_t n = vb::march_extent(g);
+    return n >= 64 ? 32 : (int)((n + 1) / 2);
+}
 
 // Geometry of a descriptor, validated as Problem is (src/problem.jl:39-46),
 // and RefMesh's derived widths, areas and volume (lib/RefMesh/src/RefMesh.jl:
@@ -180,14 +190,20 @@ vb::BoxDesc make_box(const vb::TiledMaps &mU, const vb::TiledMaps &mU1, const vb
     b.U1 = U1;
     b.ctrl = ctrl;
     b.kz = kz;
-    b.ntx = (int)(g.n[0] / 16);
-    b.ntiles = (int)((g.n[0] / 16) * (g.n[1] / 16));
+    if (g.nd == 2) {
+        b.ntx = (int)(g.n[0] / 256);
+        b.ntiles = b.ntx;
+    } else {
+        b.ntx = (int)(g.n[0] / 16);
+        b.ntiles = (int)((g.n[0] / 16) * (g.n[1] / 16));
+    }
     b.item0 = item0;
     return b;
 }
 
 int64_t box_items(const vb::Geom &g, int kz)
 {
+    if (g.nd == 2) return (g.n[0] / 256) * ((g.n[1] + kz - 1) / kz);
     return (g.n[0] / 16) * (g.n[1] / 16) * ((g.n[2] + kz - 1) / kz);
 }
 
@@ -218,6 +234,13 @@ int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout
         const int64_t items = box_items(gr->g, gr->kz);
         if (items > 0x7fffffff) return fail(VB_ENOTSUP, "too many tiled work items");
         unsigned int *work = gr->ctrl->work;  // device address of the cursors
+        if (gr->g.nd == 2) {
+            int n2 = gr->precision == VB_MIXED
+                         ? vb::launch_stage_tiled2d_mixed(&gr->box, (int)items, work, st, gr->ctx->stream)
+                         : vb::launch_stage_tiled2d_fp64(&gr->box, (int)items, work, st, gr->ctx->stream);
+            VB_CHECK_LAUNCH(gr->ctx, n2);
+            return VB_OK;
+        }
         int n = gr->precision == VB_MIXED
                     ? vb::launch_stage_tiled3d_mixed(&gr->box, nullptr, nullptr, (int)items, work,
                                                      st, gr->ctx->stream)
@@ -476,7 +499,7 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
         std::string m = g_err;
         return cleanup(rc, m);
     }
-    if (vb::tiled3d_supported(g)) {
+    if (vb::tiled_supported(g)) {
         rc = encode_maps(&gr->maps_U, gr->U, g);
         if (!rc) rc = encode_maps(&gr->maps_U1, gr->U1, g);
         if (rc) {
@@ -518,7 +541,7 @@ int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
     const int cand[] = {16, 24, 32, 48, 64, 96, 128};
     for (int kz : cand) {
         if (rc) break;
-        if (kz > gr->g.n[2]) continue;
+        if (kz > vb::march_extent(gr->g)) continue;
         gr->kz = kz;
         rc = ensure_cfl(gr);
         if (!rc) rc = queue_steps(gr, 1);  // warm-up
@@ -565,9 +588,10 @@ int vb_grid_set_option(vb_grid *gr, int option, int64_t value)
         if (value == VB_KERNEL_CELL) {
             gr->tiled = false;
         } else if (value == VB_KERNEL_AUTO || value == VB_KERNEL_TILED) {
-            if (!vb::tiled3d_supported(gr->g)) {
+            if (!vb::tiled_supported(gr->g)) {
                 if (value == VB_KERNEL_TILED)
-                    return fail(VB_ENOTSUP, "tiled kernel needs a 3D grid with nx, ny multiples of 16");
+                    return fail(VB_ENOTSUP, "tiled kernels need a 3D grid with nx, ny multiples of "
+                                            "16 or a 2D grid with nx a multiple of 256");
                 gr->tiled = false;
                 return VB_OK;
             }
@@ -582,7 +606,8 @@ int vb_grid_set_option(vb_grid *gr, int option, int64_t value)
         }
         return VB_OK;
     case VB_OPT_TILE_KZ:
-        if (value < 1 || value > gr->g.n[2]) return fail(VB_EINVAL, "kz must be in 1..nz");
+        if (value < 1 || value > vb::march_extent(gr->g))
+            return fail(VB_EINVAL, "the chunk must be in 1..nz (3D) or 1..ny (2D)");
         gr->kz = (int)value;
         return VB_OK;
     default:

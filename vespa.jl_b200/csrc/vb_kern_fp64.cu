@@ -9,6 +9,7 @@
 #include "vb_launch.h"
 #include "vb_stage_generic.cuh"
 #include "vb_stage_tiled3d.cuh"
+#include "vb_stage_tiled2d.cuh"
 
 namespace vb {
 
@@ -156,6 +157,12 @@ int launch_stage_fp64(const Geom &g, int stage, const double *Uin, const double 
     case 32: return launch_generic<3, 2>(g, Uin, U0, Uout, ctrl, bflux, s);
     default: return -1;
     }
+}
+
+int launch_stage_tiled2d_fp64(const BoxDesc *hbox, int nitems, unsigned int *work, int stage,
+                              cudaStream_t s)
+{
+    return launch_tiled2d<false, 2>(hbox, nitems, work, stage, s);
 }
 
 int launch_stage_tiled3d_fp64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,

@@ -4,6 +4,7 @@
 #include "vb_launch.h"
 #include "vb_stage_generic.cuh"
 #include "vb_stage_tiled3d_mixed.cuh"
+#include "vb_stage_tiled2d.cuh"
 
 namespace vb {
 
@@ -26,6 +27,12 @@ int launch_stage_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const 
                                int nitems, unsigned int *work, int stage, cudaStream_t s)
 {
     return launch_tiled3d_mixed<2>(hbox, boxes, item_box, nitems, work, stage, s);
+}
+
+int launch_stage_tiled2d_mixed(const BoxDesc *hbox, int nitems, unsigned int *work, int stage,
+                               cudaStream_t s)
+{
+    return launch_tiled2d<true, 2>(hbox, nitems, work, stage, s);
 }
 
 int launch_stage_mixed(const Geom &g, int stage, const double *Uin, const double *U0,

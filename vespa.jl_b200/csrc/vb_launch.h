@@ -40,6 +40,16 @@ inline bool tiled3d_supported(const Geom &g)
            g.n[0] <= (1 << 30) && g.n[1] <= (1 << 30) && g.n[2] <= (1 << 30);
 }
 
+// Tiled 2D path applicability: 256-cell row segments marching y.
+inline bool tiled2d_supported(const Geom &g)
+{
+    return g.nd == 2 && g.n[0] % 256 == 0 && g.n[1] >= 2 && g.n[0] <= (1 << 30) &&
+           g.n[1] <= (1 << 30);
+}
+inline bool tiled_supported(const Geom &g) { return tiled3d_supported(g) || tiled2d_supported(g); }
+// cells along the marching axis (z in 3D, y in 2D)
+inline int64_t march_extent(const Geom &g) { return g.nd == 3 ? g.n[2] : g.n[1]; }
+
 // vb_kern_fp64.cu (compiled with -fmad=false)
 int launch_stage_fp64(const Geom &g, int stage, const double *Uin, const double *U0,
                       double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s);
@@ -58,6 +68,11 @@ int launch_hllc_faces(int64_t nf, const double *WL, const double *WR, const int3
 // its box.  `work` holds the two stage cursors (reset by the dt kernels).
 int launch_stage_tiled3d_fp64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
                               int nitems, unsigned int *work, int stage, cudaStream_t s);
+// Tiled 2D stage (single box by value).
+int launch_stage_tiled2d_fp64(const BoxDesc *hbox, int nitems, unsigned int *work, int stage,
+                              cudaStream_t s);
+int launch_stage_tiled2d_mixed(const BoxDesc *hbox, int nitems, unsigned int *work, int stage,
+                               cudaStream_t s);
 // Per-box dt finalisation (evolve!'s loop head) and clock advance for a table.
 int launch_finalize_boxes(const BoxDesc *boxes, int nbox, unsigned int *work, cudaStream_t s);
 int launch_advance_boxes(const BoxDesc *boxes, int nbox, cudaStream_t s);

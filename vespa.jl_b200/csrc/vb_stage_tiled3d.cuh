@@ -36,6 +36,10 @@ constexpr int U_XHI = U_XLO + 2 * TY * 5;
 constexpr int U_YLO = U_XHI + 2 * TY * 5;
 constexpr int U_YHI = U_YLO + 2 * TX * 5;
 constexpr uint32_t PLANE_BYTES = UPLANE * 8;
+// every TMA destination in shared memory is 128-byte aligned
+static_assert((U_XLO * 8) % 128 == 0 && (U_XHI * 8) % 128 == 0 && (U_YLO * 8) % 128 == 0 &&
+                  (U_YHI * 8) % 128 == 0 && (UPLANE * 8) % 128 == 0,
+              "TMA destinations must be 128-byte aligned");
 
 // halo index -> staged-plane offset of field 0 (add f * region field stride)
 __device__ __forceinline__ int halo_uoff(int h, int f)
@@ -101,6 +105,16 @@ __device__ __forceinline__ double cfl_term_exact(const double un[5], const Geom 
     m = nan_max(m, (fabs(W[1]) + cs) / g.w[0]);
     m = nan_max(m, (fabs(W[2]) + cs) / g.w[1]);
     return nan_max(m, (fabs(W[3]) + cs) / g.w[2]);
+}
+
+// The same over x and y only (2D grids: compute_dt loops d in 1:N)
+__device__ __forceinline__ double cfl_term2d_exact(const double un[5], const Geom &g, double m)
+{
+    double W[5];
+    cons2prim(un, g.gamma, W);
+    const double cs = sound_speed(W, g.gamma);
+    m = nan_max(m, (fabs(W[1]) + cs) / g.w[0]);
+    return nan_max(m, (fabs(W[2]) + cs) / g.w[1]);
 }
 
 // Persistent: a grid of (2 x SMs) blocks pulls work items from work[STAGE-1].

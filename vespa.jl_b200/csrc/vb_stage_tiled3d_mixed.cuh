@@ -100,6 +100,16 @@ __device__ __forceinline__ double cfl_term(const double un[5], const Geom &g, do
     return nan_max(m, (double)t);
 }
 
+// the same over x and y only (2D grids)
+__device__ __forceinline__ double cfl_term2d(const double un[5], const Geom &g, double m)
+{
+    float W[5];
+    cons2prim_mixed(un, g.gamma, W);
+    const float cs = sqrt_approx((float)g.gamma * W[4] * rcp_approx(W[0]));
+    const float t = fmaxf((fabsf(W[1]) + cs) * (float)g.invw[0], (fabsf(W[2]) + cs) * (float)g.invw[1]);
+    return nan_max(m, (double)t);
+}
+
 }  // namespace t3m
 
 template <int NS, int STAGE, bool BATCH>
