@@ -58,41 +58,58 @@ def parse():
 
 # ----------------------------------------------------------------- ranks
 class Ranks:
-    def __init__(self, n_gpus: int):
+    """One process per GPU (torchrun env vars).  NCCL on GPUs; gloo (CPU
+    tensors) when no GPU is present, which the multi-rank host tests use."""
+
+    def __init__(self, n_gpus: int, backend: str | None = None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.dist = None
+        self.device = "cpu"
         if self.world > 1:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.device = f"cuda:{self.local}"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
             self.dist = dist
             self.torch = torch
 
     def barrier(self):
         if self.dist:
-            self.dist.barrier(device_ids=[self.local])
+            if self.device == "cpu":
+                self.dist.barrier()
+            else:
+                self.dist.barrier(device_ids=[self.local])
 
     def max(self, x: float) -> float:
         if not self.dist:
             return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
     def sum(self, x: float) -> float:
         if not self.dist:
             return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t)
         return float(t.item())
 
     def close(self):
         if self.dist:
             self.dist.destroy_process_group()
+
+
+def weak_scaling_value(cells_per_rank: int, world: int, steps: int, ms_max: float) -> float:
+    """Whole-job Mcell-updates/s: all ranks' cells x steps over the slowest
+    rank's device time."""
+    return cells_per_rank * world * steps / (ms_max / 1e3) / 1e6
 
 
 # ----------------------------------------------------------------- clocks
@@ -315,8 +332,8 @@ def run_ours(args, ranks: Ranks):
     hbm, hbm_kind = measured_hbm()
     mixed = out["mixed"]
     total_cells = cells * ranks.world
-    value = total_cells * K / (mixed["ms"] / 1e3) / 1e6
-    fp64_value = total_cells * K / (out["fp64"]["ms"] / 1e3) / 1e6
+    value = weak_scaling_value(cells, ranks.world, K, mixed["ms"])
+    fp64_value = weak_scaling_value(cells, ranks.world, K, out["fp64"]["ms"])
 
     def roofline(d, kname):
         bytes_launch = BYTES_PER_CELL_STAGE[2] * cells
