@@ -1,24 +1,23 @@
 // vb_amr.cu -- the extern "C" AMR API: a composite leaf-only mesh over a base
 // grid (lib/HGBackend/src/HGBackend.jl), its regrid (src/driver.jl:400-462)
 // and the single-rate and subcycled drivers (src/driver.jl:483-605,
-// src/reflux.jl:51-103), with the stepping on the device.
+// src/reflux.jl:51-103).
 //
-// Host side: the cell tree (leaves keyed by level and integer coordinates),
-// 2:1 face balance on refinement, depth-first leaf order, and the tables the
-// kernels read (representative neighbours, faces in emission order, per-leaf
-// CSR of face contributions).  The tables are rebuilt after each regrid;
-// between regrids every step runs on the device.
+// Everything that touches leaves runs on the device: the stage kernels
+// (vb_amr_kern.cu) and the topology work of a regrid -- tags, 2:1 balance,
+// in-place children, the leaf hash, neighbour kinds, faces in emission order
+// and the per-leaf CSR (vb_amr_regrid.cu).  The host keeps the counts, the
+// clock and the driver loops; it reads a few words back per regrid.
 //
 // Choices where the reference defers to HierarchicalGrids.jl (absent here):
 // the base grid is a forest of roots in column-major order, children are
 // ordered x fastest (x + 2y + 4z), the representative of a face with finer
 // leaves is the first of them in that order, and balance is across faces.
-#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstring>
 #include <new>
-#include <unordered_map>
+#include <utility>
 #include <vector>
 
 #include "vb_amr.h"
@@ -28,165 +27,48 @@ using vb::detail::fail;
 using vb::detail::use;
 
 namespace {
-
 constexpr int CBITS = 20;  // bits per integer coordinate in a leaf key
-
-struct Tree {
-    int nd = 1;
-    int64_t base[3] = {1, 1, 1};
-    int bc_lo[3] = {0, 0, 0}, bc_hi[3] = {0, 0, 0};
-    std::vector<int> lev;
-    std::vector<int64_t> cx;  // 3 per leaf
-    std::unordered_map<uint64_t, int> index;
-
-    static uint64_t key(int l, const int64_t *c)
-    {
-        return ((uint64_t)l << 60) | ((uint64_t)c[0] << 40) | ((uint64_t)c[1] << 20) | (uint64_t)c[2];
-    }
-    int find(int l, const int64_t *c) const
-    {
-        auto it = index.find(key(l, c));
-        return it == index.end() ? -1 : it->second;
-    }
-    int64_t n() const { return (int64_t)lev.size(); }
-
-    uint64_t dfs_key(int l, const int64_t *c) const
-    {
-        uint64_t root = 0, mul = 1;
-        for (int d = 0; d < nd; ++d) {
-            root += (uint64_t)(c[d] >> l) * mul;
-            mul *= (uint64_t)base[d];
-        }
-        uint64_t path = 0;
-        for (int k = vb::AMR_MAX_LEVEL - 1; k >= 0; --k) {
-            uint64_t digit = 0;
-            for (int d = 0; d < nd; ++d) {
-                const uint64_t s = (uint64_t)(c[d] & ((1LL << l) - 1)) << (vb::AMR_MAX_LEVEL - l);
-                digit |= ((s >> k) & 1u) << d;
-            }
-            path = (path << nd) | digit;
-        }
-        return (root << (nd * vb::AMR_MAX_LEVEL)) | path;
-    }
-
-    // adjacent same-level coordinates across (d, hi); false at a non-periodic edge
-    bool adjacent(int l, const int64_t *c, int d, bool hi, int64_t *cc) const
-    {
-        cc[0] = c[0];
-        cc[1] = c[1];
-        cc[2] = c[2];
-        const int64_t nmax = base[d] << l;
-        cc[d] += hi ? 1 : -1;
-        if (cc[d] < 0 || cc[d] >= nmax) {
-            if ((hi ? bc_hi[d] : bc_lo[d]) != vb::BC_PERIODIC) return false;
-            cc[d] = (cc[d] + nmax) % nmax;
-        }
-        return true;
-    }
-
-    // 0 boundary, 1 same level, 2 coarser, 3 finer; *rep representative
-    int neighbor(int i, int d, bool hi, int *rep) const
-    {
-        const int l = lev[i];
-        int64_t cc[3];
-        if (!adjacent(l, &cx[3 * i], d, hi, cc)) return 0;
-        int j = find(l, cc);
-        if (j >= 0) { *rep = j; return 1; }
-        if (l > 0) {
-            const int64_t cp[3] = {cc[0] >> 1, cc[1] >> 1, cc[2] >> 1};
-            j = find(l - 1, cp);
-            if (j >= 0) { *rep = j; return 2; }
-        }
-        int64_t cf[3] = {2 * cc[0], 2 * cc[1], 2 * cc[2]};
-        if (!hi) cf[d] += 1;
-        *rep = find(l + 1, cf);
-        return 3;
-    }
-};
-
-// One refinement batch: live cells keyed by coordinates, each remembering the
-// pre-batch leaf whose cell mean it inherits.
-struct Batch {
-    const Tree &t;
-    std::unordered_map<uint64_t, int> live;  // key -> slot
-    std::vector<int> lev;
-    std::vector<int64_t> cx;
-    std::vector<int> src;
-    std::vector<char> dead;
-    int err = 0;
-
-    explicit Batch(const Tree &tree) : t(tree)
-    {
-        const int64_t n = t.n();
-        lev = t.lev;
-        cx = t.cx;
-        src.resize(n);
-        dead.assign(n, 0);
-        for (int64_t i = 0; i < n; ++i) {
-            src[i] = (int)i;
-            live[Tree::key(lev[i], &cx[3 * i])] = (int)i;
-        }
-    }
-    int get(int l, const int64_t *c) const
-    {
-        auto it = live.find(Tree::key(l, c));
-        return it == live.end() ? -1 : it->second;
-    }
-    // refine (l, c) after refining coarser face neighbours (2:1 balance)
-    void refine(int l, const int64_t *c)
-    {
-        if (get(l, c) < 0) return;
-        for (int d = 0; d < t.nd; ++d)
-            for (int hi = 0; hi < 2; ++hi) {
-                int64_t cc[3];
-                if (l == 0 || !t.adjacent(l, c, d, hi, cc)) continue;
-                if (get(l, cc) >= 0) continue;
-                const int64_t cp[3] = {cc[0] >> 1, cc[1] >> 1, cc[2] >> 1};
-                if (get(l - 1, cp) >= 0) refine(l - 1, cp);
-            }
-        const int s = get(l, c);
-        if (s < 0) return;
-        for (int d = 0; d < t.nd; ++d)
-            if ((t.base[d] << (l + 1)) >= (1LL << CBITS)) err = 1;
-        if (l + 1 > vb::AMR_MAX_LEVEL) err = 1;
-        if (err) return;
-        live.erase(Tree::key(l, c));
-        dead[s] = 1;
-        const int nch = 1 << t.nd;
-        for (int ch = 0; ch < nch; ++ch) {
-            int64_t k[3] = {0, 0, 0};
-            for (int d = 0; d < t.nd; ++d) k[d] = 2 * c[d] + ((ch >> d) & 1);
-            const int slot = (int)lev.size();
-            lev.push_back(l + 1);
-            cx.insert(cx.end(), k, k + 3);
-            src.push_back(src[s]);
-            dead.push_back(0);
-            live[Tree::key(l + 1, k)] = slot;
-        }
-    }
-};
-
 }  // namespace
 
 struct vb_amr {
     vb_ctx *ctx = nullptr;
     vb::Geom g{};  // base geometry: nd, bcs, gamma, cfl, aexp (cells per axis = base)
-    Tree tree;
+    int nd = 1;
+    int64_t base[3] = {1, 1, 1};
     double w0[3] = {1, 1, 1};
     double t = 0.0;
     int64_t step = 0;
-    // device buffers
-    int64_t cap = 0, fcap = 0, ecap = 0;
-    double *U = nullptr, *U1 = nullptr, *F = nullptr, *reg = nullptr;
-    int *lev = nullptr, *rep = nullptr, *fL = nullptr, *fR = nullptr, *off = nullptr, *ent = nullptr;
-    int8_t *fax = nullptr;
-    double *farea = nullptr;
+    int n = 0;          // leaves
+    int maxlev = 0;     // deepest leaf level
+    int nface = 0, nent = 0;
+    // leaf-indexed device buffers (stride cap)
+    int64_t cap = 0;
+    double *U = nullptr, *U1 = nullptr, *reg = nullptr;
+    int *lev = nullptr, *cx = nullptr;          // level, [3][cap] coordinates
+    double *U2 = nullptr;                       // refinement targets, swapped in
+    int *lev2 = nullptr, *cx2 = nullptr;
+    int *rep = nullptr, *faceid = nullptr;      // [6][cap]
+    int8_t *kind = nullptr;                     // [6][cap]
+    int *off = nullptr, *fbase = nullptr;       // cap + 1
+    int *cnt = nullptr, *fcnt = nullptr, *ecnt = nullptr;
+    int *bsum = nullptr;                        // scan block sums
     uint8_t *tag = nullptr;
+    // face-indexed (stride fcap) and CSR
+    int64_t fcap = 0, ecap = 0;
+    double *F = nullptr, *farea = nullptr;
+    int *fL = nullptr, *fR = nullptr, *ent = nullptr;
+    int8_t *fax = nullptr;
+    // hash of (level, coordinates) -> leaf
+    int64_t hcap = 0;
+    uint64_t *hkey = nullptr;
+    int *hval = nullptr;
+    // small device words: [0] error bits, [1] changed, [2] max level, [3] scan total, [4] tags
+    int *word = nullptr, *hword = nullptr;
     vb::Ctrl *ctrl = nullptr, *hctrl = nullptr;
     double *partials = nullptr, *totals = nullptr, *htot = nullptr;
-    int nface = 0;
     vb::AmrDev dev{};
-    double ms_regrid = 0.0;  // host wall time of the last evolve's regrids
+    vb::AmrAreas areas{};
+    double ms_regrid = 0.0;
 };
 
 namespace {
@@ -195,22 +77,12 @@ double level_width(const vb_amr *a, int l, int d) { return a->w0[d] * std::ldexp
 
 void release(vb_amr *a)
 {
-    cudaFree(a->U);
-    cudaFree(a->U1);
-    cudaFree(a->F);
-    cudaFree(a->reg);
-    cudaFree(a->lev);
-    cudaFree(a->rep);
-    cudaFree(a->fL);
-    cudaFree(a->fR);
-    cudaFree(a->off);
-    cudaFree(a->ent);
-    cudaFree(a->fax);
-    cudaFree(a->farea);
-    cudaFree(a->tag);
-    cudaFree(a->ctrl);
-    cudaFree(a->partials);
-    cudaFree(a->totals);
+    void *p[] = {a->U, a->U1, a->U2, a->lev2, a->cx2, a->reg, a->lev, a->cx, a->rep, a->faceid, a->kind, a->off,
+                 a->fbase, a->cnt, a->fcnt, a->ecnt, a->bsum, a->tag, a->F, a->farea,
+                 a->fL, a->fR, a->ent, a->fax, a->hkey, a->hval, a->word, a->ctrl,
+                 a->partials, a->totals};
+    for (void *q : p) cudaFree(q);
+    cudaFreeHost(a->hword);
     cudaFreeHost(a->hctrl);
     cudaFreeHost(a->htot);
 }
@@ -224,54 +96,82 @@ int realloc_dev(T **p, int64_t count)
     return VB_OK;
 }
 
-// Build the kernels' tables from the tree and upload them.
+// Leaf buffers other than U, lev and cx (which a refinement replaces itself).
+int alloc_leaf_buffers(vb_amr *a, int64_t c)
+{
+    int rc = realloc_dev(&a->U1, 5 * c);
+    if (!rc) rc = realloc_dev(&a->U2, 5 * c);
+    if (!rc) rc = realloc_dev(&a->lev2, c);
+    if (!rc) rc = realloc_dev(&a->cx2, 3 * c);
+    if (!rc) rc = realloc_dev(&a->reg, 5 * c);
+    if (!rc) rc = realloc_dev(&a->rep, 6 * c);
+    if (!rc) rc = realloc_dev(&a->faceid, 6 * c);
+    if (!rc) rc = realloc_dev(&a->kind, 6 * c);
+    if (!rc) rc = realloc_dev(&a->off, c + 1);
+    if (!rc) rc = realloc_dev(&a->fbase, c + 1);
+    if (!rc) rc = realloc_dev(&a->cnt, c);
+    if (!rc) rc = realloc_dev(&a->fcnt, c);
+    if (!rc) rc = realloc_dev(&a->ecnt, c);
+    if (!rc) rc = realloc_dev(&a->bsum, c / 1024 + 2);
+    if (!rc) rc = realloc_dev(&a->tag, c);
+    if (rc) return rc;
+    VB_CUDA(cudaMemsetAsync(a->reg, 0, sizeof(double) * 5 * c, a->ctx->stream));
+    a->cap = c;
+    return VB_OK;
+}
+
+int sync_words(vb_amr *a)
+{
+    VB_CUDA(cudaMemcpyAsync(a->hword, a->word, sizeof(int) * 8, cudaMemcpyDeviceToHost,
+                            a->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(a->ctx->stream));
+    return VB_OK;
+}
+
+vb::AmrTopo topo(const vb_amr *a)
+{
+    vb::AmrTopo t{};
+    t.nd = a->nd;
+    for (int d = 0; d < 3; ++d) {
+        t.base[d] = a->base[d];
+        t.bc_lo[d] = a->g.bc_lo[d];
+        t.bc_hi[d] = a->g.bc_hi[d];
+    }
+    t.n = a->n;
+    t.cap = a->cap;
+    t.lev = a->lev;
+    t.cx = a->cx;
+    t.hkey = a->hkey;
+    t.hval = a->hval;
+    t.hmask = (uint64_t)a->hcap - 1;
+    return t;
+}
+
+// Rebuild the hash and every table from (lev, cx) of the current leaves.
 int build_tables(vb_amr *a)
 {
-    const Tree &t = a->tree;
-    const int n = (int)t.n(), nd = t.nd;
-    std::vector<int> rep((size_t)6 * a->cap, -1);
-    std::vector<int> fL, fR;
-    std::vector<int8_t> fax;
-    std::vector<double> farea;
-    std::vector<std::vector<int>> lists((size_t)n);
-    auto emit = [&](int L, int R, int d, double area) {
-        const int f = (int)fL.size();
-        fL.push_back(L);
-        fR.push_back(R);
-        fax.push_back((int8_t)d);
-        farea.push_back(area);
-        if (L >= 0) lists[L].push_back(2 * f);
-        if (R >= 0) lists[R].push_back(2 * f + 1);
-    };
-    for (int i = 0; i < n; ++i) {
-        const int li = t.lev[i];
-        for (int d = 0; d < nd; ++d) {
-            for (int hi = 0; hi < 2; ++hi) {
-                int j = -1;
-                if (t.neighbor(i, d, hi, &j)) rep[(size_t)(2 * d + hi) * a->cap + i] = j;
-            }
-            double area = 1.0;
-            for (int e = 0; e < nd; ++e)
-                if (e != d) area = area * level_width(a, li, e);
-            int j = -1;
-            int kind = t.neighbor(i, d, true, &j);
-            if (kind == 0) emit(i, -1, d, area);
-            else if (kind != 3) emit(i, j, d, area);
-            kind = t.neighbor(i, d, false, &j);
-            if (kind == 0) emit(-1, i, d, area);
-            else if (kind == 2) emit(j, i, d, area);
-        }
+    cudaStream_t s = a->ctx->stream;
+    int64_t hc = 1024;
+    while (hc < 2 * (int64_t)a->n) hc *= 2;
+    if (hc != a->hcap) {
+        int rc = realloc_dev(&a->hkey, hc);
+        if (!rc) rc = realloc_dev(&a->hval, hc);
+        if (rc) return rc;
+        a->hcap = hc;
     }
-    std::vector<int> off((size_t)n + 1, 0), ent;
-    for (int i = 0; i < n; ++i) {
-        off[i + 1] = off[i] + (int)lists[i].size();
-        ent.insert(ent.end(), lists[i].begin(), lists[i].end());
-    }
-    const int nf = (int)fL.size();
+    VB_CUDA(cudaMemsetAsync(a->word, 0, sizeof(int) * 8, s));
+    vb::AmrTopo t = topo(a);
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_hash_build(t, a->hkey, a->hval, a->word, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_kinds(t, a->kind, a->rep, a->fcnt, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->fcnt, a->n, a->fbase, a->bsum, a->word + 3, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_csr_count(t, a->kind, a->fcnt, a->ecnt, s));
+    int rc = sync_words(a);
+    if (rc) return rc;
+    const int nf = a->hword[3];
     if (nf > a->fcap) {
-        int64_t c = a->fcap ? a->fcap : 1024;
+        int64_t c = a->fcap ? a->fcap : 4096;
         while (c < nf) c *= 2;
-        int rc = realloc_dev(&a->fL, c);
+        rc = realloc_dev(&a->fL, c);
         if (!rc) rc = realloc_dev(&a->fR, c);
         if (!rc) rc = realloc_dev(&a->fax, c);
         if (!rc) rc = realloc_dev(&a->farea, c);
@@ -279,29 +179,28 @@ int build_tables(vb_amr *a)
         if (rc) return rc;
         a->fcap = c;
     }
-    if ((int64_t)ent.size() > a->ecap) {
-        int64_t c = a->ecap ? a->ecap : 4096;
-        while (c < (int64_t)ent.size()) c *= 2;
-        int rc = realloc_dev(&a->ent, c);
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_faces(t, a->kind, a->rep, a->fbase, a->areas, a->fL,
+                                                 a->fR, a->fax, a->farea, a->faceid, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->ecnt, a->n, a->off, a->bsum, a->word + 3, s));
+    rc = sync_words(a);
+    if (rc) return rc;
+    const int ne = a->hword[3];
+    if (ne > a->ecap) {
+        int64_t c = a->ecap ? a->ecap : 8192;
+        while (c < ne) c *= 2;
+        rc = realloc_dev(&a->ent, c);
         if (rc) return rc;
         a->ecap = c;
     }
-    cudaStream_t s = a->ctx->stream;
-    VB_CUDA(cudaMemcpyAsync(a->lev, t.lev.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-    VB_CUDA(cudaMemcpyAsync(a->rep, rep.data(), sizeof(int) * rep.size(), cudaMemcpyHostToDevice, s));
-    if (nf) {
-        VB_CUDA(cudaMemcpyAsync(a->fL, fL.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s));
-        VB_CUDA(cudaMemcpyAsync(a->fR, fR.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, s));
-        VB_CUDA(cudaMemcpyAsync(a->fax, fax.data(), sizeof(int8_t) * nf, cudaMemcpyHostToDevice, s));
-        VB_CUDA(cudaMemcpyAsync(a->farea, farea.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s));
-    }
-    VB_CUDA(cudaMemcpyAsync(a->off, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
-    if (!ent.empty())
-        VB_CUDA(cudaMemcpyAsync(a->ent, ent.data(), sizeof(int) * ent.size(), cudaMemcpyHostToDevice, s));
-    VB_CUDA(cudaStreamSynchronize(s));  // the host vectors die here
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_csr_fill(t, a->kind, a->rep, a->faceid, a->off,
+                                                    a->ent, a->word, s));
+    rc = sync_words(a);
+    if (rc) return rc;
+    if (a->hword[0]) return fail(VB_ECUDA, "AMR table build failed (hash or CSR overflow)");
     a->nface = nf;
+    a->nent = ne;
     vb::AmrDev &m = a->dev;
-    m.nd = nd;
+    m.nd = a->nd;
     for (int d = 0; d < 3; ++d) {
         m.bc_lo[d] = a->g.bc_lo[d];
         m.bc_hi[d] = a->g.bc_hi[d];
@@ -310,7 +209,7 @@ int build_tables(vb_amr *a)
     m.aexp = a->g.aexp;
     m.cap = a->cap;
     m.fcap = a->fcap;
-    m.nleaf = n;
+    m.nleaf = a->n;
     m.nface = nf;
     m.lev = a->lev;
     m.rep = a->rep;
@@ -321,28 +220,74 @@ int build_tables(vb_amr *a)
     m.off = a->off;
     m.ent = a->ent;
     m.reg = a->reg;
-    for (int l = 0; l <= vb::AMR_MAX_LEVEL; ++l) {
-        double v = 1.0;
-        for (int d = 0; d < 3; ++d) m.w[l][d] = d < nd ? level_width(a, l, d) : 1.0;
-        for (int d = 0; d < nd; ++d) v = v * m.w[l][d];
-        m.vol[l] = v;
-    }
     return VB_OK;
 }
 
-// (Re)allocate the leaf-indexed buffers other than the state for `c` leaves.
-int alloc_leaf_buffers(vb_amr *a, int64_t c)
+// Refine the leaves marked in a->tag (with 2:1 balance), remap the state and
+// rebuild the tables.
+int refine_marked(vb_amr *a)
 {
-    int rc = realloc_dev(&a->U1, 5 * c);
-    if (!rc) rc = realloc_dev(&a->reg, 5 * c);
-    if (!rc) rc = realloc_dev(&a->lev, c);
-    if (!rc) rc = realloc_dev(&a->rep, 6 * c);
-    if (!rc) rc = realloc_dev(&a->off, c + 1);
-    if (!rc) rc = realloc_dev(&a->tag, c);
+    cudaStream_t s = a->ctx->stream;
+    vb::AmrTopo t = topo(a);
+    for (int round = 0;; ++round) {
+        if (round > 2 * vb::AMR_MAX_LEVEL + 4) return fail(VB_ECUDA, "AMR balance did not converge");
+        VB_CUDA(cudaMemsetAsync(a->word + 1, 0, sizeof(int), s));
+        VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_balance(t, a->tag, a->word + 1, s));
+        int rc = sync_words(a);
+        if (rc) return rc;
+        if (!a->hword[1]) break;
+    }
+    VB_CUDA(cudaMemsetAsync(a->word + 2, 0, sizeof(int), s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_count_children(t, a->tag, a->cnt, a->word + 2, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->cnt, a->n, a->fbase, a->bsum, a->word + 3, s));
+    int rc = sync_words(a);
     if (rc) return rc;
-    VB_CUDA(cudaMemsetAsync(a->reg, 0, sizeof(double) * 5 * c, a->ctx->stream));
-    a->cap = c;
-    return VB_OK;
+    const int64_t n_new = a->hword[3];
+    const int maxlev = a->hword[2];
+    if (n_new == a->n) return VB_OK;  // nothing refined
+    if (maxlev > vb::AMR_MAX_LEVEL) return fail(VB_ENOTSUP, "refinement beyond the supported depth");
+    for (int d = 0; d < a->nd; ++d)
+        if ((a->base[d] << maxlev) >= (1LL << CBITS))
+            return fail(VB_ENOTSUP, "refinement beyond the supported coordinate range");
+    if (n_new > INT_MAX / 8) return fail(VB_ENOTSUP, "too many leaves");
+    int64_t cap_new = a->cap;
+    while (cap_new < n_new) cap_new *= 2;
+    if (cap_new > a->cap) {
+        // grow: fresh targets of the new capacity; the other leaf buffers follow
+        double *Unew = nullptr;
+        int *lev_new = nullptr, *cx_new = nullptr;
+        cudaError_t e = cudaMalloc(&Unew, sizeof(double) * 5 * cap_new);
+        if (e == cudaSuccess) e = cudaMalloc(&lev_new, sizeof(int) * cap_new);
+        if (e == cudaSuccess) e = cudaMalloc(&cx_new, sizeof(int) * 3 * cap_new);
+        if (e == cudaSuccess) e = cudaMemsetAsync(cx_new, 0, sizeof(int) * 3 * cap_new, s);
+        if (e != cudaSuccess) {
+            cudaFree(Unew);
+            cudaFree(lev_new);
+            cudaFree(cx_new);
+            return fail(VB_ENOMEM, std::string("regrid buffers: ") + cudaGetErrorString(e));
+        }
+        VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_emit(t, a->tag, a->fbase, lev_new, cx_new, cap_new,
+                                                    a->U, Unew, s));
+        VB_CUDA(cudaStreamSynchronize(s));
+        cudaFree(a->U);
+        cudaFree(a->lev);
+        cudaFree(a->cx);
+        a->U = Unew;
+        a->lev = lev_new;
+        a->cx = cx_new;
+        rc = alloc_leaf_buffers(a, cap_new);
+        if (rc) return rc;
+    } else {
+        // same capacity: emit into the spare buffers and swap
+        VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_emit(t, a->tag, a->fbase, a->lev2, a->cx2, a->cap,
+                                                    a->U, a->U2, s));
+        std::swap(a->U, a->U2);
+        std::swap(a->lev, a->lev2);
+        std::swap(a->cx, a->cx2);
+    }
+    a->n = (int)n_new;
+    a->maxlev = maxlev;
+    return build_tables(a);
 }
 
 int pull_ctrl(vb_amr *a)
@@ -359,69 +304,6 @@ int push_ctrl(vb_amr *a)
                             a->ctx->stream));
     VB_CUDA(cudaStreamSynchronize(a->ctx->stream));
     return VB_OK;
-}
-
-// Refine the given leaves (with balance), remap the state and rebuild tables.
-int refine_leaves(vb_amr *a, const std::vector<int> &which)
-{
-    if (which.empty()) return VB_OK;
-    Tree &t = a->tree;
-    Batch b(t);
-    for (int i : which) {
-        const int l = t.lev[i];
-        const int64_t c[3] = {t.cx[3 * i], t.cx[3 * i + 1], t.cx[3 * i + 2]};
-        b.refine(l, c);
-        if (b.err) return fail(VB_ENOTSUP, "refinement beyond the supported depth");
-    }
-    // depth-first order of the live cells
-    std::vector<std::pair<uint64_t, int>> order;
-    order.reserve(b.live.size());
-    for (size_t s = 0; s < b.lev.size(); ++s)
-        if (!b.dead[s]) order.emplace_back(t.dfs_key(b.lev[s], &b.cx[3 * s]), (int)s);
-    std::sort(order.begin(), order.end());
-    const int64_t n = (int64_t)order.size();
-    std::vector<int> lev(n), src(n);
-    std::vector<int64_t> cx(3 * n);
-    for (int64_t k = 0; k < n; ++k) {
-        const int s = order[k].second;
-        lev[k] = b.lev[s];
-        std::memcpy(&cx[3 * k], &b.cx[3 * s], 3 * sizeof(int64_t));
-        src[k] = b.src[s];
-    }
-    cudaStream_t st = a->ctx->stream;
-    // remap the cell means into a buffer of the new capacity
-    int64_t cap_new = a->cap;
-    while (cap_new < n) cap_new *= 2;
-    double *Unew = nullptr;
-    int *dsrc = nullptr;
-    VB_CUDA(cudaMalloc(&Unew, sizeof(double) * 5 * cap_new));
-    cudaError_t e = cudaMalloc(&dsrc, sizeof(int) * n);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(dsrc, src.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) {
-        cudaFree(Unew);
-        cudaFree(dsrc);
-        return fail(VB_ECUDA, std::string("regrid remap: ") + cudaGetErrorString(e));
-    }
-    int nl = vb::launch_amr_prolong((int)n, a->cap, cap_new, dsrc, a->U, Unew, st);
-    a->ctx->launches += nl;
-    e = cudaStreamSynchronize(st);
-    cudaFree(dsrc);
-    if (e != cudaSuccess) {
-        cudaFree(Unew);
-        return fail(VB_ECUDA, std::string("regrid remap: ") + cudaGetErrorString(e));
-    }
-    cudaFree(a->U);
-    a->U = Unew;
-    if (cap_new > a->cap) {
-        int rc = alloc_leaf_buffers(a, cap_new);
-        if (rc) return rc;
-    }
-    t.lev.swap(lev);
-    t.cx.swap(cx);
-    t.index.clear();
-    for (int64_t i = 0; i < n; ++i) t.index[Tree::key(t.lev[i], &t.cx[3 * i])] = (int)i;
-    return build_tables(a);
 }
 
 int compute_dt_level(vb_amr *a, int level, double *dt)
@@ -456,12 +338,7 @@ int step_level(vb_amr *a, double dt, int level, int nreg, const int *rl, const d
     return VB_OK;
 }
 
-int max_level(const vb_amr *a)
-{
-    int m = 0;
-    for (int l : a->tree.lev) m = l > m ? l : m;
-    return m;
-}
+int max_level(const vb_amr *a) { return a->maxlev; }
 
 inline double jmin(double x, double y)
 {
@@ -501,17 +378,15 @@ int evolve_level(vb_amr *a, int level, double dt_target, bool has_parent)
 
 int regrid(vb_amr *a, double above, int maxl, int64_t *ntag)
 {
-    const int n = (int)a->tree.n();
     cudaStream_t st = a->ctx->stream;
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_tag(a->dev, a->U, above, maxl, a->tag, nullptr, st));
-    std::vector<uint8_t> h((size_t)n);
-    VB_CUDA(cudaMemcpyAsync(h.data(), a->tag, n, cudaMemcpyDeviceToHost, st));
-    VB_CUDA(cudaStreamSynchronize(st));
-    std::vector<int> which;
-    for (int i = 0; i < n; ++i)
-        if (h[i]) which.push_back(i);
-    if (ntag) *ntag = (int64_t)which.size();
-    return refine_leaves(a, which);
+    VB_CUDA(cudaMemsetAsync(a->word + 4, 0, sizeof(int), st));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_tag(a->dev, a->U, above, maxl, a->tag, nullptr,
+                                               a->word + 4, st));
+    int rc = sync_words(a);
+    if (rc) return rc;
+    if (ntag) *ntag = a->hword[4];
+    if (!a->hword[4]) return VB_OK;
+    return refine_marked(a);
 }
 
 }  // namespace
@@ -533,27 +408,29 @@ int vb_amr_create(vb_ctx *ctx, const vb_problem_desc *d, vb_amr **out)
     if (!a) return fail(VB_ENOMEM, "host allocation failed");
     a->ctx = ctx;
     a->g = g;
-    Tree &t = a->tree;
-    t.nd = g.nd;
+    a->nd = g.nd;
     for (int k = 0; k < 3; ++k) {
-        t.base[k] = k < g.nd ? g.n[k] : 1;
-        t.bc_lo[k] = g.bc_lo[k];
-        t.bc_hi[k] = g.bc_hi[k];
+        a->base[k] = k < g.nd ? g.n[k] : 1;
         a->w0[k] = k < g.nd ? g.w[k] : 1.0;
     }
-    const int64_t n = t.base[0] * t.base[1] * t.base[2];
+    for (int l = 0; l <= vb::AMR_MAX_LEVEL; ++l) {
+        double v = 1.0;
+        for (int d = 0; d < 3; ++d) {
+            double ar = 1.0;
+            for (int e2 = 0; e2 < a->nd; ++e2)
+                if (e2 != d) ar = ar * level_width(a, l, e2);
+            a->areas.area[l][d] = ar;
+            a->dev.w[l][d] = d < a->nd ? level_width(a, l, d) : 1.0;
+        }
+        for (int d = 0; d < a->nd; ++d) v = v * a->dev.w[l][d];
+        a->dev.vol[l] = v;
+    }
+    const int64_t n = a->base[0] * a->base[1] * a->base[2];
     if (n > INT_MAX / 8) {
         delete a;
         return fail(VB_EINVAL, "base grid too large");
     }
-    t.lev.assign(n, 0);
-    t.cx.resize(3 * n);
-    for (int64_t i = 0; i < n; ++i) {
-        t.cx[3 * i] = i % t.base[0];
-        t.cx[3 * i + 1] = (i / t.base[0]) % t.base[1];
-        t.cx[3 * i + 2] = i / (t.base[0] * t.base[1]);
-        t.index[Tree::key(0, &t.cx[3 * i])] = (int)i;
-    }
+    std::vector<int> lev0((size_t)n, 0), cx0;
     cudaError_t e = cudaMalloc(&a->ctrl, sizeof(vb::Ctrl));
     if (e == cudaSuccess) e = cudaMallocHost(&a->hctrl, sizeof(vb::Ctrl));
     if (e == cudaSuccess) e = cudaMalloc(&a->partials, sizeof(double) * 5 * vb::TOTALS_PARTS);
@@ -567,10 +444,31 @@ int vb_amr_create(vb_ctx *ctx, const vb_problem_desc *d, vb_amr **out)
     std::memset(a->hctrl, 0, sizeof(vb::Ctrl));
     a->hctrl->tfinal = INFINITY;
     a->hctrl->step_limit = LLONG_MAX;
+    e = cudaMalloc(&a->word, sizeof(int) * 8);
+    if (e == cudaSuccess) e = cudaMallocHost(&a->hword, sizeof(int) * 8);
+    if (e != cudaSuccess) {
+        release(a);
+        delete a;
+        return fail(VB_ENOMEM, std::string("AMR buffers: ") + cudaGetErrorString(e));
+    }
     int64_t cap = 1024;
     while (cap < n) cap *= 2;
+    // base leaves: level 0, column-major
+    cx0.assign((size_t)(3 * cap), 0);
+    for (int64_t i = 0; i < n; ++i) {
+        cx0[i] = (int)(i % a->base[0]);
+        cx0[cap + i] = (int)((i / a->base[0]) % a->base[1]);
+        cx0[2 * cap + i] = (int)(i / (a->base[0] * a->base[1]));
+    }
     rc = realloc_dev(&a->U, 5 * cap);
+    if (!rc) rc = realloc_dev(&a->lev, cap);
+    if (!rc) rc = realloc_dev(&a->cx, 3 * cap);
     if (!rc) rc = alloc_leaf_buffers(a, cap);
+    if (!rc && (cudaMemcpy(a->lev, lev0.data(), sizeof(int) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(a->cx, cx0.data(), sizeof(int) * 3 * cap, cudaMemcpyHostToDevice) != cudaSuccess))
+        rc = fail(VB_ECUDA, "AMR base upload failed");
+    a->n = (int)n;
+    a->maxlev = 0;
     if (!rc) rc = push_ctrl(a);
     if (!rc) rc = build_tables(a);
     if (!rc) {
@@ -599,17 +497,26 @@ int vb_amr_destroy(vb_amr *a)
 int vb_amr_nleaf(const vb_amr *a, int64_t *n)
 {
     if (!a || !n) return fail(VB_EINVAL, "null argument");
-    *n = a->tree.n();
+    *n = a->n;
     return VB_OK;
 }
 
 int vb_amr_leaves(const vb_amr *a, int32_t *level, int64_t *coords)
 {
     if (!a) return fail(VB_EINVAL, "null argument");
-    const int64_t n = a->tree.n();
+    int rc = use(a->ctx);
+    if (rc) return rc;
+    const int64_t n = a->n;
+    std::vector<int> lev((size_t)n), cx((size_t)(3 * n));
+    VB_CUDA(cudaStreamSynchronize(a->ctx->stream));
+    VB_CUDA(cudaMemcpy(lev.data(), a->lev, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    for (int d = 0; d < 3; ++d)
+        VB_CUDA(cudaMemcpy(cx.data() + d * n, a->cx + d * a->cap, sizeof(int) * n,
+                           cudaMemcpyDeviceToHost));
     for (int64_t i = 0; i < n; ++i) {
-        if (level) level[i] = a->tree.lev[i];
-        if (coords) std::memcpy(coords + 3 * i, &a->tree.cx[3 * i], 3 * sizeof(int64_t));
+        if (level) level[i] = lev[i];
+        if (coords)
+            for (int d = 0; d < 3; ++d) coords[3 * i + d] = cx[d * n + i];
     }
     return VB_OK;
 }
@@ -624,7 +531,7 @@ int vb_amr_nface(const vb_amr *a, int64_t *n)
 int vb_amr_max_level(const vb_amr *a, int32_t *level)
 {
     if (!a || !level) return fail(VB_EINVAL, "null argument");
-    *level = max_level(a);
+    *level = a->maxlev;
     return VB_OK;
 }
 
@@ -633,7 +540,7 @@ int vb_amr_upload(vb_amr *a, const double *U)
     if (!a || !U) return fail(VB_EINVAL, "null argument");
     int rc = use(a->ctx);
     if (rc) return rc;
-    const int64_t n = a->tree.n();
+    const int64_t n = a->n;
     VB_CUDA(cudaMemcpy2DAsync(a->U, sizeof(double) * a->cap, U, sizeof(double) * n,
                               sizeof(double) * n, 5, cudaMemcpyHostToDevice, a->ctx->stream));
     VB_CUDA(cudaStreamSynchronize(a->ctx->stream));
@@ -645,7 +552,7 @@ int vb_amr_download(vb_amr *a, double *U)
     if (!a || !U) return fail(VB_EINVAL, "null argument");
     int rc = use(a->ctx);
     if (rc) return rc;
-    const int64_t n = a->tree.n();
+    const int64_t n = a->n;
     VB_CUDA(cudaMemcpy2DAsync(U, sizeof(double) * n, a->U, sizeof(double) * a->cap,
                               sizeof(double) * n, 5, cudaMemcpyDeviceToHost, a->ctx->stream));
     VB_CUDA(cudaStreamSynchronize(a->ctx->stream));
@@ -671,15 +578,17 @@ int vb_amr_get_time(const vb_amr *a, double *t, int64_t *step)
 int vb_amr_refine(vb_amr *a, const int64_t *leaves, int64_t n)
 {
     if (!a || (n > 0 && !leaves)) return fail(VB_EINVAL, "null argument");
-    const int64_t nl = a->tree.n();
-    std::vector<int> which;
+    const int64_t nl = a->n;
+    std::vector<uint8_t> mark((size_t)nl, 0);
     for (int64_t k = 0; k < n; ++k) {
         if (leaves[k] < 0 || leaves[k] >= nl) return fail(VB_EINVAL, "leaf index out of range");
-        which.push_back((int)leaves[k]);
+        mark[(size_t)leaves[k]] = 1;
     }
     int rc = use(a->ctx);
     if (rc) return rc;
-    return refine_leaves(a, which);
+    if (n == 0) return VB_OK;
+    VB_CUDA(cudaMemcpy(a->tag, mark.data(), (size_t)nl, cudaMemcpyHostToDevice));
+    return refine_marked(a);
 }
 
 int vb_amr_indicator(vb_amr *a, double *out)
@@ -687,10 +596,11 @@ int vb_amr_indicator(vb_amr *a, double *out)
     if (!a || !out) return fail(VB_EINVAL, "null argument");
     int rc = use(a->ctx);
     if (rc) return rc;
-    const int64_t n = a->tree.n();
+    const int64_t n = a->n;
     double *d = nullptr;
     VB_CUDA(cudaMalloc(&d, sizeof(double) * (n > 0 ? n : 1)));
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_tag(a->dev, a->U, INFINITY, 0, a->tag, d, a->ctx->stream));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_tag(a->dev, a->U, INFINITY, 0, a->tag, d, nullptr,
+                                               a->ctx->stream));
     cudaError_t e = cudaMemcpyAsync(out, d, sizeof(double) * n, cudaMemcpyDeviceToHost, a->ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(a->ctx->stream);
     cudaFree(d);

@@ -40,13 +40,46 @@ struct AmrStageArgs {
     int cfl_all;
 };
 
+// Topology view for the regrid kernels (vb_amr_regrid.cu).
+struct AmrTopo {
+    int nd;
+    int64_t base[3];
+    int bc_lo[3], bc_hi[3];
+    int n;          // leaves
+    int64_t cap;    // leaf stride of cx and the per-side tables
+    const int *lev;
+    const int *cx;  // [3][cap] integer coordinates at the leaf's level
+    const uint64_t *hkey;
+    const int *hval;
+    uint64_t hmask;  // hash capacity - 1 (a power of two minus one)
+};
+
+// face area per level and axis
+struct AmrAreas {
+    double area[AMR_MAX_LEVEL + 1][3];
+};
+
+int amr_scan(const int *in, int n, int *out, int *bsum, int *total, cudaStream_t s);
+int launch_amr_hash_build(const AmrTopo &t, uint64_t *keys, int *vals, int *err, cudaStream_t s);
+int launch_amr_balance(const AmrTopo &t, uint8_t *mark, int *changed, cudaStream_t s);
+int launch_amr_count_children(const AmrTopo &t, const uint8_t *mark, int *cnt, int *maxlev,
+                              cudaStream_t s);
+int launch_amr_emit(const AmrTopo &t, const uint8_t *mark, const int *off, int *lev_new,
+                    int *cx_new, int64_t cap_new, const double *Uold, double *Unew, cudaStream_t s);
+int launch_amr_kinds(const AmrTopo &t, int8_t *kind, int *rep, int *fcnt, cudaStream_t s);
+int launch_amr_faces(const AmrTopo &t, const int8_t *kind, const int *rep, const int *fbase,
+                     const AmrAreas &ar, int *fL, int *fR, int8_t *fax, double *farea, int *faceid,
+                     cudaStream_t s);
+int launch_amr_csr_count(const AmrTopo &t, const int8_t *kind, const int *fcnt, int *ecnt,
+                         cudaStream_t s);
+int launch_amr_csr_fill(const AmrTopo &t, const int8_t *kind, const int *rep, const int *faceid,
+                        const int *off, int *ent, int *err, cudaStream_t s);
+
 int launch_amr_stage(const AmrDev &m, int stage, const double *Uin, const double *U0,
                      double *Uout, double *F, const AmrStageArgs &a, Ctrl *ctrl, cudaStream_t s);
 int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cudaStream_t s);
 int launch_amr_tag(const AmrDev &m, const double *U, double above, int max_level, uint8_t *tag,
-                   double *ind, cudaStream_t s);
-int launch_amr_prolong(int n, int64_t cap_old, int64_t cap_new, const int *src, const double *Uold,
-                       double *Unew, cudaStream_t s);
+                   double *ind, int *ntag, cudaStream_t s);
 int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s);
 int launch_amr_zero_reg(const AmrDev &m, int level, cudaStream_t s);
 int launch_amr_totals(const AmrDev &m, const double *U, double *partials, int npart, double *out,

@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(256) k_amr_cfl(AmrDev m, const double *__restr
 // density_gradient_indicator (src/driver.jl:406-420) and the regrid! tag
 __global__ void __launch_bounds__(256) k_amr_tag(AmrDev m, const double *__restrict__ U,
                                                  double above, int max_level, uint8_t *tag,
-                                                 double *ind)
+                                                 double *ind, int *ntag)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.nleaf) return;
@@ -201,19 +201,9 @@ __global__ void __launch_bounds__(256) k_amr_tag(AmrDev m, const double *__restr
         g = fmax(g, fabs(rn - rc) / fmax(fmax(rc, rn), 2.220446049250313e-16));
     }
     if (ind) ind[i] = g;
-    tag[i] = (m.lev[i] < max_level && g > above) ? 1 : 0;
-}
-
-// new state from the old one after a regrid: every new leaf copies the cell
-// mean of the old leaf it came from (itself or its refined ancestor)
-__global__ void k_amr_prolong(int n, int64_t cap_old, int64_t cap_new, const int *__restrict__ src,
-                              const double *__restrict__ Uold, double *__restrict__ Unew)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int s = src[i];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) Unew[(int64_t)k * cap_new + i] = Uold[(int64_t)k * cap_old + s];
+    const bool on = m.lev[i] < max_level && g > above;
+    tag[i] = on ? 1 : 0;
+    if (on && ntag) atomicAdd(ntag, 1);
 }
 
 // _reflux_apply! (src/reflux.jl:91-101) for the leaves of one level
@@ -286,17 +276,9 @@ int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cuda
 }
 
 int launch_amr_tag(const AmrDev &m, const double *U, double above, int max_level, uint8_t *tag,
-                   double *ind, cudaStream_t s)
+                   double *ind, int *ntag, cudaStream_t s)
 {
-    k_amr_tag<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, above, max_level, tag, ind);
-    return 1;
-}
-
-int launch_amr_prolong(int n, int64_t cap_old, int64_t cap_new, const int *src, const double *Uold,
-                       double *Unew, cudaStream_t s)
-{
-    if (n <= 0) return 0;
-    k_amr_prolong<<<blocks(n, 256), 256, 0, s>>>(n, cap_old, cap_new, src, Uold, Unew);
+    k_amr_tag<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, above, max_level, tag, ind, ntag);
     return 1;
 }
 
