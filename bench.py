@@ -51,8 +51,11 @@ def parse():
                     help="skip the Sedov 48^2 AMR run")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the KH 512^2 adjoint timing and finite-difference check")
-    ap.add_argument("--workload", choices=["cube", "batch64"], default="cube",
-                    help="cube: the 256^3 headline; batch64: 64 uneven Riemann boxes in one batch")
+    ap.add_argument("--workload", choices=["cube", "batch64", "plane", "adjoint", "amr"],
+                    default="cube",
+                    help="cube: the 256^3 headline line (with the plane, adjoint and AMR "
+                         "sections); batch64: 64 uneven Riemann boxes in one batch; plane, "
+                         "adjoint, amr: that section alone")
     return ap.parse_args()
 
 
@@ -603,6 +606,26 @@ def run_batch64(args, ranks: Ranks):
     print(json.dumps(line), flush=True)
 
 
+def run_section(args, ranks: Ranks):
+    """One of the secondary workloads alone, printed as its own JSON line."""
+    import vespa_b200 as vb
+    ctx = vb.Context(ranks.local)
+    if args.workload == "plane":
+        sec = plane_section(ctx, ranks, args.steps, args.warmup)
+        metric, value = "Mcell-updates/s 2D 4096^2 PLM+HLLC RK2 (mixed)", sec["mixed"]["value"]
+    elif args.workload == "adjoint":
+        sec = adjoint_section(ctx, ranks)
+        metric, value = ("adjoint step / forward step, KH 512^2 float64",
+                         sec["textured"]["adj_step_over_fwd_step"])
+    else:
+        sec = amr_section(ctx, ranks)
+        metric, value = ("Mleaf-updates/s, Sedov 48^2 AMR single rate",
+                         sec["single_rate"]["value"])
+    if ranks.rank == 0:
+        print(json.dumps({"metric": metric, "value": value, "n_gpus": ranks.world,
+                          "workload": args.workload, args.workload: sec}), flush=True)
+
+
 def main():
     args = parse()
     ranks = Ranks(args.gpus)
@@ -611,6 +634,8 @@ def main():
             run_reference(args, ranks)
         elif args.workload == "batch64":
             run_batch64(args, ranks)
+        elif args.workload in ("plane", "adjoint", "amr"):
+            run_section(args, ranks)
         else:
             run_ours(args, ranks)
     finally:
