@@ -228,12 +228,37 @@ def choose_sample(nthreads: int, target_s: float):
     return n, rate
 
 
+def oracle_rate_serial(dims, budget_s: float):
+    """The oracle's faithful serial path (face enumeration in the reference's
+    order, one thread, like the reference's loop): Mcell-updates/s."""
+    from oracle import oracle as O
+    import vespa_b200 as vb
+    prob = vb.smooth_random_problem(dims)
+    U = vb.initial_state(prob)
+    g = O.grid_from_problem(prob)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        O.step(g, U, O.compute_dt(g, U), mode=0)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return prob.ncell * done / el / 1e6, done, el
+
+
 def cpu_baseline(nthreads: int) -> dict:
     n, _ = choose_sample(nthreads, 6.0)
     rate, done, el = oracle_rate(n, 64, 15.0, nthreads)
+    ser, sdone, sel = oracle_rate_serial((64, 64, 64), 3.0)
+    ser2, s2done, s2el = oracle_rate_serial((512, 512), 3.0)
     return {"value": round(rate, 3), "unit": UNIT, "cores": nthreads, "kind": "port",
             "sample": f"{done} RK2 step(s) of a {n}^3 periodic box from the same generator "
-                      f"({el:.1f} s), C oracle per-cell gather with OpenMP"}
+                      f"({el:.1f} s), C oracle per-cell gather with OpenMP",
+            "serial": {"value": round(ser, 3), "cores": 1,
+                       "sample": f"{sdone} step(s) of 64^3, faithful serial face loop ({sel:.1f} s)"},
+            "serial_2d": {"value": round(ser2, 3), "cores": 1,
+                          "sample": f"{s2done} step(s) of 512^2 (the 4096^2 plane's generator), "
+                                    f"faithful serial face loop ({s2el:.1f} s)"}}
 
 
 def run_reference(args, ranks: Ranks):
