@@ -33,6 +33,7 @@ def test_batch_boxes_equal_single_runs(vb, precision):
     batch.run_steps(2)  # a second graph (different length), continuing the clocks
     for i, p in enumerate(probs):
         sim = vb.Simulation(vb.B200Mesh(p.dims, p.domain), p, precision=precision)
+        sim.set_kernel("tiled")  # the batch always runs the tiled kernel
         vb.evolve(sim, tfinal=math.inf, max_steps=5)
         t, n = batch.time(i)
         assert n == 5 and t == sim.t, (i, t, sim.t)

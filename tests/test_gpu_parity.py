@@ -238,6 +238,7 @@ def test_autotune_restores_state_and_keeps_results(vb):
     prob = P.smooth_random_problem((64, 48, 80), seed=31)
     U0 = P.initial_state(prob)
     a = make_sim(prob, U0)
+    a.set_kernel("tiled")
     kz, ms = a.autotune(nsteps=2)
     assert kz in (16, 24, 32, 48, 64) and ms > 0
     assert a.kz == kz
@@ -273,6 +274,8 @@ def test_tiled_mixed_precision_conserves(vb):
     U0 = P.initial_state(prob)
     a = make_sim(prob, U0, "fp64")
     b = make_sim(prob, U0, "mixed")
+    a.set_kernel("tiled")
+    b.set_kernel("tiled")
     assert b.kernel == "tiled"
     t0 = np.array(vb.conserved_totals(b))
     vb.evolve(a, max_steps=20)
@@ -298,6 +301,8 @@ def test_tiled_mixed_on_sharp_data(vb, bcs):
     U0 = P.initial_state(prob)
     a = make_sim(prob, U0, "fp64")
     b = make_sim(prob, U0, "mixed")
+    a.set_kernel("tiled")
+    b.set_kernel("tiled")
     assert b.kernel == "tiled"
     t0 = np.array(vb.conserved_totals(b))
     vb.evolve(a, tfinal=math.inf, max_steps=15)

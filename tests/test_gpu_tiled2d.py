@@ -63,6 +63,7 @@ def test_tiled2d_sharp_walls_bit_identical(vb, oracle):
                                            np.where(x + 2 * y < 0.5, 1.0, 0.1)))
     U0 = P.initial_state(prob)
     sim = make_sim(prob, U0)
+    sim.set_kernel("tiled")
     assert sim.kernel == "tiled"
     vb.evolve(sim, max_steps=12)
     g = oracle.grid_from_problem(prob)
@@ -77,6 +78,8 @@ def test_tiled2d_mixed_accuracy_and_conservation(vb):
     U0 = P.initial_state(prob)
     a = make_sim(prob, U0, "fp64")
     b = make_sim(prob, U0, "mixed")
+    a.set_kernel("tiled")
+    b.set_kernel("tiled")
     assert a.kernel == "tiled" and b.kernel == "tiled"
     t0 = np.array(vb.conserved_totals(b))
     vb.evolve(a, max_steps=20)

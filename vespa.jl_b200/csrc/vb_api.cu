@@ -118,6 +118,34 @@ int default_kz(const vb::Geom &g)
     return n >= 64 ? 32 : (int)((n + 1) / 2);
 }
 
+// Column tiles (3D) or row segments (2D) per chunk of the marching axis.
+int64_t tiles_per_chunk(const vb::Geom &g)
+{
+    return g.nd == 2 ? g.n[0] / 256 : (g.n[0] / 16) * (g.n[1] / 16);
+}
+
+// The automatic kernel choice takes a tiled kernel only when it yields enough
+// work items for the persistent grid (two blocks per SM on 148 SMs, with a
+// chunk of at least 8 planes/rows); small grids keep the cell-centric kernel.
+bool tiled_auto(const vb::Geom &g)
+{
+    if (!vb::tiled_supported(g)) return false;
+    const int64_t ext = vb::march_extent(g);
+    return tiles_per_chunk(g) * ((ext + 7) / 8) >= 296;
+}
+
+// Default chunk of a single grid: the largest of 32, 16, 8 that still gives
+// two work items per persistent block.
+int grid_default_kz(const vb::Geom &g)
+{
+    const int64_t ext = vb::march_extent(g);
+    for (int kz : {32, 16}) {
+        if (kz > ext) continue;
+        if (tiles_per_chunk(g) * ((ext + kz - 1) / kz) >= 592) return kz;
+    }
+    return (int)(ext >= 8 ? 8 : ext);
+}
+
 // Geometry of a descriptor, validated as Problem is (src/problem.jl:39-46),
 // and RefMesh's derived widths, areas and volume (lib/RefMesh/src/RefMesh.jl:
 // 122-142).
@@ -285,12 +313,72 @@ int ensure_cfl(vb_grid *gr)
 }
 
 // Queue `count` CFL-limited steps (each: finalize dt, stage 1, stage 2).
-int queue_steps(vb_grid *gr, int64_t count)
+int queue_direct(vb_grid *gr, int64_t count)
 {
     for (int64_t i = 0; i < count; ++i) {
         VB_CHECK_LAUNCH(gr->ctx, vb::launch_finalize_cfl(gr->g, gr->ctrl, gr->ctx->stream));
         int rc = rk2(gr);
         if (rc) return rc;
+    }
+    return VB_OK;
+}
+
+constexpr int64_t GRAPH_STEPS = 8;
+
+uint64_t graph_key(const vb_grid *gr)
+{
+    return (gr->tiled ? 1u : 0u) | (gr->bflux_on ? 2u : 0u) | ((uint64_t)gr->kz << 2);
+}
+
+// Capture GRAPH_STEPS steps into the grid's graph for its current configuration.
+int capture_steps(vb_grid *gr)
+{
+    if (gr->gexec) {
+        cudaGraphExecDestroy(gr->gexec);
+        gr->gexec = nullptr;
+    }
+    cudaStream_t s = gr->ctx->stream;
+    VB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = gr->ctx->launches;
+    int rc = queue_direct(gr, GRAPH_STEPS);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &graph);
+    const int64_t n = gr->ctx->launches - before;
+    gr->ctx->launches = before;  // counted per replay
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(VB_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&gr->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        gr->gexec = nullptr;
+        return fail(VB_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    gr->gkey = graph_key(gr);
+    gr->glaunches = n;
+    return VB_OK;
+}
+
+// Queue `count` CFL-limited steps (each: finalize dt, stage 1, stage 2,
+// advance): whole groups of GRAPH_STEPS replay one captured graph, the rest
+// launch directly.
+int queue_steps(vb_grid *gr, int64_t count)
+{
+    while (gr->warmed && count >= GRAPH_STEPS) {
+        if (!gr->gexec || gr->gkey != graph_key(gr)) {
+            int rc = capture_steps(gr);
+            if (rc) return rc;
+        }
+        VB_CUDA(cudaGraphLaunch(gr->gexec, gr->ctx->stream));
+        gr->ctx->launches += gr->glaunches;
+        count -= GRAPH_STEPS;
+    }
+    if (count > 0) {
+        int rc = queue_direct(gr, count);
+        if (rc) return rc;
+        gr->warmed = true;
     }
     return VB_OK;
 }
@@ -506,8 +594,8 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
             std::string m = g_err;
             return cleanup(rc, m);
         }
-        gr->tiled = true;
-        gr->kz = vb::detail::default_kz(g);
+        gr->tiled = vb::detail::tiled_auto(g);
+        gr->kz = vb::detail::grid_default_kz(g);
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_kz.find(tune_key(ctx->device, g, precision));
         if (it != g_tune_kz.end()) gr->kz = it->second;
@@ -600,7 +688,7 @@ int vb_grid_set_option(vb_grid *gr, int option, int64_t value)
                 if (!rc) rc = encode_maps(&gr->maps_U1, gr->U1, gr->g);
                 if (rc) return rc;
             }
-            gr->tiled = true;
+            gr->tiled = value == VB_KERNEL_TILED || vb::detail::tiled_auto(gr->g);
         } else {
             return fail(VB_EINVAL, "unknown kernel selector");
         }
@@ -632,6 +720,7 @@ int vb_grid_destroy(vb_grid *gr)
         cudaSetDevice(gr->ctx->device);
         cudaStreamSynchronize(gr->ctx->stream);
     }
+    if (gr->gexec) cudaGraphExecDestroy(gr->gexec);
     cudaFree(gr->U);
     cudaFree(gr->U1);
     cudaFree(gr->ctrl);

@@ -36,6 +36,11 @@ struct vb_grid {
     vb::TiledMaps maps_U{}, maps_U1{};  // TMA descriptors of the two stage inputs
     vb::BoxDesc box{};                  // the tiled kernels' box descriptor (passed by value)
     int box_kz = 0;                     // kz the descriptor was written with
+    // CUDA graph of GRAPH_STEPS steps (finalize + RK2), replayed by the step loop
+    cudaGraphExec_t gexec = nullptr;
+    uint64_t gkey = 0;                  // kernel configuration it was captured for
+    int64_t glaunches = 0;              // kernels per replay
+    bool warmed = false;                // one direct step ran (launch setup done)
 };
 
 namespace vb {
@@ -53,8 +58,11 @@ int encode_maps(TiledMaps *m, const double *base, const Geom &g);
 BoxDesc make_box(const TiledMaps &mU, const TiledMaps &mU1, const Geom &g, double *U, double *U1,
                  Ctrl *ctrl, int kz, int item0);
 int64_t box_items(const Geom &g, int kz);
-// default z-chunk of a tiled grid
+// default z-chunk of a tiled box (batches)
 int default_kz(const Geom &g);
+// automatic kernel choice and default chunk of a single grid
+bool tiled_auto(const Geom &g);
+int grid_default_kz(const Geom &g);
 
 // Grid stepping helpers shared with the adjoint (vb_api.cu).
 int grid_ensure_cfl(vb_grid *gr);   // CFL max of the current state, if stale
