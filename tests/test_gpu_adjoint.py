@@ -167,3 +167,25 @@ def test_kh512_200_steps_matches_finite_differences(vb):
     assert np.median(errs) <= 1e-6, errs
     assert np.mean(errs <= 1e-6) >= 0.9, errs
     assert errs.max() <= 1e-5, errs
+
+
+def test_evolve_function_backpropagates_through_the_device_run(vb):
+    """The torch.autograd bridge (rrule shape): a torch objective of the final
+    state differentiates to the same gradient as the adjoint's backward."""
+    prob = vb.kelvin_helmholtz_problem(n=32, texture=1e-2)
+    sim = _sim(vb, prob)
+    U0 = torch.tensor(sim.state(), requires_grad=True)
+    UT = vb.EvolveFunction.apply(U0, sim, 6, 2)
+    V = sim.backend.cell_volume()
+    J = (UT[0] * UT[0]).sum() * V
+    J.backward()
+    # the same through the explicit API
+    sim2 = _sim(vb, prob)
+    adj = vb.Adjoint(sim2, 6, 2)
+    adj.forward(max_steps=6)
+    ref = adj.backward(vb.rho2_seed(sim2, sim2.state()))
+    assert np.array_equal(UT.detach().numpy(), sim2.state())
+    np.testing.assert_allclose(U0.grad.numpy(), ref, rtol=0, atol=1e-15 * np.abs(ref).max())
+    adj.close()
+    sim.close()
+    sim2.close()
