@@ -39,7 +39,7 @@ typedef enum {
     VB_ENOMEM = 3,      /* device or pinned allocation failed */
     VB_ENONFINITE = 4,  /* a non-finite or negative density/pressure reached the CFL reduction */
     VB_ETIMEOUT = 5,    /* a bounded device wait gave up */
-    VB_ENOTSUP = 6      /* configuration not supported by this build */
+    VB_ENOTSUP = 6      /* configuration the library does not support */
 } vb_status;
 
 /* Boundary conditions, lib/MeshInterface/src/MeshInterface.jl:74-83. */

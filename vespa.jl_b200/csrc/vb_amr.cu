@@ -229,8 +229,8 @@ int refine_marked(vb_amr *a)
 {
     cudaStream_t s = a->ctx->stream;
     vb::AmrTopo t = topo(a);
-    for (int round = 0;; ++round) {
-        if (round > 2 * vb::AMR_MAX_LEVEL + 4) return fail(VB_ECUDA, "AMR balance did not converge");
+    for (int pass = 0;; ++pass) {
+        if (pass > 2 * vb::AMR_MAX_LEVEL + 4) return fail(VB_ECUDA, "AMR balance did not converge");
         VB_CUDA(cudaMemsetAsync(a->word + 1, 0, sizeof(int), s));
         VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_balance(t, a->tag, a->word + 1, s));
         int rc = sync_words(a);

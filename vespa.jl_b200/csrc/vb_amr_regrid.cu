@@ -123,7 +123,7 @@ __global__ void k_hash_insert(AmrTopo t, uint64_t *keys, int *vals, int *err)
     atomicOr(err, 1);
 }
 
-// refine marks of coarser face neighbours of marked leaves (one round)
+// refine marks of coarser face neighbours of marked leaves (one pass)
 __global__ void k_balance(AmrTopo t, uint8_t *mark, int *changed)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
