@@ -224,6 +224,55 @@ __device__ __forceinline__ void hllc_flux_fast(const float WL[5], const float WR
     F[4] += SK * (factor * Estar - E);
 }
 
+// hllc_flux_fast without branches: the wave pattern becomes selects and the
+// star correction is always computed, then selected (same operations, same
+// results).
+template <int DIM>
+__device__ __forceinline__ void hllc_flux_fast_bf(const float WL[5], const float WR[5], float g,
+                                                  float ig1, float F[5])
+{
+    const float rhoL = WL[0], rhoR = WR[0];
+    const float pL = WL[4], pR = WR[4];
+    const float unL = WL[DIM], unR = WR[DIM];
+    const float irL = rcp_approx(rhoL), irR = rcp_approx(rhoR);
+    const float cL = sqrt_approx(g * pL * irL);
+    const float cR = sqrt_approx(g * pR * irR);
+    const float SL = fminf(unL - cL, unR - cR);
+    const float SR = fmaxf(unL + cL, unR + cR);
+    const float aL = rhoL * (SL - unL), aR = rhoR * (SR - unR);
+    const float Ss = (pR - pL + unL * aL - unR * aR) * rcp_approx(aL - aR);
+    const bool supL = SL >= 0.f, supR = SR <= 0.f;
+    const bool star = !supL && !supR;
+    const bool left = supL || (star && Ss >= 0.f);
+    const float Sstar = star ? Ss : 0.f;
+    const float SK = left ? SL : SR, ir = left ? irL : irR;
+    const float rho = left ? WL[0] : WR[0], vx = left ? WL[1] : WR[1];
+    const float vy = left ? WL[2] : WR[2], vz = left ? WL[3] : WR[3];
+    const float p = left ? WL[4] : WR[4];
+    const float un = DIM == 1 ? vx : (DIM == 2 ? vy : vz);
+    const float E = p * ig1 + 0.5f * rho * (vx * vx + vy * vy + vz * vz);
+    const float mun = rho * un;
+    float G[5];
+    G[0] = mun;
+    G[1] = mun * vx;
+    G[2] = mun * vy;
+    G[3] = mun * vz;
+    G[DIM] += p;
+    G[4] = (E + p) * un;
+    const float a = SK - un;
+    const float ra = rho * a;
+    const float factor = ra * rcp_approx(SK - Sstar);
+    const float Estar = E * ir + (Sstar - un) * (Sstar + p * rcp_approx(ra));
+    const float vs[3] = {vx, vy, vz};
+    F[0] = star ? G[0] + SK * (factor - rho) : G[0];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float us = (d == DIM - 1) ? factor * Sstar : factor * vs[d];
+        F[1 + d] = star ? G[1 + d] + SK * (us - rho * vs[d]) : G[1 + d];
+    }
+    F[4] = star ? G[4] + SK * (factor * Estar - E) : G[4];
+}
+
 // Runtime-axis dispatch for the batched face kernel.
 template <typename T>
 __device__ __forceinline__ void hllc_flux_axis(const T WL[5], const T WR[5], double gamma,

@@ -3,14 +3,22 @@
 // Same tiling, TMA pipeline and persistent work queue as k_stage_tiled3d
 // (16 x 16 column tiles marching z; see vb_stage_tiled3d.cuh), specialised
 // for float32 reconstruction and Riemann solves with float64 state:
-//   - each cell's four x/y face values (lo/hi per axis) are computed once from
-//     packed (x, y) minmod slopes and stored as float4 + float records, so a
-//     face reads both of its states with four shared-memory loads;
-//   - every thread solves its x face and its y face together as one packed
-//     float32x2 HLLC (vb_hllc_x2.cuh, faces rotated into their normal frame);
-//     the z face runs in registers down the thread's column;
+//   - primitives live in a ring of three float32 planes (k, k+1, k+2) whose
+//     layout puts the x/y halo and, at a non-periodic boundary, mirror ghost
+//     cells beside the interior, so every slope and face formula is the
+//     interior one;
+//   - every thread reconstructs both states of its own lo x face and lo y face
+//     from the four cells across each (the neighbour's slope is recomputed
+//     rather than exchanged, which saves a barrier per plane) and solves the
+//     pair as one packed float32x2 HLLC (vb_hllc_x2.cuh, faces rotated into
+//     their normal frame); warp 7 adds the tile's hi-edge faces;
+//   - the z face runs in registers down the thread's column, solved before
+//     the plane's first barrier by warps 4..7 and after it by warps 0..3, so
+//     that it balances the halo conversions (warps 0..3) and the edge faces
+//     (warp 7) across the two phases;
 //   - face fluxes are stored once, multiplied by the face area, in float64;
 //     the flux divergence and the stage update stay in float64.
+// Two barriers per plane: (1) plane k+2 converted, (2) fluxes of plane k ready.
 #pragma once
 
 #include "vb_hllc_x2.cuh"
@@ -25,38 +33,31 @@ using t3::NT;
 using t3::TX;
 using t3::TY;
 
-enum { XLO = 0, XHI = 1, YLO = 2, YHI = 3 };
-
-// primitives in one buffer: the current plane's interior [5][NT], then the
-// halo strips of the three planes in flight [3][5][NH]; one index space makes
-// every neighbour fetch a branch-free load
-constexpr int HB = 5 * NT;
+// Primitive planes in shared memory: a ring of three planes (k, k+1, k+2).
+// Per plane and field, 384 floats: rows ly = -2..17 of columns lx = 0..15
+// (row-major, 16 wide, so a warp's two rows never share a bank), then the
+// x halo columns lx = -2, -1, 16, 17 of rows 0..15 (4 per row).  At a
+// non-periodic boundary the halo holds mirror ghosts (the boundary cells
+// reflected by ghost_state), which makes every face and slope formula the
+// same as in the interior.
+constexpr int PC = 384;          // floats per field
+constexpr int PSLOT = 5 * PC;    // floats per plane
+constexpr int XS = 320;          // first x halo column entry
+__host__ __device__ constexpr int wrow(int lx, int ly) { return (ly + 2) * 16 + lx; }
+__host__ __device__ constexpr int wxs(int lx, int ly)
+{
+    return XS + ly * 4 + (lx < 0 ? lx + 2 : lx - 14);
+}
 
 template <int NS>
 struct Smem {
     double u[NS][t3::UPLANE];  // TMA stage buffers (raw conserved state)
     double ep[2][5][NT];       // own-cell epilogue inputs (Uin, U0), fetched by cp.async
-    float w[5 * NT + 3 * 5 * NH];
-    float4 fv4[4][NT];         // face values of interior cells: comps 0..3 of set XLO..YHI
-    float fv1[4][NT];          //   ... comp 4
-    float4 hv4[4][16];         // face values of the cells just outside the tile:
-    float hv1[4][16];          //   XHI of lx=-1, XLO of lx=TX, YHI of ly=-1, YLO of ly=TY
+    float w[3][PSLOT];         // primitive ring
     double gx[5][TY * (TX + 1)];  // x-face area * flux
     double gy[5][(TY + 1) * TX];  // y-face area * flux
     uint64_t bar[NS];
 };
-
-__device__ __forceinline__ void put5(float4 *a4, float *a1, int i, const float v[5])
-{
-    a4[i] = make_float4(v[0], v[1], v[2], v[3]);
-    a1[i] = v[4];
-}
-__device__ __forceinline__ void get5(const float4 *a4, const float *a1, int i, float v[5])
-{
-    const float4 q = a4[i];
-    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
-    v[4] = a1[i];
-}
 
 // minmod slope of (l, c, r), scalar
 __device__ __forceinline__ float mm(float l, float c, float r)
@@ -112,6 +113,54 @@ __device__ __forceinline__ double cfl_term2d(const double un[5], const Geom &g, 
 
 }  // namespace t3m
 
+namespace t3m {
+
+// minmod slopes of two packed differences (same algebra as mm)
+__device__ __forceinline__ f2 minmod2(f2 a, f2 b)
+{
+    const f2 pr = a * b;
+    const float sx = pr.v.x <= 0.f ? 0.f : (fabsf(a.v.x) < fabsf(b.v.x) ? a.v.x : b.v.x);
+    const float sy = pr.v.y <= 0.f ? 0.f : (fabsf(a.v.y) < fabsf(b.v.y) ? a.v.y : b.v.y);
+    return f2(sx, sy);
+}
+
+// Left / right states of a packed face pair, lane x an x face and lane y a y
+// face, each reconstructed from the four cells across it (ring offsets o[0..3]
+// along the face normal: two cells behind the face, two ahead).  Components
+// come out in the face-normal frame (rho, u_n, u_t1, u_t2, p).
+__device__ __forceinline__ void face_pair(const float *wk, const int ox[4], const int oy[4],
+                                          Face2 &L, Face2 &R)
+{
+    f2 l[5], r[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        const int fx = j, fy = j == 1 ? 2 : (j == 2 ? 1 : j);
+        const float *px = wk + fx * PC, *py = wk + fy * PC;
+        const f2 a0(px[ox[0]], py[oy[0]]), a1(px[ox[1]], py[oy[1]]);
+        const f2 a2(px[ox[2]], py[oy[2]]), a3(px[ox[3]], py[oy[3]]);
+        const f2 d2 = a2 - a1;
+        const f2 sl = minmod2(a1 - a0, d2), sc = minmod2(d2, a3 - a2);
+        l[j] = fma2(f2::splat(0.5f), sl, a1);
+        r[j] = fma2(f2::splat(-0.5f), sc, a2);
+    }
+    L = Face2{l[0], l[1], l[2], l[3], l[4]};
+    R = Face2{r[0], r[1], r[2], r[3], r[4]};
+}
+
+// area * flux of a packed face pair into the x / y face arrays (un-rotating
+// the y face's momentum components)
+__device__ __forceinline__ void store_pair(double (*gx)[TY * (TX + 1)], double (*gy)[(TY + 1) * TX],
+                                           int ix, int iy, double ax, double ay, const f2 F[5])
+{
+    gx[0][ix] = ax * (double)F[0].v.x;  gy[0][iy] = ay * (double)F[0].v.y;
+    gx[1][ix] = ax * (double)F[1].v.x;  gy[2][iy] = ay * (double)F[1].v.y;
+    gx[2][ix] = ax * (double)F[2].v.x;  gy[1][iy] = ay * (double)F[2].v.y;
+    gx[3][ix] = ax * (double)F[3].v.x;  gy[3][iy] = ay * (double)F[3].v.y;
+    gx[4][ix] = ax * (double)F[4].v.x;  gy[4][iy] = ay * (double)F[4].v.y;
+}
+
+}  // namespace t3m
+
 template <int NS, int STAGE, bool BATCH>
 __global__ void __launch_bounds__(256, 2)
 k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__restrict__ boxes,
@@ -126,6 +175,22 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
 
     const int t = threadIdx.x;
     const int tx = t & (TX - 1), ty = t >> 4;
+    const int warp = t >> 5, lane = t & 31;
+    // ring offsets of the own cell and of the cells across the own lo x / lo y faces
+    const int o_c = wrow(tx, ty);
+    const int ox[4] = {tx >= 2 ? o_c - 2 : wxs(tx - 2, ty), tx >= 1 ? o_c - 1 : wxs(-1, ty), o_c,
+                       tx <= TX - 2 ? o_c + 1 : wxs(TX, ty)};
+    const int oy[4] = {o_c - 32, o_c - 16, o_c, o_c + 16};
+    // halo cell h = t (t < NH): staged-plane offset and ring offset
+    const int h_u = halo_uoff(t < NH ? t : 0, 0);
+    const int h_w = t < 32   ? wxs(-2 + (t & 1), t >> 1)
+                    : t < 64 ? wxs(TX + (t & 1), (t - 32) >> 1)
+                    : t < 96 ? wrow((t - 64) & 15, -2 + ((t - 64) >> 4))
+                             : wrow((t - 96) & 15, TY + ((t - 96) >> 4));
+    // the z face is solved before barrier (1) by warps 4..7 (balancing the
+    // halo conversions of warps 0..3) and after it by warps 0..3 (balancing
+    // the tile's hi-edge faces, solved by warp 7)
+    const bool z_early = warp >= 4;
 
     if (t == 0) {
         for (int s = 0; s < NS; ++s) mbar_init(&S.bar[s], 1);
@@ -170,6 +235,8 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     const int nplanes = (k1 - k0) + 4;
     const bool xlo_bnd = !perx && x0 == 0, xhi_bnd = !perx && x0 + TX == nx;
     const bool ylo_bnd = !pery && y0 == 0, yhi_bnd = !pery && y0 + TY == ny;
+    // this thread's halo strip lies outside the domain: mirror ghosts replace it
+    const bool h_ghost = t < 32 ? xlo_bnd : (t < 64 ? xhi_bnd : (t < 96 ? ylo_bnd : yhi_bnd));
 
     auto issue = [&](int q) {
         const int p = k0 - 2 + q;
@@ -191,7 +258,25 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         fence_proxy_async_smem();
         for (int q = 0; q < NS && q < nplanes; ++q) issue(q);
     }
-    auto consume = [&](int q, float Wown[5], bool halo) {
+    // Halo strips of staged plane q into ring slot q % 3 (threads t < NH; a
+    // strip outside a non-periodic boundary is left to the mirror ghosts).
+    auto halo_c2p = [&](int q) {
+        if (t < NH && !h_ghost) {
+            const double *u = S.u[(qb + q) % NS];
+            float *ws = S.w[q % 3];
+            double uu[5];
+            float w[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) uu[f] = u[h_u + f * (2 * TY)];
+            cons2prim_mixed(uu, gamma, w);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) ws[h_w + f * PC] = w[f];
+        }
+    };
+    // Wait for staged plane q and convert the own cell into Wn.  keep = 0:
+    // registers only; 1: also into ring slot q % 3 with the mirror ghosts and
+    // the halo strips; 2: as 1 without the halo strips (halo_c2p follows).
+    auto consume = [&](int q, float Wn[5], int keep) {
         const int b = (qb + q) % NS;
         if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) timed_out = true;
         const double *u = S.u[b];
@@ -199,17 +284,33 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
             double uu[5];
 #pragma unroll
             for (int f = 0; f < 5; ++f) uu[f] = u[f * NT + t];
-            cons2prim_mixed(uu, gamma, Wown);
+            cons2prim_mixed(uu, gamma, Wn);
         }
-        if (halo && t < NH) {
-            double uu[5];
-            float w[5];
+        if (!keep) return;
+        float *ws = S.w[q % 3];
 #pragma unroll
-            for (int f = 0; f < 5; ++f) uu[f] = u[halo_uoff(t, f)];
-            cons2prim_mixed(uu, gamma, w);
+        for (int f = 0; f < 5; ++f) ws[f * PC + o_c] = Wn[f];
+        if (xlo_bnd && tx < 2) {
+            float *d = ws + wxs(-1 - tx, ty);
 #pragma unroll
-            for (int f = 0; f < 5; ++f) S.w[HB + ((q % 3) * 5 + f) * NH + t] = w[f];
+            for (int f = 0; f < 5; ++f) d[f * PC] = (bx_lo == BC_REFLECTING && f == 1) ? -Wn[f] : Wn[f];
         }
+        if (xhi_bnd && tx >= TX - 2) {
+            float *d = ws + wxs(2 * TX - 1 - tx, ty);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) d[f * PC] = (bx_hi == BC_REFLECTING && f == 1) ? -Wn[f] : Wn[f];
+        }
+        if (ylo_bnd && ty < 2) {
+            float *d = ws + wrow(tx, -1 - ty);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) d[f * PC] = (by_lo == BC_REFLECTING && f == 2) ? -Wn[f] : Wn[f];
+        }
+        if (yhi_bnd && ty >= TY - 2) {
+            float *d = ws + wrow(tx, 2 * TY - 1 - ty);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) d[f * PC] = (by_hi == BC_REFLECTING && f == 2) ? -Wn[f] : Wn[f];
+        }
+        if (keep == 1) halo_c2p(q);
     };
     auto release = [&](int q) {
         if (t == 0 && q + NS < nplanes) {
@@ -218,233 +319,155 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         }
     };
 
-    float Wa[5], Wb[5], Wz0[5], Wz1[5], Wz2[5];
-    consume(0, Wa, false);
+    float Wa[5], Wb[5], Wc[5], Wd[5];
+    consume(0, Wa, 0);
     __syncthreads();
     release(0);
-    consume(1, Wb, false);
+    consume(1, Wb, 0);
     __syncthreads();
     release(1);
-    consume(2, Wz0, true);
+    consume(2, Wc, 1);
     __syncthreads();
     release(2);
-    consume(3, Wz1, true);
+    consume(3, Wd, 1);
     __syncthreads();
     release(3);
 
     // z state entering plane k0: hi face value of k0 and the flux through k0-1/2
-    float hz[5], Fzlo[5];
+    float hz[5];
+    float fzl[5];
     {
         const bool gl = !perz && k0 == 0;
         const bool gh = !perz && k0 + 1 >= nz;
-        float loz[5];
+        float loz[5], Fzlo[5];
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
-            const float wl = gl ? ((bz_lo == BC_REFLECTING && f == 3) ? -Wz0[f] : Wz0[f]) : Wb[f];
-            const float wr = gh ? ((bz_hi == BC_REFLECTING && f == 3) ? -Wz0[f] : Wz0[f]) : Wz1[f];
-            const float s = mm(wl, Wz0[f], wr);
-            hz[f] = fmaf(0.5f, s, Wz0[f]);
-            loz[f] = fmaf(-0.5f, s, Wz0[f]);
+            const float wl = gl ? ((bz_lo == BC_REFLECTING && f == 3) ? -Wc[f] : Wc[f]) : Wb[f];
+            const float wr = gh ? ((bz_hi == BC_REFLECTING && f == 3) ? -Wc[f] : Wc[f]) : Wd[f];
+            const float s = mm(wl, Wc[f], wr);
+            hz[f] = fmaf(0.5f, s, Wc[f]);
+            loz[f] = fmaf(-0.5f, s, Wc[f]);
         }
         if (gl) {
             float gst[5];
             ghost_state<float>(loz, bz_lo, 2, gst);
-            hllc_flux_fast<3>(gst, loz, gf, ig1, Fzlo);
+            hllc_flux_fast_bf<3>(gst, loz, gf, ig1, Fzlo);
         } else {
             const bool gll = !perz && k0 - 2 < 0;
             float hzm[5];
 #pragma unroll
             for (int f = 0; f < 5; ++f) {
                 const float wl = gll ? ((bz_lo == BC_REFLECTING && f == 3) ? -Wb[f] : Wb[f]) : Wa[f];
-                hzm[f] = fmaf(0.5f, mm(wl, Wb[f], Wz0[f]), Wb[f]);
+                hzm[f] = fmaf(0.5f, mm(wl, Wb[f], Wc[f]), Wb[f]);
             }
-            hllc_flux_fast<3>(hzm, loz, gf, ig1, Fzlo);
+            hllc_flux_fast_bf<3>(hzm, loz, gf, ig1, Fzlo);
         }
+#pragma unroll
+        for (int f = 0; f < 5; ++f) fzl[f] = Fzlo[f];
     }
+
+    // flux through k+1/2 from planes k, k+1 (ring) and k+2 (W2) of the own
+    // column; advances hz
+    auto zsolve = [&](int k, const float *w0, const float *w1, const float W2[5], float Fzhi[5]) {
+        float zr[5], hz1[5];
+        if (perz || k + 1 < nz) {
+            const bool gh = !perz && k + 2 >= nz;
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                const float c = w1[f * PC];
+                const float r = gh ? ((bz_hi == BC_REFLECTING && f == 3) ? -c : c) : W2[f];
+                const float s = mm(w0[f * PC], c, r);
+                zr[f] = fmaf(-0.5f, s, c);
+                hz1[f] = fmaf(0.5f, s, c);
+            }
+        } else {
+            ghost_state<float>(hz, bz_hi, 2, zr);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) hz1[f] = hz[f];
+        }
+        hllc_flux_fast_bf<3>(hz, zr, gf, ig1, Fzhi);
+#pragma unroll
+        for (int f = 0; f < 5; ++f) hz[f] = hz1[f];
+    };
+    // the own lo x face and lo y face of plane k (ring slot w0), one packed solve
+    auto xy_faces = [&](const float *w0) {
+        Face2 L, R;
+        face_pair(w0, ox, oy, L, R);
+        f2 F[5];
+        hllc_x2(L, R, gf, ig1, F);
+        store_pair(S.gx, S.gy, ty * (TX + 1) + tx, ty * TX + tx, ax, ay, F);
+    };
+    // the hi-edge faces (x at fx = TX, y at fy = TY), one pair per lane < 16
+    auto edge_faces = [&](const float *w0) {
+        const int j = lane;
+        const int ex[4] = {wrow(TX - 2, j), wrow(TX - 1, j), wxs(TX, j), wxs(TX + 1, j)};
+        const int ey[4] = {wrow(j, TY - 2), wrow(j, TY - 1), wrow(j, TY), wrow(j, TY + 1)};
+        Face2 L, R;
+        face_pair(w0, ex, ey, L, R);
+        f2 F[5];
+        hllc_x2(L, R, gf, ig1, F);
+        store_pair(S.gx, S.gy, j * (TX + 1) + TX, TY * TX + j, ax, ay, F);
+    };
 
     const int gx = x0 + tx, gy = y0 + ty;
     const int cx = lo_class(gx, nx, perx), cy = lo_class(gy, ny, pery);
-    double unp[5];  // previous plane's new state: its CFL term is folded one plane later
+    // previous plane's new state: its CFL term is folded one plane later (the
+    // initial value is a finite placeholder whose term is discarded)
+    double unp[5] = {1.0, 0.0, 0.0, 0.0, 1.0};
+    const int64_t plane_cells = (int64_t)nx * ny;
+    int64_t lin = (int64_t)gx + (int64_t)nx * ((int64_t)gy + (int64_t)ny * k0);
 
     for (int k = k0; k < k1; ++k) {
         const int q = k - k0 + 4;
-        const int slot = (q - 2) % 3;
-        const int64_t lin = (int64_t)gx + (int64_t)nx * ((int64_t)gy + (int64_t)ny * k);
-        // own-cell epilogue inputs, fetched asynchronously into shared memory
-#pragma unroll
-        for (int f = 0; f < 5; ++f) {
-            cp_async8(&S.ep[0][f][t], Uin + (int64_t)f * g.ncell + lin);
-            if constexpr (STAGE == 2) cp_async8(&S.ep[1][f][t], U0 + (int64_t)f * g.ncell + lin);
-        }
-        cp_async_commit();
-        consume(q, Wz2, true);
-        if constexpr (STAGE == 2)
-            if (k > k0) invdt = cfl_term(unp, g, invdt);  // overlaps the cons2prim chain
-#pragma unroll
-        for (int f = 0; f < 5; ++f) S.w[f * NT + t] = Wz0[f];
-        __syncthreads();  // (1)
-        release(q);
-
-        // primitive of local cell (lx, ly) of plane k, interior or halo strip
-        const int hb = HB + slot * 5 * NH;
-        auto W = [&](int f, int lx, int ly) -> float {
-            return (lx >= 0 && lx < TX && ly >= 0 && ly < TY) ? S.w[f * NT + ly * TX + lx]
-                                                              : S.w[hb + f * NH + halo_idx(lx, ly)];
-        };
-
-        // ---- face values of the interior cells from packed (x, y) slopes ----
+        const float *w0 = S.w[(q - 2) % 3], *w1 = S.w[(q - 1) % 3], *w2 = S.w[q % 3];
         {
-            // neighbour offsets and field strides, branch-free per component
-            const int oxl = tx > 0 ? t - 1 : hb + halo_idx(-1, ty);
-            const int oxr = tx < TX - 1 ? t + 1 : hb + halo_idx(TX, ty);
-            const int oyl = ty > 0 ? t - TX : hb + halo_idx(tx, -1);
-            const int oyr = ty < TY - 1 ? t + TX : hb + halo_idx(tx, TY);
-            const int sxl = tx > 0 ? NT : NH, sxr = tx < TX - 1 ? NT : NH;
-            const int syl = ty > 0 ? NT : NH, syr = ty < TY - 1 ? NT : NH;
-            const bool gxl = tx == 0 && xlo_bnd, gxr = tx == TX - 1 && xhi_bnd;
-            const bool gyl = ty == 0 && ylo_bnd, gyr = ty == TY - 1 && yhi_bnd;
-            float xl[5], xh[5], yl[5], yh[5];
+            const double *pa = Uin + lin, *pb = U0 + lin;
 #pragma unroll
             for (int f = 0; f < 5; ++f) {
-                const float wc = Wz0[f];
-                float l = S.w[oxl + f * sxl], r = S.w[oxr + f * sxr];
-                float d = S.w[oyl + f * syl], e = S.w[oyr + f * syr];
-                if (gxl) l = (bx_lo == BC_REFLECTING && f == 1) ? -wc : wc;
-                if (gxr) r = (bx_hi == BC_REFLECTING && f == 1) ? -wc : wc;
-                if (gyl) d = (by_lo == BC_REFLECTING && f == 2) ? -wc : wc;
-                if (gyr) e = (by_hi == BC_REFLECTING && f == 2) ? -wc : wc;
-                const f2 wc2 = f2::splat(wc);
-                const f2 a = wc2 - f2(l, d), b = f2(r, e) - wc2;
-                const f2 pr = a * b;
-                const float sx = pr.v.x <= 0.f ? 0.f : (fabsf(a.v.x) < fabsf(b.v.x) ? a.v.x : b.v.x);
-                const float sy = pr.v.y <= 0.f ? 0.f : (fabsf(a.v.y) < fabsf(b.v.y) ? a.v.y : b.v.y);
-                const f2 s = f2(sx, sy);
-                const f2 lo = fma2(f2::splat(-0.5f), s, wc2), hi = fma2(f2::splat(0.5f), s, wc2);
-                xl[f] = lo.v.x; yl[f] = lo.v.y;
-                xh[f] = hi.v.x; yh[f] = hi.v.y;
+                cp_async8(&S.ep[0][f][t], pa);
+                if constexpr (STAGE == 2) cp_async8(&S.ep[1][f][t], pb);
+                pa += g.ncell;
+                pb += g.ncell;
             }
-            put5(S.fv4[XLO], S.fv1[XLO], t, xl);
-            put5(S.fv4[XHI], S.fv1[XHI], t, xh);
-            put5(S.fv4[YLO], S.fv1[YLO], t, yl);
-            put5(S.fv4[YHI], S.fv1[YHI], t, yh);
         }
-        // ---- face values of the cells just outside the tile ----
-        if (t >= 160 && t < 224) {
-            const int j = t - 160;
-            const int set = j >> 4, i = j & 15;
-            float v[5];
-            bool need;
-            if (set == 0) {  // XHI of lx = -1, row i
-                need = !xlo_bnd;
-                if (need)
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        const float c = W(f, -1, i);
-                        v[f] = fmaf(0.5f, mm(W(f, -2, i), c, W(f, 0, i)), c);
-                    }
-            } else if (set == 1) {  // XLO of lx = TX, row i
-                need = !xhi_bnd;
-                if (need)
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        const float c = W(f, TX, i);
-                        v[f] = fmaf(-0.5f, mm(W(f, TX - 1, i), c, W(f, TX + 1, i)), c);
-                    }
-            } else if (set == 2) {  // YHI of ly = -1, column i
-                need = !ylo_bnd;
-                if (need)
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        const float c = W(f, i, -1);
-                        v[f] = fmaf(0.5f, mm(W(f, i, -2), c, W(f, i, 0)), c);
-                    }
-            } else {  // YLO of ly = TY, column i
-                need = !yhi_bnd;
-                if (need)
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        const float c = W(f, i, TY);
-                        v[f] = fmaf(-0.5f, mm(W(f, i, TY - 1), c, W(f, i, TY + 1)), c);
-                    }
-            }
-            if (need) put5(S.hv4[set], S.hv1[set], i, v);
-        }
-        __syncthreads();  // (2) face values ready
-
-        // ---- own lo x face and lo y face (one packed solve) and the z face
-        //      k+1/2 down the own column: independent chains, one phase ----
-        float Fzhi[5], hz1[5];
+        cp_async_commit();
+        // ---- phase 1: plane k+2 to primitives; the CFL term of plane k-1; the
+        //      z face (warps 4..7) or the halo strips (warps 0..3) ----
+        float Fzhi[5];
         {
-            float zr[5];  // right state of the z face
-            const bool plane_k1 = perz || k + 1 < nz;
-            if (plane_k1) {
-                const bool gh = !perz && k + 2 >= nz;
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    const float wr = gh ? ((bz_hi == BC_REFLECTING && f == 3) ? -Wz1[f] : Wz1[f]) : Wz2[f];
-                    const float s = mm(Wz0[f], Wz1[f], wr);
-                    zr[f] = fmaf(-0.5f, s, Wz1[f]);
-                    hz1[f] = fmaf(0.5f, s, Wz1[f]);
-                }
+            float Wn[5];
+            consume(q, Wn, 2);
+            double cf = 0.0;
+            if constexpr (STAGE == 2) cf = cfl_term(unp, g, invdt);
+            if (z_early) {
+                zsolve(k, w0 + o_c, w1 + o_c, Wn, Fzhi);
             } else {
-                ghost_state<float>(hz, bz_hi, 2, zr);
-#pragma unroll
-                for (int f = 0; f < 5; ++f) hz1[f] = hz[f];
+                halo_c2p(q);
             }
-            hllc_flux_fast<3>(hz, zr, gf, ig1, Fzhi);
+            if constexpr (STAGE == 2)
+                if (k > k0) invdt = cf;
         }
-        {
-            float Lx[5], Rx[5], Ly[5], Ry[5];
-            get5(S.fv4[XLO], S.fv1[XLO], t, Rx);
-            get5(S.fv4[YLO], S.fv1[YLO], t, Ry);
-            if (tx > 0) get5(S.fv4[XHI], S.fv1[XHI], t - 1, Lx);
-            else if (xlo_bnd) ghost_state<float>(Rx, bx_lo, 0, Lx);
-            else get5(S.hv4[0], S.hv1[0], ty, Lx);
-            if (ty > 0) get5(S.fv4[YHI], S.fv1[YHI], t - TX, Ly);
-            else if (ylo_bnd) ghost_state<float>(Ry, by_lo, 1, Ly);
-            else get5(S.hv4[2], S.hv1[2], tx, Ly);
-            const Face2 L{f2(Lx[0], Ly[0]), f2(Lx[1], Ly[2]), f2(Lx[2], Ly[1]), f2(Lx[3], Ly[3]),
-                          f2(Lx[4], Ly[4])};
-            const Face2 R{f2(Rx[0], Ry[0]), f2(Rx[1], Ry[2]), f2(Rx[2], Ry[1]), f2(Rx[3], Ry[3]),
-                          f2(Rx[4], Ry[4])};
-            f2 F[5];
-            hllc_x2(L, R, gf, ig1, F);
-            const int ix = ty * (TX + 1) + tx, iy = ty * TX + tx;
-            S.gx[0][ix] = ax * (double)F[0].v.x;  S.gy[0][iy] = ay * (double)F[0].v.y;
-            S.gx[1][ix] = ax * (double)F[1].v.x;  S.gy[2][iy] = ay * (double)F[1].v.y;
-            S.gx[2][ix] = ax * (double)F[2].v.x;  S.gy[1][iy] = ay * (double)F[2].v.y;
-            S.gx[3][ix] = ax * (double)F[3].v.x;  S.gy[3][iy] = ay * (double)F[3].v.y;
-            S.gx[4][ix] = ax * (double)F[4].v.x;  S.gy[4][iy] = ay * (double)F[4].v.y;
+        __syncthreads();  // (1) plane k+2 converted
+        release(q);
+        // ---- phase 2: the own lo x / lo y face pair; the z face (warps 0..3)
+        //      or the tile's hi-edge faces (warp 7) ----
+        if (z_early) {
+            xy_faces(w0);
+            if (warp == 7 && lane < 16) edge_faces(w0);
+        } else {
+            float W2[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) W2[f] = w2[o_c + f * PC];
+            zsolve(k, w0 + o_c, w1 + o_c, W2, Fzhi);
+            xy_faces(w0);
         }
-        // ---- the hi-edge faces (x at fx = TX, y at fy = TY), one pair per lane ----
-        if (t >= 224 && t < 240) {
-            const int j = t - 224;
-            float Lx[5], Rx[5], Ly[5], Ry[5];
-            get5(S.fv4[XHI], S.fv1[XHI], j * TX + TX - 1, Lx);
-            if (xhi_bnd) ghost_state<float>(Lx, bx_hi, 0, Rx);
-            else get5(S.hv4[1], S.hv1[1], j, Rx);
-            get5(S.fv4[YHI], S.fv1[YHI], (TY - 1) * TX + j, Ly);
-            if (yhi_bnd) ghost_state<float>(Ly, by_hi, 1, Ry);
-            else get5(S.hv4[3], S.hv1[3], j, Ry);
-            const Face2 L{f2(Lx[0], Ly[0]), f2(Lx[1], Ly[2]), f2(Lx[2], Ly[1]), f2(Lx[3], Ly[3]),
-                          f2(Lx[4], Ly[4])};
-            const Face2 R{f2(Rx[0], Ry[0]), f2(Rx[1], Ry[2]), f2(Rx[2], Ry[1]), f2(Rx[3], Ry[3]),
-                          f2(Rx[4], Ry[4])};
-            f2 F[5];
-            hllc_x2(L, R, gf, ig1, F);
-            const int ix = j * (TX + 1) + TX, iy = TY * TX + j;
-            S.gx[0][ix] = ax * (double)F[0].v.x;  S.gy[0][iy] = ay * (double)F[0].v.y;
-            S.gx[1][ix] = ax * (double)F[1].v.x;  S.gy[2][iy] = ay * (double)F[1].v.y;
-            S.gx[2][ix] = ax * (double)F[2].v.x;  S.gy[1][iy] = ay * (double)F[2].v.y;
-            S.gx[3][ix] = ax * (double)F[3].v.x;  S.gy[3][iy] = ay * (double)F[3].v.y;
-            S.gx[4][ix] = ax * (double)F[4].v.x;  S.gy[4][iy] = ay * (double)F[4].v.y;
-        }
-        __syncthreads();  // (3) fluxes ready
+        __syncthreads();  // (2) fluxes ready
 
         // ---- flux divergence (float64, reference order) and the stage update ----
         const int cz = lo_class(k, nz, perz);
         const bool interior = cx == LO_BEFORE && cy == LO_BEFORE && cz == LO_BEFORE;
         double un[5];
+        double *po = Uout + lin;
         cp_async_wait_all();  // this thread's own epilogue inputs have landed
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
@@ -454,13 +477,13 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
             const double gyh = S.gy[f][(ty + 1) * TX + tx];
             // explicit roundings: the result must not depend on how the compiler
             // contracts this code in each kernel instantiation
-            const double gzl = __dmul_rn(az, (double)Fzlo[f]);
             const double gzh = __dmul_rn(az, (double)Fzhi[f]);
+            const double gz0 = __dmul_rn(az, (double)fzl[f]);
             double a = 0.0;
             if (interior) {
-                a = a - gzl - gyl - gxl + gxh + gyh + gzh;
+                a = a - gz0 - gyl - gxl + gxh + gyh + gzh;
             } else {
-                if (cz == LO_BEFORE) a -= gzl;
+                if (cz == LO_BEFORE) a -= gz0;
                 if (cy == LO_BEFORE) a -= gyl;
                 if (cx == LO_BEFORE) a -= gxl;
                 a += gxh;
@@ -468,30 +491,25 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
                 a += gyh;
                 if (cy == LO_SELF) a -= gyl;
                 a += gzh;
-                if (cz == LO_SELF) a -= gzl;
+                if (cz == LO_SELF) a -= gz0;
                 if (cx == LO_AFTER) a -= gxl;
                 if (cy == LO_AFTER) a -= gyl;
-                if (cz == LO_AFTER) a -= gzl;
+                if (cz == LO_AFTER) a -= gz0;
             }
-            const int64_t i = (int64_t)f * g.ncell + lin;
+            fzl[f] = Fzhi[f];
             if constexpr (STAGE == 1) {
                 un[f] = __fma_rn(-invV, a, S.ep[0][f][t]);
             } else {
                 un[f] = __fma_rn(0.5, S.ep[1][f][t],
                                  __dmul_rn(0.5, __fma_rn(-invV, a, S.ep[0][f][t])));
             }
-            Uout[i] = un[f];
+            *po = un[f];
+            po += g.ncell;
         }
+        lin += plane_cells;
         if constexpr (STAGE == 2) {
 #pragma unroll
             for (int f = 0; f < 5; ++f) unp[f] = un[f];
-        }
-#pragma unroll
-        for (int f = 0; f < 5; ++f) {
-            Wz0[f] = Wz1[f];
-            Wz1[f] = Wz2[f];
-            hz[f] = hz1[f];
-            Fzlo[f] = Fzhi[f];
         }
     }
     if constexpr (STAGE == 2) invdt = cfl_term(unp, g, invdt);  // the item's last plane
