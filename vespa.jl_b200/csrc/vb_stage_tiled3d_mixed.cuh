@@ -59,12 +59,15 @@ struct Smem {
     uint64_t bar[NS];
 };
 
-// minmod slope of (l, c, r), scalar
+// minmod slope of (l, c, r) (limited_slope, src/reconstruct.jl:6-16) as a
+// clamp: minmod(a, b) = a clamped to [min(0, b), max(0, b)].  Four min/max
+// instead of a product, two compares and two selects; the value equals the
+// reference's except where a * b underflows to zero in float32 (then the
+// reference gives 0 and the clamp the smaller difference, both below 1e-22).
 __device__ __forceinline__ float mm(float l, float c, float r)
 {
     const float a = c - l, b = r - c;
-    if (a * b <= 0.f) return 0.f;
-    return fabsf(a) < fabsf(b) ? a : b;
+    return fminf(fmaxf(a, fminf(0.f, b)), fmaxf(0.f, b));
 }
 
 // cons2prim for VB_MIXED (src/eos.jl:8-25): velocities and the
@@ -115,15 +118,6 @@ __device__ __forceinline__ double cfl_term2d(const double un[5], const Geom &g, 
 
 namespace t3m {
 
-// minmod slopes of two packed differences (same algebra as mm)
-__device__ __forceinline__ f2 minmod2(f2 a, f2 b)
-{
-    const f2 pr = a * b;
-    const float sx = pr.v.x <= 0.f ? 0.f : (fabsf(a.v.x) < fabsf(b.v.x) ? a.v.x : b.v.x);
-    const float sy = pr.v.y <= 0.f ? 0.f : (fabsf(a.v.y) < fabsf(b.v.y) ? a.v.y : b.v.y);
-    return f2(sx, sy);
-}
-
 // Left / right states of a packed face pair, lane x an x face and lane y a y
 // face, each reconstructed from the four cells across it (ring offsets o[0..3]
 // along the face normal: two cells behind the face, two ahead).  Components
@@ -138,8 +132,13 @@ __device__ __forceinline__ void face_pair(const float *wk, const int ox[4], cons
         const float *px = wk + fx * PC, *py = wk + fy * PC;
         const f2 a0(px[ox[0]], py[oy[0]]), a1(px[ox[1]], py[oy[1]]);
         const f2 a2(px[ox[2]], py[oy[2]]), a3(px[ox[3]], py[oy[3]]);
-        const f2 d2 = a2 - a1;
-        const f2 sl = minmod2(a1 - a0, d2), sc = minmod2(d2, a3 - a2);
+        // the slopes of the cells behind and ahead of the face share the
+        // difference across it, so they share the clamp bounds (see mm)
+        const f2 d1 = a1 - a0, d2 = a2 - a1, d3 = a3 - a2;
+        const float lox = fminf(0.f, d2.v.x), hix = fmaxf(0.f, d2.v.x);
+        const float loy = fminf(0.f, d2.v.y), hiy = fmaxf(0.f, d2.v.y);
+        const f2 sl(fminf(fmaxf(d1.v.x, lox), hix), fminf(fmaxf(d1.v.y, loy), hiy));
+        const f2 sc(fminf(fmaxf(d3.v.x, lox), hix), fminf(fmaxf(d3.v.y, loy), hiy));
         l[j] = fma2(f2::splat(0.5f), sl, a1);
         r[j] = fma2(f2::splat(-0.5f), sc, a2);
     }
