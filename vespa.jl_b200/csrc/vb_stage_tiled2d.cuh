@@ -89,7 +89,11 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
     const double ax = g.area[0], ay = g.area[1];
     const T half = T(0.5), mhalf = T(-0.5);
 
-    auto slope = [](T l, T c, T r) -> T { return limited_slope<T>(l, c, r); };
+    // float32 slopes use the clamp form of minmod (t3m::mm), float64 the reference's
+    auto slope = [](T l, T c, T r) -> T {
+        if constexpr (MIXED) return t3m::mm(l, c, r);
+        else return limited_slope<T>(l, c, r);
+    };
     auto to_prim = [&](const double uu[5], T W[5]) {
         if constexpr (MIXED) {
             t3m::cons2prim_mixed(uu, gamma, W);

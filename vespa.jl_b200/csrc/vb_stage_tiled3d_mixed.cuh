@@ -92,16 +92,18 @@ __device__ __forceinline__ void cons2prim_mixed(const double U[5], double g, flo
 
 // VB_MIXED CFL term of a new float64 state: compute_dt's (|v_d| + c) / w_d
 // (src/driver.jl:178-185) from the mixed primitives, wave speeds in float32
-// (a dt estimate within float32 rounding of the float64 one), max in float64.
-__device__ __forceinline__ double cfl_term(const double un[5], const Geom &g, double m)
+// (a dt estimate within float32 rounding of the float64 one).  The running
+// maximum m stays in float32 (the conversion to float64 is exact and
+// monotonic, so the maximum is the same); NaN wins, as in nan_max.
+__device__ __forceinline__ float cfl_term(const double un[5], double gamma, float gf, float iw0,
+                                          float iw1, float iw2, float m)
 {
     float W[5];
-    cons2prim_mixed(un, g.gamma, W);
-    const float cs = sqrt_approx((float)g.gamma * W[4] * rcp_approx(W[0]));
-    const float t = fmaxf(fmaxf((fabsf(W[1]) + cs) * (float)g.invw[0],
-                                (fabsf(W[2]) + cs) * (float)g.invw[1]),
-                          (fabsf(W[3]) + cs) * (float)g.invw[2]);
-    return nan_max(m, (double)t);
+    cons2prim_mixed(un, gamma, W);
+    const float cs = sqrt_approx(gf * W[4] * rcp_approx(W[0]));
+    const float t = fmaxf(fmaxf((fabsf(W[1]) + cs) * iw0, (fabsf(W[2]) + cs) * iw1),
+                          (fabsf(W[3]) + cs) * iw2);
+    return (t > m || t != t) ? t : m;
 }
 
 // the same over x and y only (2D grids)
@@ -226,6 +228,8 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     const int bx_lo = g.bc_lo[0], bx_hi = g.bc_hi[0], by_lo = g.bc_lo[1], by_hi = g.bc_hi[1];
     const int bz_lo = g.bc_lo[2], bz_hi = g.bc_hi[2];
     double invdt = 0.0;
+    float invdtf = 0.f;  // running CFL maximum of this item
+    const float iw0 = (float)g.invw[0], iw1 = (float)g.invw[1], iw2 = (float)g.invw[2];
     const int local = item - B.item0;
     const int tile = local % ntiles;
     const int x0 = (tile % ntx) * TX, y0 = (tile / ntx) * TY;
@@ -436,15 +440,15 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         {
             float Wn[5];
             consume(q, Wn, 2);
-            double cf = 0.0;
-            if constexpr (STAGE == 2) cf = cfl_term(unp, g, invdt);
+            float cf = 0.f;
+            if constexpr (STAGE == 2) cf = cfl_term(unp, gamma, gf, iw0, iw1, iw2, invdtf);
             if (z_early) {
                 zsolve(k, w0 + o_c, w1 + o_c, Wn, Fzhi);
             } else {
                 halo_c2p(q);
             }
             if constexpr (STAGE == 2)
-                if (k > k0) invdt = cf;
+                if (k > k0) invdtf = cf;
         }
         __syncthreads();  // (1) plane k+2 converted
         release(q);
@@ -511,7 +515,8 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
             for (int f = 0; f < 5; ++f) unp[f] = un[f];
         }
     }
-    if constexpr (STAGE == 2) invdt = cfl_term(unp, g, invdt);  // the item's last plane
+    if constexpr (STAGE == 2)  // the item's last plane
+        invdt = (double)cfl_term(unp, gamma, gf, iw0, iw1, iw2, invdtf);
     qb += nplanes;
     if (timed_out && t == 0) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
     if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);  // this box's CFL max
