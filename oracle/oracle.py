@@ -36,6 +36,17 @@ class VoGrid(C.Structure):
     ]
 
 
+class VoGravity(C.Structure):
+    _fields_ = [
+        ("G", C.c_double),
+        ("tol", C.c_double),
+        ("bc_lo", C.c_int32 * 3),
+        ("bc_hi", C.c_int32 * 3),
+        ("maxiter", C.c_int32),
+        ("project_mean", C.c_int32),
+    ]
+
+
 def build() -> str:
     """Compile the oracle with its Makefile (idempotent)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -101,6 +112,14 @@ def lib():
         L.vo_amr_evolve.argtypes = [vp, C.c_double, i64, C.c_double, C.c_int, C.c_int, C.c_int]
         L.vo_amr_evolve.restype = i64
         L.vo_amr_totals.argtypes = [vp, dp]
+        gvp = C.POINTER(VoGravity)
+        L.vo_grav_laplacian.argtypes = [gp, gvp, dp, dp]
+        L.vo_grav_solve.argtypes = [gp, gvp, dp, dp, dp]
+        L.vo_grav_solve.restype = i64
+        L.vo_grav_accel.argtypes = [gp, gvp, dp, dp]
+        L.vo_compute_dt_gravity.argtypes = [gp, C.c_double, dp]
+        L.vo_compute_dt_gravity.restype = C.c_double
+        L.vo_step_gravity.argtypes = [gp, dp, dp, dp, dp, C.c_double]
         _lib = L
     return _lib
 
@@ -318,3 +337,55 @@ class Amr:
         out = np.empty(5)
         lib().vo_amr_totals(self.h, _dp(out))
         return out
+
+
+# ------------------------------------------------------------ self-gravity
+def make_gravity(G, bc_lo, bc_hi, maxiter=500, tol=1e-8, project_mean=True) -> VoGravity:
+    """Gravity descriptor; ``bc_lo/bc_hi`` are phi's per-axis codes (length 1-3)."""
+    P = VoGravity()
+    P.G = float(G)
+    P.tol = float(tol)
+    for d in range(3):
+        P.bc_lo[d] = int(bc_lo[d]) if d < len(bc_lo) else BC_PERIODIC
+        P.bc_hi[d] = int(bc_hi[d]) if d < len(bc_hi) else BC_PERIODIC
+    P.maxiter = int(maxiter)
+    P.project_mean = int(bool(project_mean))
+    return P
+
+
+def grav_laplacian(g: VoGrid, P: VoGravity, x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    lib().vo_grav_laplacian(C.byref(g), C.byref(P), _dp(x), _dp(out))
+    return out
+
+
+def grav_solve(g: VoGrid, P: VoGravity, U, phi):
+    """solve_poisson! in place on ``phi`` (warm start); returns (iters, relres)."""
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    assert phi.dtype == np.float64 and phi.flags.c_contiguous
+    rr = np.zeros(1)
+    it = lib().vo_grav_solve(C.byref(g), C.byref(P), _dp(U), _dp(phi), _dp(rr))
+    return int(it), float(rr[0])
+
+
+def grav_accel(g: VoGrid, P: VoGravity, phi):
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    out = np.empty((g.ndim, phi.size))
+    lib().vo_grav_accel(C.byref(g), C.byref(P), _dp(phi), _dp(out))
+    return out
+
+
+def compute_dt_gravity(g: VoGrid, G, U) -> float:
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    return float(lib().vo_compute_dt_gravity(C.byref(g), float(G), _dp(U)))
+
+
+def step_gravity(g: VoGrid, gacc, U, dt):
+    """One SSP-RK2 step with the gravity source (field gacc held), in place on U."""
+    assert U.dtype == np.float64 and U.flags.c_contiguous
+    gacc = np.ascontiguousarray(gacc, dtype=np.float64)
+    u0 = np.empty_like(U)
+    acc = np.empty_like(U)
+    lib().vo_step_gravity(C.byref(g), _dp(gacc), _dp(U), _dp(u0), _dp(acc), float(dt))
+    return U

@@ -630,3 +630,215 @@ void vo_exact_riemann_sample(const double *WL, const double *WR, double g, doubl
         }
     }
 }
+
+/* ----------------------------------------------------------- src/gravity.jl */
+/* Self-gravity on the uniform mesh.  The potential phi carries its own
+ * boundary codes (periodic wraps; any other code is the homogeneous Neumann
+ * wall of _lap_face!, src/gravity.jl:126-127). */
+
+#define VO_FOURPI (4.0 * 3.14159265358979323846) /* FOURPI, src/gravity.jl:21 */
+
+/* neighbour of `lin` across (d, hi) under phi's boundary codes, -1 at a wall */
+static inline int64_t grav_nb(const vo_gravity *P, const geom_t *G, int64_t lin, int d, int hi)
+{
+    int64_t c = coord_of(G, lin, d);
+    int64_t n = G->n[d];
+    int64_t j = c + (hi ? 1 : -1);
+    if (j >= 0 && j < n) return lin + (j - c) * G->stride[d];
+    int bc = hi ? P->bc_hi[d] : P->bc_lo[d];
+    if (bc == VO_BC_PERIODIC) return lin + ((j < 0 ? n - 1 : 0) - c) * G->stride[d];
+    return -1;
+}
+
+/* (A x)[lin] with A = -lap * V, src/gravity.jl:325-334 (_lap_csr_cpu!):
+ * s = sum_k coef_k * (x_c - x_nb(k)) over the row of the CSR adjacency that
+ * _assemble_poisson_struct (src/gravity.jl:514-545) builds from for_each_face.
+ * A row lists its faces in emission order: lo faces emitted by a lower cell
+ * (z, y, x: ascending emitter index), then the cell's own hi faces (x, y, z),
+ * then lo faces emitted by a periodic partner above it (x, y, z).  A 1-cell
+ * periodic axis yields the self face (c, c) twice, at its hi position.
+ * coef = area / face distance = area_d / (0.5 * (w_d + w_d)). */
+static double grav_row(const vo_gravity *P, const geom_t *G, const double *x, int64_t lin)
+{
+    const double xc = x[lin];
+    double s = 0.0;
+    double coef[3];
+    for (int d = 0; d < G->nd; ++d) coef[d] = G->area[d] / (0.5 * (G->w[d] + G->w[d]));
+    for (int d = G->nd - 1; d >= 0; --d) {
+        int64_t nb = grav_nb(P, G, lin, d, 0);
+        if (nb >= 0 && nb < lin) s += coef[d] * (xc - x[nb]);
+    }
+    for (int d = 0; d < G->nd; ++d) {
+        int64_t nb = grav_nb(P, G, lin, d, 1);
+        if (nb < 0) continue;
+        s += coef[d] * (xc - x[nb]);
+        if (nb == lin) s += coef[d] * (xc - x[nb]); /* 1-cell periodic axis: the self face's second entry */
+    }
+    for (int d = 0; d < G->nd; ++d) {
+        int64_t nb = grav_nb(P, G, lin, d, 0);
+        if (nb > lin) s += coef[d] * (xc - x[nb]);
+    }
+    return s;
+}
+
+void vo_grav_laplacian(const vo_grid *g, const vo_gravity *P, const double *x, double *out)
+{
+    geom_t G;
+    make_geom(g, &G);
+    for (int64_t lin = 0; lin < G.ncell; ++lin) out[lin] = grav_row(P, &G, x, lin);
+}
+
+static double dot64(const double *a, const double *b, int64_t n)
+{
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+
+/* _rhs_flat_kernel!, src/gravity.jl:215-231 (no particles, no cosmology):
+ * b = -4 pi G (rho - rhobar) V, rhobar the volume-weighted mean when the
+ * constant null mode is projected out. */
+static void grav_rhs(const vo_gravity *P, const geom_t *G, const double *U, double *b)
+{
+    double rhobar = 0.0;
+    if (P->project_mean) {
+        double s = 0.0, vsum = 0.0;
+        for (int64_t i = 0; i < G->ncell; ++i) {
+            s += U[i] * G->vol;
+            vsum += G->vol;
+        }
+        rhobar = s / vsum;
+    }
+    for (int64_t i = 0; i < G->ncell; ++i)
+        b[i] = -VO_FOURPI * P->G * (U[i] - rhobar) * G->vol * 1.0;
+}
+
+/* solve_poisson! on the CPU path, src/gravity.jl:251-300 (_cg_csr_run!):
+ * warm start from phi, plain CG on A = -lap * V, then the volume-weighted
+ * mean removed when project_mean.  Returns the iteration count. */
+int64_t vo_grav_solve(const vo_grid *g, const vo_gravity *P, const double *U, double *phi,
+                      double *relres_out)
+{
+    geom_t G;
+    make_geom(g, &G);
+    const int64_t n = G.ncell;
+    double *b = calloc((size_t)n + 1, sizeof(double)), *r = calloc((size_t)n + 1, sizeof(double));
+    double *p = calloc((size_t)n + 1, sizeof(double)), *Ap = calloc((size_t)n + 1, sizeof(double));
+    grav_rhs(P, &G, U, b);
+    vo_grav_laplacian(g, P, phi, Ap);
+    for (int64_t i = 0; i < n; ++i) r[i] = b[i] - Ap[i];
+    memcpy(p, r, sizeof(double) * n);
+    double rsold = dot64(r, r, n);
+    double bnorm = sqrt(dot64(b, b, n));
+    if (bnorm == 0.0) bnorm = 1.0;
+    int64_t iters = 0;
+    double relres = sqrt(rsold) / bnorm;
+    for (int64_t k = 1; k <= P->maxiter; ++k) {
+        iters = k;
+        vo_grav_laplacian(g, P, p, Ap);
+        double pAp = dot64(p, Ap, n);
+        if (pAp <= 0.0) break;
+        double alpha = rsold / pAp;
+        for (int64_t i = 0; i < n; ++i) {
+            phi[i] += alpha * p[i];
+            r[i] -= alpha * Ap[i];
+        }
+        double rsnew = dot64(r, r, n);
+        relres = sqrt(rsnew) / bnorm;
+        if (relres <= P->tol) break;
+        double beta = rsnew / rsold;
+        for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * p[i];
+        rsold = rsnew;
+    }
+    if (P->project_mean) {
+        double s = 0.0, vsum = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            s += G.vol * phi[i];
+            vsum += G.vol;
+        }
+        double mu = s / vsum;
+        for (int64_t i = 0; i < n; ++i) phi[i] -= mu;
+    }
+    free(b); free(r); free(p); free(Ap);
+    if (relres_out) *relres_out = relres;
+    return iters;
+}
+
+/* g = -grad phi per cell, _gax (src/gravity.jl:387-394): central difference
+ * over the two face distances; across a wall the neighbour value is the
+ * cell's own and the distance half a width.  gacc[d * ncell + lin], d < nd. */
+void vo_grav_accel(const vo_grid *g, const vo_gravity *P, const double *phi, double *gacc)
+{
+    geom_t G;
+    make_geom(g, &G);
+    for (int64_t lin = 0; lin < G.ncell; ++lin) {
+        const double pc = phi[lin];
+        for (int d = 0; d < G.nd; ++d) {
+            int64_t lo = grav_nb(P, &G, lin, d, 0), hi = grav_nb(P, &G, lin, d, 1);
+            double wlo = lo < 0 ? pc : phi[lo], whi = hi < 0 ? pc : phi[hi];
+            double fd = 0.5 * (G.w[d] + G.w[d]); /* _face_distance */
+            double dlo = lo < 0 ? 0.5 * G.w[d] : fd, dhi = hi < 0 ? 0.5 * G.w[d] : fd;
+            gacc[(int64_t)d * G.ncell + lin] = -(whi - wlo) / (dlo + dhi);
+        }
+    }
+}
+
+/* apply_gravity_source! (src/gravity.jl:419-437) into acc, from the stage
+ * state U: +rho g on momentum and +rho v.g on energy, pushed with a minus
+ * sign because the stage update subtracts acc (_grav_src_tuple, 371-382). */
+static void grav_source(const geom_t *G, const double *U, const double *gacc, double *acc)
+{
+    const int64_t n = G->ncell;
+    const double V = G->vol;
+    for (int64_t lin = 0; lin < n; ++lin) {
+        double gv[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < G->nd; ++d) gv[d] = gacc[(int64_t)d * n + lin];
+        const double rho = U[lin];
+        double es = 0.0;
+        for (int d = 0; d < 3; ++d) es += U[(int64_t)(1 + d) * n + lin] * gv[d];
+        const double esV = es * V;
+        acc[lin] += 0.0;
+        for (int d = 0; d < 3; ++d) acc[(int64_t)(1 + d) * n + lin] += -(rho * gv[d] * V);
+        acc[4 * n + lin] += -esV;
+    }
+}
+
+/* compute_dt with the free-fall limiter (src/driver.jl:169-199 with
+ * _gravity_invdt, src/gravity.jl:439-441): invdt also takes
+ * sqrt(4 pi G rho) / 0.5 over cells with rho > 0. */
+double vo_compute_dt_gravity(const vo_grid *g, double Ggrav, const double *U)
+{
+    geom_t G;
+    make_geom(g, &G);
+    double invdt = 0.0, ginv = 0.0;
+    double W[5];
+    for (int64_t lin = 0; lin < G.ncell; ++lin) {
+        prim_at(g, &G, U, lin, W);
+        double c = sqrt(g->gamma * W[4] / W[0]);
+        for (int d = 0; d < G.nd; ++d) invdt = jl_max(invdt, (fabs(W[1 + d]) + c) / G.w[d]);
+        double gi = W[0] > 0.0 ? sqrt(VO_FOURPI * Ggrav * W[0]) / 0.5 : 0.0;
+        ginv = jl_max(ginv, gi);
+    }
+    invdt = jl_max(invdt, ginv);
+    if (invdt == 0.0) return INFINITY;
+    return g->cfl / invdt;
+}
+
+/* step! with self-gravity (src/driver.jl:333-359): the source follows each
+ * accumulate_flux! with the gravity field held over the step.  Serial face
+ * enumeration (mode 0 of vo_step). */
+void vo_step_gravity(const vo_grid *g, const double *gacc, double *U, double *u0, double *acc,
+                     double dt)
+{
+    geom_t G;
+    make_geom(g, &G);
+    int64_t n5 = 5 * G.ncell;
+    memcpy(u0, U, sizeof(double) * n5);
+    vo_accumulate_flux(g, U, acc, NULL, 0.0);
+    grav_source(&G, U, gacc, acc);
+    double invV = dt / (g->aexp * G.vol);
+    for (int64_t i = 0; i < n5; ++i) U[i] = u0[i] - invV * acc[i];
+    vo_accumulate_flux(g, U, acc, NULL, 0.0);
+    grav_source(&G, U, gacc, acc);
+    for (int64_t i = 0; i < n5; ++i) U[i] = 0.5 * u0[i] + 0.5 * (U[i] - invV * acc[i]);
+}

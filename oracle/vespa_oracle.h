@@ -65,6 +65,24 @@ int64_t vo_evolve(const vo_grid *g, double *U, double *u0, double *acc, double t
 void vo_conserved_totals(const vo_grid *g, const double *U, double *out);
 int64_t vo_bflux_size(const vo_grid *g);
 
+/* self-gravity on the uniform mesh (src/gravity.jl): phi's own boundary codes
+ * (VO_BC_PERIODIC wraps, anything else is a homogeneous Neumann wall) */
+typedef struct {
+    double G;
+    double tol;
+    int32_t bc_lo[3];
+    int32_t bc_hi[3];
+    int32_t maxiter;
+    int32_t project_mean;
+} vo_gravity;
+void vo_grav_laplacian(const vo_grid *g, const vo_gravity *P, const double *x, double *out);
+int64_t vo_grav_solve(const vo_grid *g, const vo_gravity *P, const double *U, double *phi,
+                      double *relres);
+void vo_grav_accel(const vo_grid *g, const vo_gravity *P, const double *phi, double *gacc);
+double vo_compute_dt_gravity(const vo_grid *g, double G, const double *U);
+void vo_step_gravity(const vo_grid *g, const double *gacc, double *U, double *u0, double *acc,
+                     double dt);
+
 /* exact Riemann solver (src/exact_riemann.jl) */
 void vo_exact_riemann_star(const double *WL, const double *WR, double gamma, double *pu);
 void vo_exact_riemann_sample(const double *WL, const double *WR, double gamma, double s,
