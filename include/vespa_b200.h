@@ -199,6 +199,50 @@ int vb_bflux_size(const vb_grid *grid, int64_t *n);
 int vb_bflux_read(vb_grid *grid, double *out, int64_t n);
 int vb_bflux_clear(vb_grid *grid);
 
+/* Self-gravity on a uniform grid (src/gravity.jl): enable_gravity!,
+ * solve_poisson!, apply_laplacian!, and the source g = -grad phi that
+ * step!/evolve! add after each flux accumulation (+rho g on momentum, +rho v.g
+ * on energy), with the free-fall limiter sqrt(4 pi G rho)/0.5 in compute_dt.
+ *
+ * The potential phi carries its own boundary codes: VB_BC_PERIODIC wraps,
+ * any other code is a homogeneous Neumann wall.  The solver is matrix-free
+ * conjugate gradients on A = -lap * V (the reference's operator, rows summed
+ * in its order), warm-started from the stored phi, stopping when
+ * ||r|| / ||b|| <= tol or after maxiter iterations; project_mean removes the
+ * constant null mode of a fully periodic box (the reference's default for
+ * periodic bcs).  Inner products are deterministic tree sums, so a solve
+ * agrees with the reference's serial sums to the tolerance.
+ *
+ * While gravity is enabled: vb_evolve and vb_run_steps_async solve once per
+ * step before the stages (evolve!, src/driver.jl:498) and synchronise with
+ * the host for it; vb_step uses the field of the last solve (or set_phi), as
+ * step! does; the stages take the cell-centric kernel.  The adjoint refuses
+ * a grid with gravity (VB_ENOTSUP). */
+typedef struct {
+    double G;          /* gravitational constant, code units */
+    double tol;        /* relative residual target */
+    int64_t maxiter;   /* CG iteration cap */
+    int32_t bc_lo[3];  /* phi's boundary codes per axis */
+    int32_t bc_hi[3];
+    int32_t project_mean;
+    int32_t flags;     /* must be 0 */
+} vb_gravity_desc;
+
+/* Enable (or reconfigure: phi is kept) gravity; phi starts at 0. */
+int vb_gravity_enable(vb_grid *grid, const vb_gravity_desc *desc);
+int vb_gravity_disable(vb_grid *grid);
+/* solve_poisson!: iteration count and final relative residual. */
+int vb_gravity_solve(vb_grid *grid, int64_t *iters, double *relres);
+/* phi (ncell values, the state's cell order), read and written; writing it
+ * recomputes g for the next vb_step. */
+int vb_gravity_phi(vb_grid *grid, double *phi);
+int vb_gravity_set_phi(vb_grid *grid, const double *phi);
+/* g = -grad phi (ndim * ncell values, axis-major), as the stages use it. */
+int vb_gravity_accel(vb_grid *grid, double *g);
+/* Ax = A x with A = -lap * V: apply_laplacian!'s operator (src/gravity.jl:96-133)
+ * in the row form of _lap_csr_cpu! (325-334), the one the solver iterates. */
+int vb_gravity_laplacian(vb_grid *grid, const double *x, double *Ax);
+
 /* Adjoint of the float64 SSP-RK2 step on a periodic grid (no counterpart in
  * the reference, which has no adjoint; it differentiates the map that
  * step!/evolve! apply, src/driver.jl:285-359,483-508).  Reverse mode, written

@@ -76,6 +76,7 @@ int check_grid(const vb_grid *gr)
     for (int a = 0; a < gr->g.nd; ++a)
         if (gr->g.bc_lo[a] != vb::BC_PERIODIC || gr->g.bc_hi[a] != vb::BC_PERIODIC)
             return fail(VB_ENOTSUP, "the adjoint supports periodic boundaries only");
+    if (gr->grav) return fail(VB_ENOTSUP, "the adjoint does not differentiate the gravity source");
     return VB_OK;
 }
 
@@ -178,7 +179,9 @@ int vb_adjoint_forward(vb_adjoint *a, double tfinal, int64_t max_steps, double *
     if (!a) return fail(VB_EINVAL, "null adjoint");
     vb_grid *gr = a->grid;
     if (max_steps < 0 || max_steps > a->max_steps) max_steps = a->max_steps;
-    int rc = use(gr->ctx);
+    int rc = check_grid(gr);  // gravity may have been enabled since creation
+    if (rc) return rc;
+    rc = use(gr->ctx);
     if (rc) return rc;
     cudaStream_t s = gr->ctx->stream;
     rc = vb::detail::grid_pull_ctrl(gr);

@@ -265,7 +265,7 @@ int sync_box(vb_grid *gr)
 int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout)
 {
     double *bf = gr->bflux_on ? gr->bflux : nullptr;
-    if (gr->tiled && !bf) {
+    if (gr->tiled && !bf && !gr->grav) {
         int rc = sync_box(gr);
         if (rc) return rc;
         const int64_t items = box_items(gr->g, gr->kz);
@@ -321,11 +321,21 @@ int ensure_cfl(vb_grid *gr)
     return VB_OK;
 }
 
-// Queue `count` CFL-limited steps (each: finalize dt, stage 1, stage 2).
+// Queue `count` CFL-limited steps (each: finalize dt, stage 1, stage 2).  With
+// self-gravity each active step first solves the Poisson problem for its
+// starting density (evolve!, src/driver.jl:498; dt does not depend on phi,
+// so finalising first is the same); that solve synchronises with the host.
 int queue_direct(vb_grid *gr, int64_t count)
 {
     for (int64_t i = 0; i < count; ++i) {
         VB_CHECK_LAUNCH(gr->ctx, vb::launch_finalize_cfl(gr->g, gr->ctrl, gr->ctx->stream));
+        if (gr->grav) {
+            int rc = pull_ctrl(gr);
+            if (rc) return rc;
+            if (!gr->hctrl->active) return VB_OK;
+            rc = vb::detail::gravity_solve(gr, nullptr, nullptr);
+            if (rc) return rc;
+        }
         int rc = rk2(gr);
         if (rc) return rc;
     }
@@ -375,7 +385,7 @@ int capture_steps(vb_grid *gr)
 // launch directly.
 int queue_steps(vb_grid *gr, int64_t count)
 {
-    while (gr->warmed && count >= GRAPH_STEPS) {
+    while (gr->warmed && count >= GRAPH_STEPS && !gr->grav) {
         if (!gr->gexec || gr->gkey != graph_key(gr)) {
             int rc = capture_steps(gr);
             if (rc) return rc;
@@ -618,7 +628,7 @@ int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
     if (!gr || nsteps < 1) return fail(VB_EINVAL, "bad argument");
     int rc = use(gr->ctx);
     if (rc) return rc;
-    if (!gr->tiled || gr->bflux_on) {
+    if (!gr->tiled || gr->bflux_on || gr->grav) {
         if (best_kz) *best_kz = gr->kz;
         if (best_ms) *best_ms = 0.0;
         return VB_OK;
@@ -730,6 +740,7 @@ int vb_grid_destroy(vb_grid *gr)
         cudaStreamSynchronize(gr->ctx->stream);
     }
     if (gr->gexec) cudaGraphExecDestroy(gr->gexec);
+    vb::detail::gravity_free(gr->grav);
     cudaFree(gr->U);
     cudaFree(gr->U1);
     cudaFree(gr->ctrl);

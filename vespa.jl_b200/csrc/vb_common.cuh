@@ -27,7 +27,44 @@ struct Geom {
     double gamma;
     double cfl;
     double aexp;
+    // self-gravity (src/gravity.jl), set while a grid has gravity enabled:
+    // grav_g = g = -grad phi per cell (nd * ncell doubles, axis-major), held
+    // over a step; grav_G = the constant G of the free-fall dt limiter
+    const double *grav_g;
+    double grav_G;
 };
+
+// 4 pi, as FOURPI in src/gravity.jl:21
+constexpr double VB_FOURPI = 4.0 * 3.14159265358979323846;
+
+// _gravity_invdt, src/gravity.jl:439-441: the free-fall rate bound sqrt(4 pi G rho) / 0.5
+__device__ __forceinline__ double gravity_invdt(double G, double rho)
+{
+    return rho > 0.0 ? __dsqrt_rn(__dmul_rn(__dmul_rn(VB_FOURPI, G), rho)) / 0.5 : 0.0;
+}
+
+// apply_gravity_source! for one cell (src/gravity.jl:371-382, 419-437):
+// acc += (0, -rho g V, -(rho v . g) V) from the stage state u, with g zero on
+// the axes beyond ND.  Every product and sum rounded separately, in the
+// reference's order.
+template <int ND>
+__device__ __forceinline__ void gravity_source(const Geom &g, int64_t lin, const double u[5],
+                                               double acc[5])
+{
+    double gv[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < ND; ++d) gv[d] = g.grav_g[d * g.ncell + lin];
+    const double rho = u[0], V = g.vol;
+    double es = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) es = __dadd_rn(es, __dmul_rn(u[1 + d], gv[d]));
+    const double esV = __dmul_rn(es, V);
+    acc[0] = __dadd_rn(acc[0], 0.0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        acc[1 + d] = __dadd_rn(acc[1 + d], -__dmul_rn(__dmul_rn(rho, gv[d]), V));
+    acc[4] = __dadd_rn(acc[4], -esV);
+}
 
 // Per-grid control block in device memory.  The stepping kernels read dt and
 // invV from here so a whole evolve! loop can run without host round trips.

@@ -1,0 +1,608 @@
+// vb_gravity.cu -- self-gravity on uniform grids (src/gravity.jl): the
+// Poisson solve nabla^2 phi = 4 pi G rho by matrix-free conjugate gradients on
+// the device, and the field g = -grad phi that the stage kernels add as a
+// source (gravity_source in vb_common.cuh) while the grid has gravity enabled.
+//
+// Compiled with -fmad=false: the operator row, the field and the CG vector
+// updates round every product and sum separately, like the reference's Julia
+// loops.  The operator row is summed in the reference's CSR order
+// (_assemble_poisson_struct, src/gravity.jl:514-545), so A x is bit-identical
+// to the reference's _lap_csr_cpu! (325-334).  The CG inner products are
+// deterministic block-tree sums (fixed partial count and order) rather than
+// the reference's serial sums, so a solve matches the reference's to the
+// solver tolerance, not bit for bit.
+//
+// Every pass is a grid-stride loop over cells in x-fastest order: an HBM
+// stream of the CG vectors (the stencil's neighbours come from L1/L2).  One
+// CG iteration is five launches (matvec + p.Ap partials, alpha, vector update
+// + r.r partials, beta, direction update); groups of iterations replay as one
+// CUDA graph, each launch returning at once after convergence, and the host
+// reads the stop flag between groups.
+#include <cmath>
+#include <cstring>
+
+#include "vb_internal.h"
+
+namespace vb {
+namespace {
+
+constexpr int GB = 256;  // threads per block
+constexpr int GP = 592;  // blocks (= partial sums) per reduction pass: 4 per SM, fixed
+constexpr int GRAPH_ITERS = 8;
+
+struct GravCtrl {
+    double rhobar, rsold, pAp, alpha, beta, bnorm, relres, mu;
+    long long iters, maxiter;
+    int done, pad;
+    double tol;
+};
+
+// phi's boundary codes and the operator's per-axis coefficient area / distance
+struct GravP {
+    int per_lo[3], per_hi[3];  // 1: periodic side
+    double coef[3];
+    double G;
+    int project_mean;
+};
+
+// neighbour of `lin` (coordinate c on axis d) across its lo or hi face under
+// phi's codes; -1 at a wall (homogeneous Neumann)
+__device__ __forceinline__ int64_t gnb(const Geom &g, const GravP &P, int64_t lin, int64_t c,
+                                       int d, bool hi)
+{
+    const int64_t n = g.n[d];
+    const int64_t j = hi ? c + 1 : c - 1;
+    if (j >= 0 && j < n) return hi ? lin + g.stride[d] : lin - g.stride[d];
+    if (hi ? P.per_hi[d] : P.per_lo[d]) return lin + ((j < 0 ? n - 1 : 0) - c) * g.stride[d];
+    return -1;
+}
+
+__device__ __forceinline__ void coords(const Geom &g, int64_t lin, int64_t cc[3])
+{
+    cc[0] = lin % g.n[0];
+    cc[1] = (lin / g.n[0]) % g.n[1];
+    cc[2] = lin / (g.n[0] * g.n[1]);
+}
+
+// (A x)[lin], A = -nabla^2 V: sum over the row's faces of coef * (x_c - x_nb),
+// in the order the reference's CSR row lists them: lo faces emitted by a lower
+// cell (z, y, x), the cell's own hi faces (x, y, z; a 1-cell periodic axis
+// lists its self face twice), lo faces emitted by a periodic partner above
+// (x, y, z).
+template <int ND>
+__device__ __forceinline__ double lap_row(const Geom &g, const GravP &P, const double *__restrict__ x,
+                                          int64_t lin)
+{
+    int64_t cc[3];
+    coords(g, lin, cc);
+    const double xc = x[lin];
+    double s = 0.0;
+#pragma unroll
+    for (int d = ND - 1; d >= 0; --d) {
+        const int64_t nb = gnb(g, P, lin, cc[d], d, false);
+        if (nb >= 0 && nb < lin) s = s + P.coef[d] * (xc - x[nb]);
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        const int64_t nb = gnb(g, P, lin, cc[d], d, true);
+        if (nb < 0) continue;
+        s = s + P.coef[d] * (xc - x[nb]);
+        if (nb == lin) s = s + P.coef[d] * (xc - x[nb]);
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        const int64_t nb = gnb(g, P, lin, cc[d], d, false);
+        if (nb > lin) s = s + P.coef[d] * (xc - x[nb]);
+    }
+    return s;
+}
+
+// Deterministic block sum of GB values (fixed tree).
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    sh[threadIdx.x] = v;
+    __syncthreads();
+#pragma unroll
+    for (int s = GB / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// Sum of the GP partials part[0..GP) by one block of 1024 threads (fixed tree).
+__device__ __forceinline__ double final_sum(const double *part, double *sh)
+{
+    const int t = threadIdx.x;
+    sh[t] = t < GP ? part[t] : 0.0;
+    __syncthreads();
+    for (int s = 512; s > 0; s >>= 1) {
+        if (t < s) sh[t] = sh[t] + sh[t + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// partials of sum(x * V) and sum(V) (the volume-weighted mean of a field)
+__global__ void __launch_bounds__(GB) k_meanpart(Geom g, const double *__restrict__ x, double *part)
+{
+    __shared__ double sh[GB];
+    double s = 0.0, v = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
+        s = s + x[i] * g.vol;
+        v = v + g.vol;
+    }
+    s = block_sum(s, sh);
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = s;
+        part[GP + blockIdx.x] = v;
+    }
+}
+
+// which = 0: rhobar; 1: mu (the potential's mean)
+__global__ void __launch_bounds__(1024) k_mean_final(const double *part, GravCtrl *gc, int which)
+{
+    __shared__ double sh[1024];
+    const double s = final_sum(part, sh);
+    const double v = final_sum(part + GP, sh);
+    if (threadIdx.x == 0) {
+        if (which == 0) gc->rhobar = s / v;
+        else gc->mu = s / v;
+    }
+}
+
+// _rhs_flat_kernel!, src/gravity.jl:215-231: b = -4 pi G (rho - rhobar) V
+__global__ void __launch_bounds__(GB) k_rhs(Geom g, GravP P, const double *__restrict__ U, double *b,
+                                           const GravCtrl *gc)
+{
+    const double rhobar = P.project_mean ? gc->rhobar : 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB)
+        b[i] = -VB_FOURPI * P.G * (U[i] - rhobar) * g.vol * 1.0;
+}
+
+// CG start, src/gravity.jl:272-279: r = b - A phi, p = r; partials of r.r and b.b
+template <int ND>
+__global__ void __launch_bounds__(GB) k_cg_init(Geom g, GravP P, const double *__restrict__ phi,
+                                               const double *__restrict__ b, double *r, double *p,
+                                               double *part)
+{
+    __shared__ double sh[GB];
+    double rr = 0.0, bb = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
+        const double ri = b[i] - lap_row<ND>(g, P, phi, i);
+        r[i] = ri;
+        p[i] = ri;
+        rr = rr + ri * ri;
+        bb = bb + b[i] * b[i];
+    }
+    rr = block_sum(rr, sh);
+    bb = block_sum(bb, sh);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = rr;
+        part[GP + blockIdx.x] = bb;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_cg_init_final(const double *part, GravCtrl *gc)
+{
+    __shared__ double sh[1024];
+    const double rr = final_sum(part, sh);
+    const double bb = final_sum(part + GP, sh);
+    if (threadIdx.x == 0) {
+        double bnorm = sqrt(bb);
+        if (bnorm == 0.0) bnorm = 1.0;
+        gc->rsold = rr;
+        gc->bnorm = bnorm;
+        gc->relres = sqrt(rr) / bnorm;
+        gc->iters = 0;
+        gc->done = gc->maxiter <= 0 ? 1 : 0;
+    }
+}
+
+// Ap = A p; partials of p.Ap
+template <int ND>
+__global__ void __launch_bounds__(GB) k_cg_matvec(Geom g, GravP P, const double *__restrict__ p,
+                                                 double *Ap, double *part, const GravCtrl *gc)
+{
+    __shared__ double sh[GB];
+    if (gc->done) return;
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
+        const double a = lap_row<ND>(g, P, p, i);
+        Ap[i] = a;
+        s = s + p[i] * a;
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// iters = k; stop when p.Ap <= 0, else alpha = rsold / p.Ap
+__global__ void __launch_bounds__(1024) k_cg_alpha(const double *part, GravCtrl *gc)
+{
+    __shared__ double sh[1024];
+    if (gc->done) return;
+    const double pAp = final_sum(part, sh);
+    if (threadIdx.x == 0) {
+        gc->iters += 1;
+        gc->pAp = pAp;
+        if (pAp <= 0.0) gc->done = 1;
+        else gc->alpha = gc->rsold / pAp;
+    }
+}
+
+// phi += alpha p; r -= alpha Ap; partials of r.r
+__global__ void __launch_bounds__(GB) k_cg_update(Geom g, double *phi, const double *__restrict__ p,
+                                                 double *r, const double *__restrict__ Ap,
+                                                 double *part, const GravCtrl *gc)
+{
+    __shared__ double sh[GB];
+    if (gc->done) return;
+    const double alpha = gc->alpha;
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
+        phi[i] = phi[i] + alpha * p[i];
+        const double ri = r[i] - alpha * Ap[i];
+        r[i] = ri;
+        s = s + ri * ri;
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// relres; stop at tol, else beta = rsnew / rsold; stop after maxiter
+__global__ void __launch_bounds__(1024) k_cg_beta(const double *part, GravCtrl *gc)
+{
+    __shared__ double sh[1024];
+    if (gc->done) return;
+    const double rsnew = final_sum(part, sh);
+    if (threadIdx.x == 0) {
+        gc->relres = sqrt(rsnew) / gc->bnorm;
+        if (gc->relres <= gc->tol) {
+            gc->done = 1;
+            return;
+        }
+        gc->beta = rsnew / gc->rsold;
+        gc->rsold = rsnew;
+        if (gc->iters >= gc->maxiter) gc->done = 1;
+    }
+}
+
+// p = r + beta p
+__global__ void __launch_bounds__(GB) k_cg_dir(Geom g, double *p, const double *__restrict__ r,
+                                              const GravCtrl *gc)
+{
+    if (gc->done) return;
+    const double beta = gc->beta;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB)
+        p[i] = r[i] + beta * p[i];
+}
+
+__global__ void __launch_bounds__(GB) k_sub_mean(Geom g, double *phi, const GravCtrl *gc)
+{
+    const double mu = gc->mu;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB)
+        phi[i] = phi[i] - mu;
+}
+
+// g = -grad phi, _gax (src/gravity.jl:387-394): central difference over the two
+// face distances; across a wall the neighbour value is the cell's own and the
+// distance half a width
+template <int ND>
+__global__ void __launch_bounds__(GB) k_accel(Geom g, GravP P, const double *__restrict__ phi,
+                                             double *gacc)
+{
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
+        int64_t cc[3];
+        coords(g, i, cc);
+        const double pc = phi[i];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const int64_t lo = gnb(g, P, i, cc[d], d, false), hi = gnb(g, P, i, cc[d], d, true);
+            const double wlo = lo < 0 ? pc : phi[lo], whi = hi < 0 ? pc : phi[hi];
+            const double fd = 0.5 * (g.w[d] + g.w[d]);  // _face_distance
+            const double dlo = lo < 0 ? 0.5 * g.w[d] : fd, dhi = hi < 0 ? 0.5 * g.w[d] : fd;
+            gacc[d * g.ncell + i] = -(whi - wlo) / (dlo + dhi);
+        }
+    }
+}
+
+template <int ND>
+__global__ void __launch_bounds__(GB) k_lap(Geom g, GravP P, const double *__restrict__ x, double *out)
+{
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB)
+        out[i] = lap_row<ND>(g, P, x, i);
+}
+
+}  // namespace
+}  // namespace vb
+
+using vb::detail::fail;
+using vb::detail::use;
+
+struct vb_gravity {
+    vb::GravP P{};
+    double *phi = nullptr, *b = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr;
+    double *gacc = nullptr, *part = nullptr;
+    vb::GravCtrl *gc = nullptr;   // device
+    vb::GravCtrl *hgc = nullptr;  // pinned host mirror
+    cudaGraphExec_t gexec = nullptr;
+    int64_t maxiter = 500;
+    double tol = 1e-8;
+};
+
+namespace {
+
+// launch kern<ND> on the grid-stride grid; evaluates to 1 (one launch)
+#define ND_DISPATCH(nd, kern, ...)                                        \
+    ((nd) == 1   ? (kern<1><<<vb::GP, vb::GB, 0, s>>>(__VA_ARGS__), 1)   \
+     : (nd) == 2 ? (kern<2><<<vb::GP, vb::GB, 0, s>>>(__VA_ARGS__), 1)   \
+                 : (kern<3><<<vb::GP, vb::GB, 0, s>>>(__VA_ARGS__), 1))
+
+// One CG iteration (five launches; each returns at once after convergence).
+int queue_iteration(vb_grid *gr, vb_gravity *gv)
+{
+    cudaStream_t s = gr->ctx->stream;
+    const vb::Geom &g = gr->g;
+    VB_CHECK_LAUNCH(gr->ctx, ND_DISPATCH(g.nd, vb::k_cg_matvec, g, gv->P, gv->p, gv->Ap, gv->part, gv->gc));
+    vb::k_cg_alpha<<<1, 1024, 0, s>>>(gv->part, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 1);
+    vb::k_cg_update<<<vb::GP, vb::GB, 0, s>>>(g, gv->phi, gv->p, gv->r, gv->Ap, gv->part, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 1);
+    vb::k_cg_beta<<<1, 1024, 0, s>>>(gv->part, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 1);
+    vb::k_cg_dir<<<vb::GP, vb::GB, 0, s>>>(g, gv->p, gv->r, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 1);
+    return VB_OK;
+}
+
+int capture_iterations(vb_grid *gr, vb_gravity *gv)
+{
+    cudaStream_t s = gr->ctx->stream;
+    VB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = gr->ctx->launches;
+    int rc = VB_OK;
+    for (int k = 0; k < vb::GRAPH_ITERS && !rc; ++k) rc = queue_iteration(gr, gv);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &graph);
+    gr->ctx->launches = before;  // counted per replay
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(VB_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&gv->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        gv->gexec = nullptr;
+        return fail(VB_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    return VB_OK;
+}
+
+int refresh_accel(vb_grid *gr, vb_gravity *gv)
+{
+    cudaStream_t s = gr->ctx->stream;
+    const vb::Geom &g = gr->g;
+    VB_CHECK_LAUNCH(gr->ctx, ND_DISPATCH(g.nd, vb::k_accel, g, gv->P, gv->phi, gv->gacc));
+    return VB_OK;
+}
+
+void free_gravity(vb_gravity *gv)
+{
+    if (!gv) return;
+    if (gv->gexec) cudaGraphExecDestroy(gv->gexec);
+    cudaFree(gv->phi);
+    cudaFree(gv->b);
+    cudaFree(gv->r);
+    cudaFree(gv->p);
+    cudaFree(gv->Ap);
+    cudaFree(gv->gacc);
+    cudaFree(gv->part);
+    cudaFree(gv->gc);
+    cudaFreeHost(gv->hgc);
+    delete gv;
+}
+
+int check_grid(vb_grid *gr)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    if (!gr->grav) return fail(VB_EINVAL, "gravity is not enabled on this grid");
+    return use(gr->ctx);
+}
+
+}  // namespace
+
+// solve_poisson! (src/gravity.jl:251-300) for the grid's current density,
+// warm-started from the stored potential; then g = -grad phi for the stages.
+int vb::detail::gravity_solve(vb_grid *gr, int64_t *iters, double *relres)
+{
+    vb_gravity *gv = gr->grav;
+    cudaStream_t s = gr->ctx->stream;
+    const Geom &g = gr->g;
+    gv->hgc->maxiter = gv->maxiter;
+    gv->hgc->tol = gv->tol;
+    VB_CUDA(cudaMemcpyAsync(&gv->gc->maxiter, &gv->hgc->maxiter, sizeof(long long),
+                            cudaMemcpyHostToDevice, s));
+    VB_CUDA(cudaMemcpyAsync(&gv->gc->tol, &gv->hgc->tol, sizeof(double), cudaMemcpyHostToDevice, s));
+    if (gv->P.project_mean) {
+        k_meanpart<<<GP, GB, 0, s>>>(g, gr->U, gv->part);
+        VB_CHECK_LAUNCH(gr->ctx, 1);
+        k_mean_final<<<1, 1024, 0, s>>>(gv->part, gv->gc, 0);
+        VB_CHECK_LAUNCH(gr->ctx, 1);
+    }
+    k_rhs<<<GP, GB, 0, s>>>(g, gv->P, gr->U, gv->b, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 1);
+    VB_CHECK_LAUNCH(gr->ctx, ND_DISPATCH(g.nd, k_cg_init, g, gv->P, gv->phi, gv->b, gv->r, gv->p, gv->part));
+    k_cg_init_final<<<1, 1024, 0, s>>>(gv->part, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 1);
+    if (!gv->gexec) {
+        int rc = capture_iterations(gr, gv);
+        if (rc) return rc;
+    }
+    // the stop flag is set by convergence, p.Ap <= 0 or maxiter, so this ends
+    for (;;) {
+        VB_CUDA(cudaGraphLaunch(gv->gexec, s));
+        gr->ctx->launches += 5 * GRAPH_ITERS;
+        VB_CUDA(cudaMemcpyAsync(gv->hgc, gv->gc, sizeof(GravCtrl), cudaMemcpyDeviceToHost, s));
+        VB_CUDA(cudaStreamSynchronize(s));
+        if (gv->hgc->done) break;
+    }
+    if (gv->P.project_mean) {
+        k_meanpart<<<GP, GB, 0, s>>>(g, gv->phi, gv->part);
+        VB_CHECK_LAUNCH(gr->ctx, 1);
+        k_mean_final<<<1, 1024, 0, s>>>(gv->part, gv->gc, 1);
+        VB_CHECK_LAUNCH(gr->ctx, 1);
+        k_sub_mean<<<GP, GB, 0, s>>>(g, gv->phi, gv->gc);
+        VB_CHECK_LAUNCH(gr->ctx, 1);
+    }
+    int rc = refresh_accel(gr, gv);
+    if (rc) return rc;
+    if (iters) *iters = gv->hgc->iters;
+    if (relres) *relres = gv->hgc->relres;
+    return VB_OK;
+}
+
+void vb::detail::gravity_free(vb_gravity *gv) { free_gravity(gv); }
+
+extern "C" {
+
+int vb_gravity_enable(vb_grid *gr, const vb_gravity_desc *d)
+{
+    if (!gr || !d) return fail(VB_EINVAL, "null argument");
+    if (d->flags != 0) return fail(VB_EINVAL, "flags must be 0");
+    if (!(d->tol >= 0.0) || d->maxiter < 0) return fail(VB_EINVAL, "tol and maxiter must be non-negative");
+    if (!std::isfinite(d->G)) return fail(VB_EINVAL, "G must be finite");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    const vb::Geom &g = gr->g;
+    vb::GravP P{};
+    for (int a = 0; a < 3; ++a) {
+        if (a < g.nd) {
+            for (int side = 0; side < 2; ++side) {
+                const int bc = side ? d->bc_hi[a] : d->bc_lo[a];
+                if (bc < VB_BC_OUTFLOW || bc > VB_BC_REFLECTING)
+                    return fail(VB_EINVAL, "unknown boundary condition");
+            }
+            if ((d->bc_lo[a] == VB_BC_PERIODIC) != (d->bc_hi[a] == VB_BC_PERIODIC))
+                return fail(VB_EINVAL, "a periodic axis must be periodic on both sides");
+            P.per_lo[a] = d->bc_lo[a] == VB_BC_PERIODIC;
+            P.per_hi[a] = d->bc_hi[a] == VB_BC_PERIODIC;
+            P.coef[a] = g.area[a] / (0.5 * (g.w[a] + g.w[a]));  // area / _face_distance
+        } else {
+            P.per_lo[a] = P.per_hi[a] = 1;
+            P.coef[a] = 0.0;
+        }
+    }
+    P.G = d->G;
+    P.project_mean = d->project_mean ? 1 : 0;
+    vb_gravity *gv = gr->grav;
+    if (!gv) {
+        gv = new vb_gravity;
+        const size_t n = (size_t)g.ncell * sizeof(double);
+        cudaError_t e = cudaSuccess;
+        for (double **buf : {&gv->phi, &gv->b, &gv->r, &gv->p, &gv->Ap})
+            if (e == cudaSuccess) e = cudaMalloc(buf, n);
+        if (e == cudaSuccess) e = cudaMalloc(&gv->gacc, n * g.nd);
+        if (e == cudaSuccess) e = cudaMalloc(&gv->part, sizeof(double) * 2 * vb::GP);
+        if (e == cudaSuccess) e = cudaMalloc(&gv->gc, sizeof(vb::GravCtrl));
+        if (e == cudaSuccess) e = cudaMallocHost(&gv->hgc, sizeof(vb::GravCtrl));
+        if (e == cudaSuccess) e = cudaMemsetAsync(gv->phi, 0, n, gr->ctx->stream);  // phi starts at 0
+        if (e == cudaSuccess) e = cudaMemsetAsync(gv->gacc, 0, n * g.nd, gr->ctx->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(gv->gc, 0, sizeof(vb::GravCtrl), gr->ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(gr->ctx->stream);
+        if (e != cudaSuccess) {
+            free_gravity(gv);
+            return fail(e == cudaErrorMemoryAllocation ? VB_ENOMEM : VB_ECUDA,
+                        std::string("gravity allocation: ") + cudaGetErrorString(e));
+        }
+        std::memset(gv->hgc, 0, sizeof(vb::GravCtrl));
+    }
+    gv->P = P;
+    gv->maxiter = d->maxiter;
+    gv->tol = d->tol;
+    gr->grav = gv;
+    gr->g.grav_g = gv->gacc;
+    gr->g.grav_G = d->G;
+    gr->invdt_valid = false;  // the free-fall limiter joins the CFL maximum
+    return VB_OK;
+}
+
+int vb_gravity_disable(vb_grid *gr)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    if (!gr->grav) return VB_OK;
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    cudaStreamSynchronize(gr->ctx->stream);
+    free_gravity(gr->grav);
+    gr->grav = nullptr;
+    gr->g.grav_g = nullptr;
+    gr->g.grav_G = 0.0;
+    gr->invdt_valid = false;
+    return VB_OK;
+}
+
+int vb_gravity_solve(vb_grid *gr, int64_t *iters, double *relres)
+{
+    int rc = check_grid(gr);
+    if (rc) return rc;
+    return vb::detail::gravity_solve(gr, iters, relres);
+}
+
+int vb_gravity_phi(vb_grid *gr, double *phi)
+{
+    int rc = check_grid(gr);
+    if (rc) return rc;
+    if (!phi) return fail(VB_EINVAL, "null output");
+    VB_CUDA(cudaMemcpyAsync(phi, gr->grav->phi, sizeof(double) * gr->g.ncell, cudaMemcpyDeviceToHost,
+                            gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    return VB_OK;
+}
+
+int vb_gravity_set_phi(vb_grid *gr, const double *phi)
+{
+    int rc = check_grid(gr);
+    if (rc) return rc;
+    if (!phi) return fail(VB_EINVAL, "null input");
+    VB_CUDA(cudaMemcpyAsync(gr->grav->phi, phi, sizeof(double) * gr->g.ncell, cudaMemcpyHostToDevice,
+                            gr->ctx->stream));
+    rc = refresh_accel(gr, gr->grav);
+    if (rc) return rc;
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    return VB_OK;
+}
+
+int vb_gravity_accel(vb_grid *gr, double *gout)
+{
+    int rc = check_grid(gr);
+    if (rc) return rc;
+    if (!gout) return fail(VB_EINVAL, "null output");
+    VB_CUDA(cudaMemcpyAsync(gout, gr->grav->gacc, sizeof(double) * gr->g.ncell * gr->g.nd,
+                            cudaMemcpyDeviceToHost, gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+    return VB_OK;
+}
+
+int vb_gravity_laplacian(vb_grid *gr, const double *x, double *Ax)
+{
+    int rc = check_grid(gr);
+    if (rc) return rc;
+    if (!x || !Ax) return fail(VB_EINVAL, "null argument");
+    vb_gravity *gv = gr->grav;
+    cudaStream_t s = gr->ctx->stream;
+    const size_t n = sizeof(double) * gr->g.ncell;
+    // the CG scratch r (input) and Ap (output) are free between solves
+    VB_CUDA(cudaMemcpyAsync(gv->r, x, n, cudaMemcpyHostToDevice, s));
+    VB_CHECK_LAUNCH(gr->ctx, ND_DISPATCH(gr->g.nd, vb::k_lap, gr->g, gv->P, gv->r, gv->Ap));
+    VB_CUDA(cudaMemcpyAsync(Ax, gv->Ap, n, cudaMemcpyDeviceToHost, s));
+    VB_CUDA(cudaStreamSynchronize(s));
+    return VB_OK;
+}
+
+}  // extern "C"

@@ -16,6 +16,8 @@ struct vb_ctx {
     cudaEvent_t marks[16] = {};
 };
 
+struct vb_gravity;  // self-gravity state of a grid (vb_gravity.cu)
+
 struct vb_grid {
     vb_ctx *ctx = nullptr;
     vb::Geom g{};
@@ -41,6 +43,7 @@ struct vb_grid {
     uint64_t gkey = 0;                  // kernel configuration it was captured for
     int64_t glaunches = 0;              // kernels per replay
     bool warmed = false;                // one direct step ran (launch setup done)
+    vb_gravity *grav = nullptr;         // self-gravity (stages take the cell-centric kernel)
 };
 
 namespace vb {
@@ -69,6 +72,11 @@ int grid_ensure_cfl(vb_grid *gr);   // CFL max of the current state, if stale
 int grid_rk2(vb_grid *gr);          // one RK2 step with dt already in the control block
 int grid_pull_ctrl(vb_grid *gr);    // device control block -> gr->hctrl (synchronous)
 int grid_push_ctrl(vb_grid *gr);    // gr->hctrl -> device control block (synchronous)
+
+// Self-gravity (vb_gravity.cu): solve_poisson! for the current density and
+// refresh the field g the stages add; free a grid's gravity state.
+int gravity_solve(vb_grid *gr, int64_t *iters, double *relres);
+void gravity_free(vb_gravity *gv);
 
 }  // namespace detail
 }  // namespace vb

@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(256) k_cfl(Geom g, const double *__restrict__ 
         cons2prim(u, g.gamma, W);
         const double c = sound_speed(W, g.gamma);
         for (int d = 0; d < g.nd; ++d) m = nan_max(m, (fabs(W[1 + d]) + c) / g.w[d]);
+        if (g.grav_g) m = nan_max(m, gravity_invdt(g.grav_G, W[0]));
     }
     block_max_to(&ctrl->invdt_bits, m, red);
 }

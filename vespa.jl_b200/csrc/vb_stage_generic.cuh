@@ -177,6 +177,12 @@ k_stage_generic(Geom g, const double *__restrict__ Uin, const double *U0, double
                 if (af[d].cat == LO_AFTER) a += (-g.area[d]) * double(af[d].lo[k]);
             acc[k] = a;
         }
+        if (g.grav_g) {  // gravity source from the stage state, after the fluxes
+            double u[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) u[k] = Uin[k * g.ncell + lin];
+            gravity_source<ND>(g, lin, u, acc);
+        }
 
         const double invV = ctrl->invV;
         double un[5];
@@ -218,6 +224,7 @@ k_stage_generic(Geom g, const double *__restrict__ Uin, const double *U0, double
             const double cs = sound_speed(W, g.gamma);
 #pragma unroll
             for (int d = 0; d < ND; ++d) invdt = nan_max(invdt, (fabs(W[1 + d]) + cs) / g.w[d]);
+            if (g.grav_g) invdt = nan_max(invdt, gravity_invdt(g.grav_G, W[0]));
         }
     }
     if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);

@@ -3,13 +3,14 @@
 The compute path is the CUDA library (sm_100a) behind the C ABI in
 include/vespa_b200.h; this package only marshals arguments and mirrors the
 reference's public names (Simulation, step!, evolve!, compute_dt,
-conserved_totals, compute_face_fluxes!).
+conserved_totals, compute_face_fluxes!, enable_gravity!, solve_poisson!).
 """
 from ._lib import Context, VespaB200Error, default_context, load
 from . import amr
 from .amr import AmrMesh, AmrSimulation, RefinementPolicy
 from .adjoint import Adjoint, EvolveFunction, evolve_with_adjoint, rho2_integral, rho2_seed
 from .flux import AbstractFluxBackend, B200Flux, compute_face_fluxes
+from .gravity import GravityField, apply_laplacian, disable_gravity, enable_gravity, solve_poisson
 from .problem import (BC, IdealHydro, Outflow, Periodic, Problem, Reflecting, cons2prim,
                       initial_primitive, initial_state, kelvin_helmholtz_problem, prim2cons,
                       riemann_box_problem, sedov_problem, smooth_random_problem,
@@ -23,6 +24,7 @@ __all__ = [
     "amr", "AmrMesh", "AmrSimulation", "RefinementPolicy",
     "Adjoint", "EvolveFunction", "evolve_with_adjoint", "rho2_integral", "rho2_seed",
     "AbstractFluxBackend", "B200Flux", "compute_face_fluxes",
+    "GravityField", "apply_laplacian", "disable_gravity", "enable_gravity", "solve_poisson",
     "BC", "IdealHydro", "Outflow", "Periodic", "Problem", "Reflecting", "cons2prim",
     "initial_primitive", "initial_state", "kelvin_helmholtz_problem", "prim2cons",
     "riemann_box_problem", "sedov_problem", "smooth_random_problem", "sod_problem_defaults",

@@ -44,6 +44,19 @@ class ProblemDesc(C.Structure):
     ]
 
 
+class GravityDesc(C.Structure):
+    """vb_gravity_desc"""
+    _fields_ = [
+        ("G", C.c_double),
+        ("tol", C.c_double),
+        ("maxiter", C.c_int64),
+        ("bc_lo", C.c_int32 * 3),
+        ("bc_hi", C.c_int32 * 3),
+        ("project_mean", C.c_int32),
+        ("flags", C.c_int32),
+    ]
+
+
 # name -> (argtypes); every entry point returns int
 _VP = C.c_void_p
 _DP = C.POINTER(C.c_double)
@@ -92,6 +105,13 @@ SIGNATURES = {
     "vb_bflux_size": [_VP, _I64P],
     "vb_bflux_read": [_VP, _DP, C.c_int64],
     "vb_bflux_clear": [_VP],
+    "vb_gravity_enable": [_VP, C.POINTER(GravityDesc)],
+    "vb_gravity_disable": [_VP],
+    "vb_gravity_solve": [_VP, _I64P, _DP],
+    "vb_gravity_phi": [_VP, _DP],
+    "vb_gravity_set_phi": [_VP, _DP],
+    "vb_gravity_accel": [_VP, _DP],
+    "vb_gravity_laplacian": [_VP, _DP, _DP],
     "vb_adjoint_create": [_VP, C.c_int64, C.c_int64, C.POINTER(_VP)],
     "vb_adjoint_destroy": [_VP],
     "vb_adjoint_forward": [_VP, C.c_double, C.c_int64, _DP, _I64P],

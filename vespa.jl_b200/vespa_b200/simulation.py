@@ -168,6 +168,7 @@ class Simulation:
                   C.byref(h))
         self.handle = h
         self._dependents = weakref.WeakSet()  # adjoints bound to this grid
+        self.grav = None  # GravityField while self-gravity is enabled (gravity.py)
         self.ncell = backend.n_cells()
         U = initial if initial is not None else initial_state(problem)
         self.upload(U)
