@@ -51,11 +51,13 @@ def parse():
                     help="skip the Sedov 48^2 AMR run")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the KH 512^2 adjoint timing and finite-difference check")
-    ap.add_argument("--workload", choices=["cube", "batch64", "plane", "adjoint", "amr"],
+    ap.add_argument("--no-gravity", action="store_true",
+                    help="skip the 256^3 self-gravity run")
+    ap.add_argument("--workload", choices=["cube", "batch64", "plane", "adjoint", "amr", "gravity"],
                     default="cube",
-                    help="cube: the 256^3 headline line (with the plane, adjoint and AMR "
-                         "sections); batch64: 64 uneven Riemann boxes in one batch; plane, "
-                         "adjoint, amr: that section alone")
+                    help="cube: the 256^3 headline line (with the plane, adjoint, AMR and "
+                         "gravity sections); batch64: 64 uneven Riemann boxes in one batch; plane, "
+                         "adjoint, amr, gravity: that section alone")
     return ap.parse_args()
 
 
@@ -376,6 +378,7 @@ def run_ours(args, ranks: Ranks):
     adjoint = None if args.no_adjoint else adjoint_section(ctx, ranks)
     amr = None if args.no_amr else amr_section(ctx, ranks)
     plane = None if args.no_plane else plane_section(ctx, ranks, K, W)
+    gravity = None if args.no_gravity else gravity_section(ctx, ranks, min(K, 20), W)
 
     cpu = None
     if ranks.world == 1 and ranks.rank == 0 and not args.no_cpu_baseline:
@@ -418,6 +421,8 @@ def run_ours(args, ranks: Ranks):
         line["amr"] = amr
     if plane:
         line["plane2d"] = plane
+    if gravity is not None:
+        line["gravity"] = gravity
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -525,6 +530,75 @@ def plane_section(ctx, ranks: Ranks, K: int, W: int, n=4096):
                      "ms_per_step": round(ms / K, 4), "kernel": sim.kernel, "row_chunk": ky,
                      "stage2_hbm_frac": round(s2 / hbm, 4)}
         sim.close()
+    return out
+
+
+def gravity_section(ctx, ranks: Ranks, K: int, W: int, n=256, cpu_n=64):
+    """Self-gravity (src/gravity.jl) on the 256^3 cube: (a) a cold Poisson solve
+    (phi = 0, tol 1e-8) for a white-noise density, whose conjugate-gradient
+    iterations stream 88 B/cell (matvec r p w Ap, update r phi p r Ap w phi r,
+    direction r p w p); (b) K evolve! steps with gravity after W warm-up steps
+    (one warm-started solve per step, stages on the cell-centric kernel), both
+    precisions.  CPU: the oracle's CG on a cpu_n^3 sample of (a), serial."""
+    import numpy as np
+    import vespa_b200 as vb
+    prob = vb.smooth_random_problem((n, n, n), seed=vb.problem.DEFAULT_SEED + ranks.rank)
+    U0 = vb.initial_state(prob)
+    mesh = vb.B200Mesh(prob.dims, prob.domain)
+    rng = np.random.default_rng(20261203 + ranks.rank)
+    Un = U0.copy()
+    Un[0] = 0.5 + rng.random(n ** 3)
+    out = {"config": f"3D {n}^3 periodic, G = 1, phi periodic with the mean projected out; "
+                     "(a) cold solve of a white-noise density U[0.5, 1.5), tol 1e-8; "
+                     "(b) the cube's smooth random state, CFL 0.4, solve per step"}
+    sim = vb.Simulation(mesh, prob, precision="fp64", ctx=ctx, initial=Un)
+    grav = vb.enable_gravity(sim, G=1.0, tol=1e-8, maxiter=5000)
+    vb.solve_poisson(sim, grav)  # warm-up (captures the iteration graph)
+    grav.phi = np.zeros(n ** 3)
+    ctx.synchronize()
+    ranks.barrier()
+    ctx.mark(10)
+    its, rr = vb.solve_poisson(sim, grav)
+    ctx.mark(11)
+    ms = ranks.max(ctx.elapsed_ms(10, 11))
+    hbm, _ = measured_hbm()
+    per_it = ms / its
+    bw = 88 * n ** 3 / (per_it / 1e3) / 1e9
+    out["cold_solve"] = {"iters": its, "relres": rr, "ms": round(ms, 3),
+                         "ms_per_iteration": round(per_it, 4),
+                         "Mcell_iterations_per_s": round(n ** 3 / (per_it / 1e3) / 1e6, 1),
+                         "achieved_gbs": round(bw, 1), "hbm_frac": round(bw / hbm, 4),
+                         "bytes_per_cell_iteration": 88}
+    sim.close()
+    for prec in ("fp64", "mixed"):
+        sim = vb.Simulation(mesh, prob, precision=prec, ctx=ctx, initial=U0)
+        vb.enable_gravity(sim, G=1.0)
+        vb.evolve(sim, tfinal=math.inf, max_steps=W)
+        ctx.synchronize()
+        ranks.barrier()
+        ctx.mark(12)
+        vb.evolve(sim, tfinal=math.inf, max_steps=K)
+        ctx.mark(13)
+        ms = ranks.max(ctx.elapsed_ms(12, 13))
+        out[prec] = {"value": round(n ** 3 * ranks.world * K / (ms / 1e3) / 1e6, 1), "unit": UNIT,
+                     "ms_per_step": round(ms / K, 4), "kernel": sim.kernel}
+        sim.close()
+    if ranks.rank == 0:
+        from oracle import oracle as O
+        O.build()
+        cprob = vb.smooth_random_problem((cpu_n,) * 3)
+        Uc = vb.initial_state(cprob)
+        Uc[0] = 0.5 + rng.random(cpu_n ** 3)
+        g = O.grid_from_problem(cprob)
+        Pg = O.make_gravity(1.0, (1, 1, 1), (1, 1, 1), 5000, 1e-8, True)
+        phi = np.zeros(cpu_n ** 3)
+        t0 = time.perf_counter()
+        cits, _ = O.grav_solve(g, Pg, Uc, phi)
+        cs = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(cpu_n ** 3 * cits / cs / 1e6, 2),
+                               "unit": "Mcell-CG-iterations/s", "cores": 1, "kind": "port",
+                               "sample": f"cold solve of a {cpu_n}^3 white-noise density, tol 1e-8 "
+                                         f"({cits} iterations, {cs:.2f} s), serial C oracle"}
     return out
 
 
@@ -642,6 +716,9 @@ def run_section(args, ranks: Ranks):
         sec = adjoint_section(ctx, ranks)
         metric, value = ("adjoint step / forward step, KH 512^2 float64",
                          sec["textured"]["adj_step_over_fwd_step"])
+    elif args.workload == "gravity":
+        sec = gravity_section(ctx, ranks, min(args.steps, 20), args.warmup)
+        metric, value = ("Mcell-updates/s 3D 256^3 with self-gravity (fp64)", sec["fp64"]["value"])
     else:
         sec = amr_section(ctx, ranks)
         metric, value = ("Mleaf-updates/s, Sedov 48^2 AMR single rate",
@@ -659,7 +736,7 @@ def main():
             run_reference(args, ranks)
         elif args.workload == "batch64":
             run_batch64(args, ranks)
-        elif args.workload in ("plane", "adjoint", "amr"):
+        elif args.workload in ("plane", "adjoint", "amr", "gravity"):
             run_section(args, ranks)
         else:
             run_ours(args, ranks)

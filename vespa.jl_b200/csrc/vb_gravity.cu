@@ -12,8 +12,9 @@
 // the reference's serial sums, so a solve matches the reference's to the
 // solver tolerance, not bit for bit.
 //
-// Every pass is a grid-stride loop over cells in x-fastest order: an HBM
-// stream of the CG vectors (the stencil's neighbours come from L1/L2).  One
+// Every pass streams the CG vectors from HBM over a fixed grid of GP blocks
+// (the stencil's neighbours come from L1/L2); the stencil passes walk rows of
+// x so that a cell's coordinates cost no division.  One
 // CG iteration is five launches (matvec + p.Ap partials, alpha, vector update
 // + r.r partials, beta, direction update); groups of iterations replay as one
 // CUDA graph, each launch returning at once after convergence, and the host
@@ -57,11 +58,28 @@ __device__ __forceinline__ int64_t gnb(const Geom &g, const GravP &P, int64_t li
     return -1;
 }
 
-__device__ __forceinline__ void coords(const Geom &g, int64_t lin, int64_t cc[3])
+// Visit this block's cells: rows of x (coordinates derived once per row), rows
+// strided over the GP blocks and x over the block's threads; 1D grids stride
+// cells directly.  A fixed order per thread, so the partial sums are
+// deterministic.
+template <int ND, typename F>
+__device__ __forceinline__ void for_cells(const Geom &g, F &&f)
 {
-    cc[0] = lin % g.n[0];
-    cc[1] = (lin / g.n[0]) % g.n[1];
-    cc[2] = lin / (g.n[0] * g.n[1]);
+    if constexpr (ND == 1) {
+        for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
+            const int64_t cc[3] = {i, 0, 0};
+            f(i, cc);
+        }
+    } else {
+        const int64_t n0 = g.n[0], nrow = g.ncell / n0;
+        for (int64_t row = blockIdx.x; row < nrow; row += GP) {
+            const int64_t cy = row % g.n[1], cz = row / g.n[1];
+            for (int64_t cx = threadIdx.x; cx < n0; cx += GB) {
+                const int64_t cc[3] = {cx, cy, cz};
+                f(row * n0 + cx, cc);
+            }
+        }
+    }
 }
 
 // (A x)[lin], A = -nabla^2 V: sum over the row's faces of coef * (x_c - x_nb),
@@ -71,10 +89,8 @@ __device__ __forceinline__ void coords(const Geom &g, int64_t lin, int64_t cc[3]
 // (x, y, z).
 template <int ND>
 __device__ __forceinline__ double lap_row(const Geom &g, const GravP &P, const double *__restrict__ x,
-                                          int64_t lin)
+                                          int64_t lin, const int64_t cc[3])
 {
-    int64_t cc[3];
-    coords(g, lin, cc);
     const double xc = x[lin];
     double s = 0.0;
 #pragma unroll
@@ -173,13 +189,13 @@ __global__ void __launch_bounds__(GB) k_cg_init(Geom g, GravP P, const double *_
 {
     __shared__ double sh[GB];
     double rr = 0.0, bb = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
-        const double ri = b[i] - lap_row<ND>(g, P, phi, i);
+    for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
+        const double ri = b[i] - lap_row<ND>(g, P, phi, i, cc);
         r[i] = ri;
         p[i] = ri;
         rr = rr + ri * ri;
         bb = bb + b[i] * b[i];
-    }
+    });
     rr = block_sum(rr, sh);
     bb = block_sum(bb, sh);
     if (threadIdx.x == 0) {
@@ -212,11 +228,11 @@ __global__ void __launch_bounds__(GB) k_cg_matvec(Geom g, GravP P, const double 
     __shared__ double sh[GB];
     if (gc->done) return;
     double s = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
-        const double a = lap_row<ND>(g, P, p, i);
+    for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
+        const double a = lap_row<ND>(g, P, p, i, cc);
         Ap[i] = a;
         s = s + p[i] * a;
-    }
+    });
     s = block_sum(s, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
@@ -296,9 +312,7 @@ template <int ND>
 __global__ void __launch_bounds__(GB) k_accel(Geom g, GravP P, const double *__restrict__ phi,
                                              double *gacc)
 {
-    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
-        int64_t cc[3];
-        coords(g, i, cc);
+    for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
         const double pc = phi[i];
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
@@ -308,14 +322,13 @@ __global__ void __launch_bounds__(GB) k_accel(Geom g, GravP P, const double *__r
             const double dlo = lo < 0 ? 0.5 * g.w[d] : fd, dhi = hi < 0 ? 0.5 * g.w[d] : fd;
             gacc[d * g.ncell + i] = -(whi - wlo) / (dlo + dhi);
         }
-    }
+    });
 }
 
 template <int ND>
 __global__ void __launch_bounds__(GB) k_lap(Geom g, GravP P, const double *__restrict__ x, double *out)
 {
-    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB)
-        out[i] = lap_row<ND>(g, P, x, i);
+    for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) { out[i] = lap_row<ND>(g, P, x, i, cc); });
 }
 
 }  // namespace
