@@ -535,11 +535,13 @@ def plane_section(ctx, ranks: Ranks, K: int, W: int, n=4096):
 
 def gravity_section(ctx, ranks: Ranks, K: int, W: int, n=256, cpu_n=64):
     """Self-gravity (src/gravity.jl) on the 256^3 cube: (a) a cold Poisson solve
-    (phi = 0, tol 1e-8) for a white-noise density, whose conjugate-gradient
-    iterations stream 88 B/cell (matvec r p w Ap, update r phi p r Ap w phi r,
-    direction r p w p); (b) K evolve! steps with gravity after W warm-up steps
-    (one warm-started solve per step, stages on the cell-centric kernel), both
-    precisions.  CPU: the oracle's CG on a cpu_n^3 sample of (a), serial."""
+    (phi = 0, tol 1e-8) of a white-noise density with plain CG (the reference's
+    default), whose iterations stream 88 B/cell (matvec r p w Ap, update r phi
+    p r Ap w phi r, direction r p w p), and with the multigrid preconditioner
+    (precond = :mg, ext/mg_pcg.jl); (b) K evolve! steps with gravity after W
+    warm-up steps (one warm-started solve per step, stages on the cell-centric
+    kernel): both precisions with the preconditioner, float64 with plain CG.
+    CPU: the oracle's plain CG on a cpu_n^3 sample of (a), serial."""
     import numpy as np
     import vespa_b200 as vb
     prob = vb.smooth_random_problem((n, n, n), seed=vb.problem.DEFAULT_SEED + ranks.rank)
@@ -550,29 +552,31 @@ def gravity_section(ctx, ranks: Ranks, K: int, W: int, n=256, cpu_n=64):
     Un[0] = 0.5 + rng.random(n ** 3)
     out = {"config": f"3D {n}^3 periodic, G = 1, phi periodic with the mean projected out; "
                      "(a) cold solve of a white-noise density U[0.5, 1.5), tol 1e-8; "
-                     "(b) the cube's smooth random state, CFL 0.4, solve per step"}
-    sim = vb.Simulation(mesh, prob, precision="fp64", ctx=ctx, initial=Un)
-    grav = vb.enable_gravity(sim, G=1.0, tol=1e-8, maxiter=5000)
-    vb.solve_poisson(sim, grav)  # warm-up (captures the iteration graph)
-    grav.phi = np.zeros(n ** 3)
-    ctx.synchronize()
-    ranks.barrier()
-    ctx.mark(10)
-    its, rr = vb.solve_poisson(sim, grav)
-    ctx.mark(11)
-    ms = ranks.max(ctx.elapsed_ms(10, 11))
+                     "(b) the cube's smooth random state, CFL 0.4, solve per step (tol 1e-8)"}
     hbm, _ = measured_hbm()
-    per_it = ms / its
-    bw = 88 * n ** 3 / (per_it / 1e3) / 1e9
-    out["cold_solve"] = {"iters": its, "relres": rr, "ms": round(ms, 3),
-                         "ms_per_iteration": round(per_it, 4),
-                         "Mcell_iterations_per_s": round(n ** 3 / (per_it / 1e3) / 1e6, 1),
-                         "achieved_gbs": round(bw, 1), "hbm_frac": round(bw / hbm, 4),
-                         "bytes_per_cell_iteration": 88}
-    sim.close()
-    for prec in ("fp64", "mixed"):
+    for pc in ("none", "mg"):
+        sim = vb.Simulation(mesh, prob, precision="fp64", ctx=ctx, initial=Un)
+        grav = vb.enable_gravity(sim, G=1.0, tol=1e-8, maxiter=5000, precond=pc)
+        vb.solve_poisson(sim, grav)  # warm-up (captures the iteration graph)
+        grav.phi = np.zeros(n ** 3)
+        ctx.synchronize()
+        ranks.barrier()
+        ctx.mark(10)
+        its, rr = vb.solve_poisson(sim, grav)
+        ctx.mark(11)
+        ms = ranks.max(ctx.elapsed_ms(10, 11))
+        per_it = ms / its
+        rec = {"iters": its, "relres": rr, "ms": round(ms, 3), "ms_per_iteration": round(per_it, 4)}
+        if pc == "none":
+            bw = 88 * n ** 3 / (per_it / 1e3) / 1e9
+            rec.update({"Mcell_iterations_per_s": round(n ** 3 / (per_it / 1e3) / 1e6, 1),
+                        "achieved_gbs": round(bw, 1), "hbm_frac": round(bw / hbm, 4),
+                        "bytes_per_cell_iteration": 88})
+        out[f"cold_solve_{pc}"] = rec
+        sim.close()
+    for prec, pc in (("fp64", "mg"), ("mixed", "mg"), ("fp64", "none")):
         sim = vb.Simulation(mesh, prob, precision=prec, ctx=ctx, initial=U0)
-        vb.enable_gravity(sim, G=1.0)
+        vb.enable_gravity(sim, G=1.0, precond=pc)
         vb.evolve(sim, tfinal=math.inf, max_steps=W)
         ctx.synchronize()
         ranks.barrier()
@@ -580,8 +584,9 @@ def gravity_section(ctx, ranks: Ranks, K: int, W: int, n=256, cpu_n=64):
         vb.evolve(sim, tfinal=math.inf, max_steps=K)
         ctx.mark(13)
         ms = ranks.max(ctx.elapsed_ms(12, 13))
-        out[prec] = {"value": round(n ** 3 * ranks.world * K / (ms / 1e3) / 1e6, 1), "unit": UNIT,
-                     "ms_per_step": round(ms / K, 4), "kernel": sim.kernel}
+        out[f"{prec}_{pc}"] = {"value": round(n ** 3 * ranks.world * K / (ms / 1e3) / 1e6, 1),
+                               "unit": UNIT, "ms_per_step": round(ms / K, 4), "steps": K,
+                               "stages": "cell-centric kernel with the gravity source"}
         sim.close()
     if ranks.rank == 0:
         from oracle import oracle as O
@@ -597,8 +602,8 @@ def gravity_section(ctx, ranks: Ranks, K: int, W: int, n=256, cpu_n=64):
         cs = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": round(cpu_n ** 3 * cits / cs / 1e6, 2),
                                "unit": "Mcell-CG-iterations/s", "cores": 1, "kind": "port",
-                               "sample": f"cold solve of a {cpu_n}^3 white-noise density, tol 1e-8 "
-                                         f"({cits} iterations, {cs:.2f} s), serial C oracle"}
+                               "sample": f"cold plain-CG solve of a {cpu_n}^3 white-noise density, "
+                                         f"tol 1e-8 ({cits} iterations, {cs:.2f} s), serial C oracle"}
     return out
 
 
@@ -718,7 +723,8 @@ def run_section(args, ranks: Ranks):
                          sec["textured"]["adj_step_over_fwd_step"])
     elif args.workload == "gravity":
         sec = gravity_section(ctx, ranks, min(args.steps, 20), args.warmup)
-        metric, value = ("Mcell-updates/s 3D 256^3 with self-gravity (fp64)", sec["fp64"]["value"])
+        metric, value = ("Mcell-updates/s 3D 256^3 with self-gravity (fp64, multigrid-preconditioned CG)",
+                         sec["fp64_mg"]["value"])
     else:
         sec = amr_section(ctx, ranks)
         metric, value = ("Mleaf-updates/s, Sedov 48^2 AMR single rate",

@@ -218,6 +218,13 @@ int vb_bflux_clear(vb_grid *grid);
  * the host for it; vb_step uses the field of the last solve (or set_phi), as
  * step! does; the stages take the cell-centric kernel.  The adjoint refuses
  * a grid with gravity (VB_ENOTSUP). */
+enum {
+    VB_GRAV_PRECOND_NONE = 0, /* plain CG (the reference's default) */
+    VB_GRAV_PRECOND_MG = 1    /* CG preconditioned by one base-grid multigrid cycle
+                                 (precond = :mg, ext/mg_pcg.jl); 3D cubic grids with
+                                 periodic phi only, VB_ENOTSUP otherwise */
+};
+
 typedef struct {
     double G;          /* gravitational constant, code units */
     double tol;        /* relative residual target */
@@ -225,6 +232,7 @@ typedef struct {
     int32_t bc_lo[3];  /* phi's boundary codes per axis */
     int32_t bc_hi[3];
     int32_t project_mean;
+    int32_t precond;   /* VB_GRAV_PRECOND_* */
     int32_t flags;     /* must be 0 */
 } vb_gravity_desc;
 

@@ -314,3 +314,46 @@ def test_gravity_api_errors(vb):
     grav = vb.enable_gravity(sim)
     with pytest.raises(ValueError):
         grav.phi = np.zeros(3)
+
+
+# ------------------------------------------------ multigrid-preconditioned CG
+@pytest.mark.parametrize("n", [32, 24])
+def test_mg_pcg_matches_oracle_cg_in_few_iterations(vb, oracle, n):
+    """precond="mg" (ext/mg_pcg.jl) converges to the plain-CG potential of the
+    oracle in a handful of iterations; n = 24 coarsens 24, 12, 6, 3."""
+    prob, U0 = random_density_problem((n, n, n), seed=12)
+    sim = make_sim(prob, U0)
+    grav = vb.enable_gravity(sim, tol=1e-10, maxiter=3000, precond="mg")
+    its, rr = vb.solve_poisson(sim, grav)
+    g, Pg = oracle_pair(oracle, prob, ((PER, PER),) * 3, tol=1e-10, maxiter=3000)
+    phi = np.zeros(sim.ncell)
+    its_o, _ = oracle.grav_solve(g, Pg, U0, phi)
+    assert rr <= 1e-10
+    assert its <= 25 and its * 4 < its_o, (its, its_o)
+    assert np.max(np.abs(grav.phi - phi)) <= 1e-8 * np.max(np.abs(phi))
+
+
+def test_mg_evolve_tracks_plain_cg(vb):
+    prob, U0 = random_density_problem((32, 32, 32), seed=13)
+    a = make_sim(prob, U0)
+    b = make_sim(prob, U0)
+    vb.enable_gravity(a, tol=1e-10, maxiter=3000)
+    vb.enable_gravity(b, tol=1e-10, maxiter=3000, precond="mg")
+    vb.evolve(a, tfinal=math.inf, max_steps=5)
+    vb.evolve(b, tfinal=math.inf, max_steps=5)
+    assert a.t == pytest.approx(b.t, rel=1e-12)
+    rel = np.max(np.abs(a.state() - b.state())) / np.max(np.abs(a.state()))
+    assert rel < 1e-9, rel
+
+
+def test_mg_refuses_unsupported_grids(vb):
+    prob, U0 = random_density_problem((32, 32, 16), seed=1)
+    sim = make_sim(prob, U0)
+    with pytest.raises(vb.VespaB200Error) as e:
+        vb.enable_gravity(sim, precond="mg")
+    assert e.value.status == 6
+    prob, U0 = random_density_problem((16, 16, 16), seed=1)
+    sim = make_sim(prob, U0)
+    with pytest.raises(vb.VespaB200Error) as e:
+        vb.enable_gravity(sim, precond="mg", bcs=P.Outflow)
+    assert e.value.status == 6

@@ -21,6 +21,7 @@
 // reads the stop flag between groups.
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "vb_internal.h"
 
@@ -32,7 +33,7 @@ constexpr int GP = 592;  // blocks (= partial sums) per reduction pass: 4 per SM
 constexpr int GRAPH_ITERS = 8;
 
 struct GravCtrl {
-    double rhobar, rsold, pAp, alpha, beta, bnorm, relres, mu;
+    double rhobar, rsold, pAp, alpha, beta, bnorm, relres, mu, mgmu;
     long long iters, maxiter;
     int done, pad;
     double tol;
@@ -331,6 +332,253 @@ __global__ void __launch_bounds__(GB) k_lap(Geom g, GravP P, const double *__res
     for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) { out[i] = lap_row<ND>(g, P, x, i, cc); });
 }
 
+// ---------------------------------------------------------------------------
+// Multigrid-preconditioned CG (precond = VB_GRAV_PRECOND_MG), after the
+// reference's ext/mg_pcg.jl: the outer CG runs on the exact operator A; the
+// preconditioner z = M^-1 r is one composite-smoothed two-level cycle
+// (_amg_cycle!, mg_pcg.jl:152-174): two damped-Jacobi sweeps on A from z = 0,
+// the residual moved to the base grid (on a uniform mesh the cells
+// themselves), one periodic cell-centred V-cycle of -lap there (_mg_vcycle!,
+// 123-145: damped Jacobi 2 + 2, full-weighting restriction, trilinear
+// prolongation, 30 sweeps on the coarsest level), the correction de-meaned,
+// scaled by 1/V and added, two more Jacobi sweeps on A.
+
+constexpr double MG_OMEGA = 0.8;
+
+// diag(A): the row's coefficients summed in the row's order; 1 for an empty row
+template <int ND>
+__global__ void __launch_bounds__(GB) k_diag(Geom g, GravP P, double *diag)
+{
+    for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
+        double s = 0.0;
+#pragma unroll
+        for (int d = ND - 1; d >= 0; --d) {
+            const int64_t nb = gnb(g, P, i, cc[d], d, false);
+            if (nb >= 0 && nb < i) s = s + P.coef[d];
+        }
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const int64_t nb = gnb(g, P, i, cc[d], d, true);
+            if (nb < 0) continue;
+            s = s + P.coef[d];
+            if (nb == i) s = s + P.coef[d];
+        }
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const int64_t nb = gnb(g, P, i, cc[d], d, false);
+            if (nb > i) s = s + P.coef[d];
+        }
+        diag[i] = s == 0.0 ? 1.0 : s;
+    });
+}
+
+// one damped-Jacobi sweep on A (_matvec! then _csr_jacobi!, mg_pcg.jl:148-150):
+// xout = x + omega (rhs - A x) / diag; xin == nullptr stands for x = 0
+template <int ND>
+__global__ void __launch_bounds__(GB) k_ajac(Geom g, GravP P, const double *__restrict__ xin,
+                                            const double *__restrict__ rhs,
+                                            const double *__restrict__ diag, double *xout,
+                                            const GravCtrl *gc)
+{
+    if (gc->done) return;
+    for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
+        const double ax = xin ? lap_row<ND>(g, P, xin, i, cc) : 0.0;
+        const double xv = xin ? xin[i] : 0.0;
+        xout[i] = xv + MG_OMEGA * (rhs[i] - ax) / diag[i];
+    });
+}
+
+// mr = rhs - A x, and the base-grid right-hand side (0 + mr: the scatter onto
+// a zeroed base grid, one cell per base cell on a uniform mesh)
+template <int ND>
+__global__ void __launch_bounds__(GB) k_aresid(Geom g, GravP P, const double *__restrict__ x,
+                                              const double *__restrict__ rhs, double *mr, double *tb,
+                                              const GravCtrl *gc)
+{
+    if (gc->done) return;
+    for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
+        const double m = rhs[i] - lap_row<ND>(g, P, x, i, cc);
+        mr[i] = m;
+        tb[i] = 0.0 + m;
+    });
+}
+
+__device__ __forceinline__ int mg_wrap(int a, int n) { return a < 0 ? n - 1 : (a >= n ? 0 : a); }
+
+// _mgk_jacobi! (mg_pcg.jl:21-31): phi = (1 - w) phiold + w (sum_nb + h^2 b) / 6
+__global__ void __launch_bounds__(GB) k_mg_jacobi(int n, double h2, const double *__restrict__ phiold,
+                                                 const double *__restrict__ b, double *phi,
+                                                 const GravCtrl *gc)
+{
+    if (gc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * n * n) return;
+    const int x = i % n, y = (i / n) % n, z = i / (n * n);
+    const int nn = n * n;
+    const double s = phiold[i - x + mg_wrap(x - 1, n)] + phiold[i - x + mg_wrap(x + 1, n)] +
+                     phiold[i - y * n + mg_wrap(y - 1, n) * n] + phiold[i - y * n + mg_wrap(y + 1, n) * n] +
+                     phiold[i - z * nn + mg_wrap(z - 1, n) * nn] + phiold[i - z * nn + mg_wrap(z + 1, n) * nn];
+    phi[i] = (1.0 - MG_OMEGA) * phiold[i] + MG_OMEGA * (s + h2 * b[i]) / 6.0;
+}
+
+// _mgk_residual! (33-43): r = b - (6 phi - sum_nb) / h^2
+__global__ void __launch_bounds__(GB) k_mg_residual(int n, double invh2, const double *__restrict__ phi,
+                                                   const double *__restrict__ b, double *r,
+                                                   const GravCtrl *gc)
+{
+    if (gc->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * n * n) return;
+    const int x = i % n, y = (i / n) % n, z = i / (n * n);
+    const int nn = n * n;
+    const double s = phi[i - x + mg_wrap(x - 1, n)] + phi[i - x + mg_wrap(x + 1, n)] +
+                     phi[i - y * n + mg_wrap(y - 1, n) * n] + phi[i - y * n + mg_wrap(y + 1, n) * n] +
+                     phi[i - z * nn + mg_wrap(z - 1, n) * nn] + phi[i - z * nn + mg_wrap(z + 1, n) * nn];
+    r[i] = b[i] - (6.0 * phi[i] - s) * invh2;
+}
+
+// _mgk_restrict! (45-53): coarse = mean of the 8 fine children; coarse e = 0
+__global__ void __launch_bounds__(GB) k_mg_restrict(int nc, const double *__restrict__ rf, double *bc,
+                                                   double *ec, const GravCtrl *gc)
+{
+    if (gc->done) return;
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= nc * nc * nc) return;
+    const int X = I % nc, Y = (I / nc) % nc, Z = I / (nc * nc);
+    const int n = 2 * nc, x = 2 * X, y = 2 * Y, z = 2 * Z;
+    auto f = [&](int a, int b_, int c) { return rf[a + n * (b_ + n * c)]; };
+    bc[I] = 0.125 * (f(x, y, z) + f(x + 1, y, z) + f(x, y + 1, z) + f(x + 1, y + 1, z) + f(x, y, z + 1) +
+                     f(x + 1, y, z + 1) + f(x, y + 1, z + 1) + f(x + 1, y + 1, z + 1));
+    ec[I] = 0.0;
+}
+
+// _mgk_prolong_add! (55-66): trilinear cell-centred prolongation (weights 3/4,
+// 1/4, periodic) added into the fine level
+__global__ void __launch_bounds__(GB) k_mg_prolong_add(int nc, const double *__restrict__ phic,
+                                                      double *phif, const GravCtrl *gc)
+{
+    if (gc->done) return;
+    const int n = 2 * nc;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * n * n) return;
+    const int x = i % n, y = (i / n) % n, z = i / (n * n);
+    const int ic[2] = {x / 2, mg_wrap(x / 2 + ((x & 1) ? 1 : -1), nc)};
+    const int jc[2] = {y / 2, mg_wrap(y / 2 + ((y & 1) ? 1 : -1), nc)};
+    const int kc[2] = {z / 2, mg_wrap(z / 2 + ((z & 1) ? 1 : -1), nc)};
+    const double w[2] = {0.75, 0.25};
+    double v = 0.0;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                v = v + w[a] * w[b] * w[c] * phic[ic[a] + nc * (jc[b] + nc * kc[c])];
+    phif[i] = phif[i] + v;
+}
+
+__global__ void __launch_bounds__(GB) k_fill0(int64_t n, double *e, const GravCtrl *gc)
+{
+    if (gc->done) return;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < n; i += (int64_t)gridDim.x * GB)
+        e[i] = 0.0;
+}
+
+// partials of sum(e) over the base grid (the correction's mean)
+__global__ void __launch_bounds__(GB) k_sumpart(int64_t n, const double *__restrict__ e, double *part,
+                                               const GravCtrl *gc)
+{
+    __shared__ double sh[GB];
+    if (gc->done) return;
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < n; i += (int64_t)GP * GB) s = s + e[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(1024) k_sum_final(const double *part, int64_t n, GravCtrl *gc)
+{
+    __shared__ double sh[1024];
+    if (gc->done) return;
+    const double s = final_sum(part, sh);
+    if (threadIdx.x == 0) gc->mgmu = s / (double)n;
+}
+
+// z += (e - mean) / Vbase + 0 * mr / diag  (_mgk_gather! with gamma = 0, then x .+= mc)
+__global__ void __launch_bounds__(GB) k_mg_gather_add(int64_t n, const double *__restrict__ e,
+                                                     const double *__restrict__ mr,
+                                                     const double *__restrict__ diag, double Vbase,
+                                                     double *z, const GravCtrl *gc)
+{
+    if (gc->done) return;
+    const double mu = gc->mgmu;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < n; i += (int64_t)GP * GB) {
+        const double mc = (e[i] - mu) / Vbase + 0.0 * mr[i] / diag[i];
+        z[i] = z[i] + mc;
+    }
+}
+
+// PCG start after z = M^-1 r: p = z; partials of r.z
+__global__ void __launch_bounds__(GB) k_pcg_start(Geom g, const double *__restrict__ r,
+                                                 const double *__restrict__ z, double *p, double *part)
+{
+    __shared__ double sh[GB];
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB) {
+        p[i] = z[i];
+        s = s + r[i] * z[i];
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// rz of the start (r.z): held in rsold, as the reference's rz
+__global__ void __launch_bounds__(1024) k_pcg_start_final(const double *part, GravCtrl *gc)
+{
+    __shared__ double sh[1024];
+    const double rz = final_sum(part, sh);
+    if (threadIdx.x == 0) gc->rsold = rz;
+}
+
+// relres from r.r; stop at tol (mg_pcg.jl:202-203)
+__global__ void __launch_bounds__(1024) k_pcg_check(const double *part, GravCtrl *gc)
+{
+    __shared__ double sh[1024];
+    if (gc->done) return;
+    const double rr = final_sum(part, sh);
+    if (threadIdx.x == 0) {
+        gc->relres = sqrt(rr) / gc->bnorm;
+        if (gc->relres <= gc->tol) gc->done = 1;
+    }
+}
+
+// partials of r.z (after the preconditioner)
+__global__ void __launch_bounds__(GB) k_pcg_rz(Geom g, const double *__restrict__ r,
+                                              const double *__restrict__ z, double *part,
+                                              const GravCtrl *gc)
+{
+    __shared__ double sh[GB];
+    if (gc->done) return;
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB)
+        s = s + r[i] * z[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// beta = rznew / rz; rz = rznew; stop after maxiter
+__global__ void __launch_bounds__(1024) k_pcg_beta(const double *part, GravCtrl *gc)
+{
+    __shared__ double sh[1024];
+    if (gc->done) return;
+    const double rz = final_sum(part, sh);
+    if (threadIdx.x == 0) {
+        gc->beta = rz / gc->rsold;
+        gc->rsold = rz;
+        if (gc->iters >= gc->maxiter) gc->done = 1;
+    }
+}
+
 }  // namespace
 }  // namespace vb
 
@@ -346,6 +594,17 @@ struct vb_gravity {
     cudaGraphExec_t gexec = nullptr;
     int64_t maxiter = 500;
     double tol = 1e-8;
+    // multigrid preconditioner (precond = VB_GRAV_PRECOND_MG)
+    int precond = VB_GRAV_PRECOND_NONE;
+    double *z = nullptr, *z2 = nullptr, *mr = nullptr, *diag = nullptr;
+    struct Level {
+        int n;
+        double h;
+        double *e, *b, *r, *t;
+    };
+    std::vector<Level> lev;  // base grid first, then each coarsening
+    double hbase = 0.0, vbase = 0.0;
+    int64_t graph_launches = 0;  // kernels per replay of the iteration graph
 };
 
 namespace {
@@ -373,15 +632,92 @@ int queue_iteration(vb_grid *gr, vb_gravity *gv)
     return VB_OK;
 }
 
+inline unsigned mg_blocks(int64_t n) { return (unsigned)((n + vb::GB - 1) / vb::GB); }
+
+// z = M^-1 r (one composite-smoothed two-level cycle)
+int queue_precond(vb_grid *gr, vb_gravity *gv)
+{
+    cudaStream_t s = gr->ctx->stream;
+    const vb::Geom &g = gr->g;
+    const vb::GravP &P = gv->P;
+    auto ajac = [&](const double *xin, double *xout) {
+        vb::k_ajac<3><<<vb::GP, vb::GB, 0, s>>>(g, P, xin, gv->r, gv->diag, xout, gv->gc);
+        return 1;
+    };
+    VB_CHECK_LAUNCH(gr->ctx, ajac(nullptr, gv->z2));  // pre-smooth from z = 0
+    VB_CHECK_LAUNCH(gr->ctx, ajac(gv->z2, gv->z));
+    auto &top = gv->lev[0];
+    vb::k_aresid<3><<<vb::GP, vb::GB, 0, s>>>(g, P, gv->z, gv->r, gv->mr, top.b, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 1);
+    vb::k_fill0<<<vb::GP, vb::GB, 0, s>>>((int64_t)top.n * top.n * top.n, top.e, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 1);
+    // V-cycle: down the levels, then back up
+    const int L = (int)gv->lev.size();
+    auto jacobi = [&](const vb_gravity::Level &l, int sweeps) {
+        const double h2 = l.h * l.h;
+        const unsigned nb = mg_blocks((int64_t)l.n * l.n * l.n);
+        for (int k = 0; k < sweeps; k += 2) {  // even counts end in e
+            vb::k_mg_jacobi<<<nb, vb::GB, 0, s>>>(l.n, h2, l.e, l.b, l.t, gv->gc);
+            vb::k_mg_jacobi<<<nb, vb::GB, 0, s>>>(l.n, h2, l.t, l.b, l.e, gv->gc);
+        }
+        return sweeps;
+    };
+    for (int k = 0; k + 1 < L; ++k) {
+        const auto &l = gv->lev[k], &c = gv->lev[k + 1];
+        VB_CHECK_LAUNCH(gr->ctx, jacobi(l, 2));
+        vb::k_mg_residual<<<mg_blocks((int64_t)l.n * l.n * l.n), vb::GB, 0, s>>>(
+            l.n, 1.0 / (l.h * l.h), l.e, l.b, l.r, gv->gc);
+        vb::k_mg_restrict<<<mg_blocks((int64_t)c.n * c.n * c.n), vb::GB, 0, s>>>(c.n, l.r, c.b, c.e, gv->gc);
+        VB_CHECK_LAUNCH(gr->ctx, 2);
+    }
+    VB_CHECK_LAUNCH(gr->ctx, jacobi(gv->lev[L - 1], 32));  // coarsest: 2 pre + 30 sweeps
+    for (int k = L - 2; k >= 0; --k) {
+        const auto &l = gv->lev[k], &c = gv->lev[k + 1];
+        vb::k_mg_prolong_add<<<mg_blocks((int64_t)l.n * l.n * l.n), vb::GB, 0, s>>>(c.n, c.e, l.e, gv->gc);
+        VB_CHECK_LAUNCH(gr->ctx, 1);
+        VB_CHECK_LAUNCH(gr->ctx, jacobi(l, 2));
+    }
+    const int64_t nt = (int64_t)top.n * top.n * top.n;
+    vb::k_sumpart<<<vb::GP, vb::GB, 0, s>>>(nt, top.e, gv->part + 2 * vb::GP, gv->gc);
+    vb::k_sum_final<<<1, 1024, 0, s>>>(gv->part + 2 * vb::GP, nt, gv->gc);
+    vb::k_mg_gather_add<<<vb::GP, vb::GB, 0, s>>>(nt, top.e, gv->mr, gv->diag, gv->vbase, gv->z, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 3);
+    VB_CHECK_LAUNCH(gr->ctx, ajac(gv->z, gv->z2));  // post-smooth
+    VB_CHECK_LAUNCH(gr->ctx, ajac(gv->z2, gv->z));
+    return VB_OK;
+}
+
+// One preconditioned CG iteration (mg_pcg.jl:194-209).
+int queue_pcg_iteration(vb_grid *gr, vb_gravity *gv)
+{
+    cudaStream_t s = gr->ctx->stream;
+    const vb::Geom &g = gr->g;
+    vb::k_cg_matvec<3><<<vb::GP, vb::GB, 0, s>>>(g, gv->P, gv->p, gv->Ap, gv->part, gv->gc);
+    vb::k_cg_alpha<<<1, 1024, 0, s>>>(gv->part, gv->gc);
+    vb::k_cg_update<<<vb::GP, vb::GB, 0, s>>>(g, gv->phi, gv->p, gv->r, gv->Ap, gv->part, gv->gc);
+    vb::k_pcg_check<<<1, 1024, 0, s>>>(gv->part, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, 4);
+    int rc = queue_precond(gr, gv);
+    if (rc) return rc;
+    vb::k_pcg_rz<<<vb::GP, vb::GB, 0, s>>>(g, gv->r, gv->z, gv->part, gv->gc);
+    vb::k_pcg_beta<<<1, 1024, 0, s>>>(gv->part, gv->gc);
+    vb::k_cg_dir<<<vb::GP, vb::GB, 0, s>>>(g, gv->p, gv->z, gv->gc);  // p = z + beta p
+    VB_CHECK_LAUNCH(gr->ctx, 3);
+    return VB_OK;
+}
+
 int capture_iterations(vb_grid *gr, vb_gravity *gv)
 {
     cudaStream_t s = gr->ctx->stream;
     VB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     const int64_t before = gr->ctx->launches;
     int rc = VB_OK;
-    for (int k = 0; k < vb::GRAPH_ITERS && !rc; ++k) rc = queue_iteration(gr, gv);
+    gv->graph_launches = 0;
+    for (int k = 0; k < vb::GRAPH_ITERS && !rc; ++k)
+        rc = gv->precond == VB_GRAV_PRECOND_MG ? queue_pcg_iteration(gr, gv) : queue_iteration(gr, gv);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(s, &graph);
+    gv->graph_launches = gr->ctx->launches - before;
     gr->ctx->launches = before;  // counted per replay
     if (rc) {
         if (graph) cudaGraphDestroy(graph);
@@ -418,6 +754,16 @@ void free_gravity(vb_gravity *gv)
     cudaFree(gv->part);
     cudaFree(gv->gc);
     cudaFreeHost(gv->hgc);
+    cudaFree(gv->z);
+    cudaFree(gv->z2);
+    cudaFree(gv->mr);
+    cudaFree(gv->diag);
+    for (auto &l : gv->lev) {
+        cudaFree(l.e);
+        cudaFree(l.b);
+        cudaFree(l.r);
+        cudaFree(l.t);
+    }
     delete gv;
 }
 
@@ -453,6 +799,13 @@ int vb::detail::gravity_solve(vb_grid *gr, int64_t *iters, double *relres)
     VB_CHECK_LAUNCH(gr->ctx, ND_DISPATCH(g.nd, k_cg_init, g, gv->P, gv->phi, gv->b, gv->r, gv->p, gv->part));
     k_cg_init_final<<<1, 1024, 0, s>>>(gv->part, gv->gc);
     VB_CHECK_LAUNCH(gr->ctx, 1);
+    if (gv->precond == VB_GRAV_PRECOND_MG) {  // z = M^-1 r, p = z, rz (mg_pcg.jl:188-191)
+        int rc = queue_precond(gr, gv);
+        if (rc) return rc;
+        k_pcg_start<<<GP, GB, 0, s>>>(g, gv->r, gv->z, gv->p, gv->part);
+        k_pcg_start_final<<<1, 1024, 0, s>>>(gv->part, gv->gc);
+        VB_CHECK_LAUNCH(gr->ctx, 2);
+    }
     if (!gv->gexec) {
         int rc = capture_iterations(gr, gv);
         if (rc) return rc;
@@ -460,7 +813,7 @@ int vb::detail::gravity_solve(vb_grid *gr, int64_t *iters, double *relres)
     // the stop flag is set by convergence, p.Ap <= 0 or maxiter, so this ends
     for (;;) {
         VB_CUDA(cudaGraphLaunch(gv->gexec, s));
-        gr->ctx->launches += 5 * GRAPH_ITERS;
+        gr->ctx->launches += gv->graph_launches;
         VB_CUDA(cudaMemcpyAsync(gv->hgc, gv->gc, sizeof(GravCtrl), cudaMemcpyDeviceToHost, s));
         VB_CUDA(cudaStreamSynchronize(s));
         if (gv->hgc->done) break;
@@ -513,6 +866,16 @@ int vb_gravity_enable(vb_grid *gr, const vb_gravity_desc *d)
     }
     P.G = d->G;
     P.project_mean = d->project_mean ? 1 : 0;
+    if (d->precond != VB_GRAV_PRECOND_NONE && d->precond != VB_GRAV_PRECOND_MG)
+        return fail(VB_EINVAL, "unknown preconditioner");
+    if (d->precond == VB_GRAV_PRECOND_MG) {
+        // the base-grid V-cycle is periodic and cubic (mg_pcg.jl:88-89)
+        bool ok = g.nd == 3 && g.n[0] == g.n[1] && g.n[1] == g.n[2] && g.n[0] <= 1024;
+        for (int a = 0; a < 3; ++a) ok = ok && P.per_lo[a] && P.per_hi[a];
+        if (!ok)
+            return fail(VB_ENOTSUP, "the multigrid preconditioner needs a 3D cubic grid (n <= 1024) "
+                                    "with periodic phi on every side");
+    }
     vb_gravity *gv = gr->grav;
     if (!gv) {
         gv = new vb_gravity;
@@ -521,7 +884,7 @@ int vb_gravity_enable(vb_grid *gr, const vb_gravity_desc *d)
         for (double **buf : {&gv->phi, &gv->b, &gv->r, &gv->p, &gv->Ap})
             if (e == cudaSuccess) e = cudaMalloc(buf, n);
         if (e == cudaSuccess) e = cudaMalloc(&gv->gacc, n * g.nd);
-        if (e == cudaSuccess) e = cudaMalloc(&gv->part, sizeof(double) * 2 * vb::GP);
+        if (e == cudaSuccess) e = cudaMalloc(&gv->part, sizeof(double) * 3 * vb::GP);
         if (e == cudaSuccess) e = cudaMalloc(&gv->gc, sizeof(vb::GravCtrl));
         if (e == cudaSuccess) e = cudaMallocHost(&gv->hgc, sizeof(vb::GravCtrl));
         if (e == cudaSuccess) e = cudaMemsetAsync(gv->phi, 0, n, gr->ctx->stream);  // phi starts at 0
@@ -539,6 +902,44 @@ int vb_gravity_enable(vb_grid *gr, const vb_gravity_desc *d)
     gv->maxiter = d->maxiter;
     gv->tol = d->tol;
     gr->grav = gv;
+    if (gv->gexec) {  // the iteration graph depends on the preconditioner
+        cudaGraphExecDestroy(gv->gexec);
+        gv->gexec = nullptr;
+    }
+    gv->precond = d->precond;
+    if (gv->precond == VB_GRAV_PRECOND_MG && !gv->z) {
+        // levels: coarsen while even and > 4 (mg_pcg.jl:111-116)
+        const size_t n = (size_t)g.ncell * sizeof(double);
+        cudaError_t e = cudaSuccess;
+        for (double **buf : {&gv->z, &gv->z2, &gv->mr, &gv->diag})
+            if (e == cudaSuccess) e = cudaMalloc(buf, n);
+        gv->hbase = g.w[0];
+        gv->vbase = gv->hbase * gv->hbase * gv->hbase;
+        int nl = (int)g.n[0];
+        double h = gv->hbase;
+        for (;;) {
+            vb_gravity::Level l{nl, h, nullptr, nullptr, nullptr, nullptr};
+            const size_t bytes = sizeof(double) * (size_t)nl * nl * nl;
+            for (double **buf : {&l.e, &l.b, &l.r, &l.t})
+                if (e == cudaSuccess) e = cudaMalloc(buf, bytes);
+            gv->lev.push_back(l);
+            if (!(nl > 4 && nl % 2 == 0)) break;
+            nl /= 2;
+            h *= 2.0;
+        }
+        if (e == cudaSuccess) {
+            cudaStream_t s = gr->ctx->stream;
+            vb::k_diag<3><<<vb::GP, vb::GB, 0, s>>>(g, P, gv->diag);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        }
+        if (e != cudaSuccess) {
+            gr->grav = nullptr;
+            free_gravity(gv);
+            return fail(e == cudaErrorMemoryAllocation ? VB_ENOMEM : VB_ECUDA,
+                        std::string("multigrid allocation: ") + cudaGetErrorString(e));
+        }
+    }
     gr->g.grav_g = gv->gacc;
     gr->g.grav_G = d->G;
     gr->invdt_valid = false;  // the free-fall limiter joins the CFL maximum

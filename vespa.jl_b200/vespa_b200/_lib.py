@@ -53,6 +53,7 @@ class GravityDesc(C.Structure):
         ("bc_lo", C.c_int32 * 3),
         ("bc_hi", C.c_int32 * 3),
         ("project_mean", C.c_int32),
+        ("precond", C.c_int32),
         ("flags", C.c_int32),
     ]
 

@@ -24,8 +24,14 @@ class GravityField:
     """enable_gravity!'s GravityField (src/gravity.jl:34-49): phi and the
     solver configuration, bound to one Simulation."""
 
-    def __init__(self, sim, G: float, bcs, maxiter: int, tol: float, project_mean: bool):
+    PRECONDS = {"none": 0, "mg": 1}
+
+    def __init__(self, sim, G: float, bcs, maxiter: int, tol: float, project_mean: bool,
+                 precond: str = "none"):
+        if precond not in self.PRECONDS:
+            raise ValueError("precond must be 'none' or 'mg'")
         self.sim = sim
+        self.precond = precond
         self.G = float(G)
         self.bcs = bcs
         self.maxiter = int(maxiter)
@@ -39,6 +45,7 @@ class GravityField:
             desc.bc_lo[d] = lo.code
             desc.bc_hi[d] = hi.code
         desc.project_mean = int(self.project_mean)
+        desc.precond = self.PRECONDS[precond]
         desc.flags = 0
         _lib.call("vb_gravity_enable", sim.handle, C.byref(desc))
 
@@ -63,12 +70,14 @@ class GravityField:
 
 
 def enable_gravity(sim, *, G: float = 1.0, bcs=Periodic, maxiter: int = 500, tol: float = 1e-8,
-                   project_mean: Optional[bool] = None) -> GravityField:
-    """enable_gravity!(sim; G, bcs, maxiter, tol, project_mean) (src/gravity.jl:65-83).
-    project_mean defaults to bcs being Periodic, as in the reference."""
+                   project_mean: Optional[bool] = None, precond: str = "none") -> GravityField:
+    """enable_gravity!(sim; G, bcs, maxiter, tol, project_mean, precond)
+    (src/gravity.jl:65-83).  project_mean defaults to bcs being Periodic, as in
+    the reference; precond is "none" (plain CG) or "mg" (CG preconditioned by
+    one multigrid cycle, ext/mg_pcg.jl; 3D cubic periodic grids)."""
     if project_mean is None:
         project_mean = isinstance(bcs, BC) and bcs == Periodic
-    grav = GravityField(sim, G, bcs, maxiter, tol, project_mean)
+    grav = GravityField(sim, G, bcs, maxiter, tol, project_mean, precond)
     sim.grav = grav
     return grav
 
