@@ -120,6 +120,10 @@ def lib():
         L.vo_compute_dt_gravity.argtypes = [gp, C.c_double, dp]
         L.vo_compute_dt_gravity.restype = C.c_double
         L.vo_step_gravity.argtypes = [gp, dp, dp, dp, dp, C.c_double]
+        i64p = C.POINTER(C.c_int64)
+        L.vo_muscl_step.argtypes = [i64p, C.c_int, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, C.c_int, dp]
+        L.vo_muscl_flux_line.argtypes = [i64, C.c_int, dp, C.c_double, C.c_double, C.c_double, dp]
         _lib = L
     return _lib
 
@@ -389,3 +393,23 @@ def step_gravity(g: VoGrid, gacc, U, dt):
     acc = np.empty_like(U)
     lib().vo_step_gravity(C.byref(g), _dp(gacc), _dp(U), _dp(u0), _dp(acc), float(dt))
     return U
+
+
+# ------------------------------------------------- PPMKernels unsplit MUSCL
+def muscl_step(dims, ng, U, dt, gamma, theta=1.5, dx=1.0, small_rho=1e-10, bc=0):
+    """muscl_step_3d! in place on U, a (5, N) float64 array (D, S1, S2, S3, Tau)."""
+    assert U.dtype == np.float64 and U.flags.c_contiguous
+    d = (C.c_int64 * 3)(*[int(x) for x in dims])
+    lib().vo_muscl_step(d, int(ng), float(dt), float(gamma), float(theta), float(dx),
+                        float(small_rho), int(bc), _dp(U))
+    return U
+
+
+def muscl_flux_line(prim, ng, gamma, theta=1.5, small_rho=1e-10):
+    """muscl_flux_line! on one pencil: prim (5, na) -> F (5, na - 2 ng + 1)."""
+    prim = np.ascontiguousarray(prim, dtype=np.float64)
+    na = prim.shape[1]
+    F = np.empty((5, na - 2 * ng + 1))
+    lib().vo_muscl_flux_line(na, int(ng), _dp(prim), float(gamma), float(theta),
+                             float(small_rho), _dp(F))
+    return F

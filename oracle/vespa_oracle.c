@@ -842,3 +842,178 @@ void vo_step_gravity(const vo_grid *g, const double *gacc, double *U, double *u0
     grav_source(&G, U, gacc, acc);
     for (int64_t i = 0; i < n5; ++i) U[i] = 0.5 * u0[i] + 0.5 * (U[i] - invV * acc[i]);
 }
+
+/* ------------------------------------- lib/PPMKernels: unsplit MUSCL (RK2) */
+/* muscl_step_3d! (lib/PPMKernels/src/muscl_grid.jl:314-380): Enzo's
+ * HydroMethod=3 step on five conserved arrays D, S1, S2, S3, Tau (Tau = rho *
+ * specific total energy) of dims (nx, ny, nz) flat column-major with ng ghost
+ * zones each side.  Restated in the reference's structure: per stage the
+ * primitives (_cons2prim_k!, 23-34), then per axis the PLM + HLL flux line over
+ * every pencil (ghost pencils included) and the flux divergence added into one
+ * zeroed dU (x in place, y and z through zero-filled slabs that are added over
+ * the whole grid), then the SSP-RK2 update of every cell. */
+
+static inline double msign(double x) { return x > 0.0 ? 1.0 : -1.0; } /* _msign, muscl.jl:13 */
+
+/* _minmod3, muscl.jl:16-19 */
+static inline double minmod3(double a, double b, double c)
+{
+    double sa = msign(a), sb = msign(b), sc = msign(c);
+    return 0.25 * (sa + sb) * fabs(sa + sc) * jl_min(fabs(a), jl_min(fabs(b), fabs(c)));
+}
+
+/* _plm_pt, muscl.jl:24-26: v + 0.5 * minmod3((v - vm1) th, (vp1 - v) th, 0.5 (vp1 - vm1)) */
+static inline double plm_pt(double vm1, double v, double vp1, double th)
+{
+    return v + 0.5 * minmod3((v - vm1) * th, (vp1 - v) * th, 0.5 * (vp1 - vm1));
+}
+
+/* _hll, muscl.jl:29-30 */
+static inline double hll1(double ap, double am, double fl, double fr, double ul, double ur)
+{
+    return (ap * fl + am * fr - ap * am * (ur - ul)) / (ap + am);
+}
+
+/* _hll5 / the first five of _hll6, muscl.jl:35-78: primitive L/R states
+ * (rho, eint, u_normal, v, w) -> (F_rho, F_normal, F_t1, F_t2, F_E) */
+static void hll5(double rl, double el, double ul, double vl, double wl, double rr, double er,
+                 double ur, double vr, double wr, double g, double gm1, double F[5])
+{
+    const double h = 0.5;
+    double v2l = ul * ul + vl * vl + wl * wl, pl = gm1 * rl * el, csl = sqrt(g * pl / rl);
+    double etl = el + h * v2l;
+    double UlD = rl, UlS1 = rl * ul, UlS2 = rl * vl, UlS3 = rl * wl, UlE = rl * etl;
+    double FlD = rl * ul, FlS1 = UlS1 * ul + pl, FlS2 = UlS2 * ul, FlS3 = UlS3 * ul, FlE = (UlE + pl) * ul;
+    double lpl = ul + csl, lml = ul - csl;
+    double v2r = ur * ur + vr * vr + wr * wr, pr = gm1 * rr * er, csr = sqrt(g * pr / rr);
+    double etr = er + h * v2r;
+    double UrD = rr, UrS1 = rr * ur, UrS2 = rr * vr, UrS3 = rr * wr, UrE = rr * etr;
+    double FrD = rr * ur, FrS1 = UrS1 * ur + pr, FrS2 = UrS2 * ur, FrS3 = UrS3 * ur, FrE = (UrE + pr) * ur;
+    double lpr = ur + csr, lmr = ur - csr;
+    double ap = jl_max(0.0, jl_max(lpl, lpr)), am = jl_max(0.0, jl_max(-lml, -lmr));
+    F[0] = hll1(ap, am, FlD, FrD, UlD, UrD);
+    F[1] = hll1(ap, am, FlS1, FrS1, UlS1, UrS1);
+    F[2] = hll1(ap, am, FlS2, FrS2, UlS2, UrS2);
+    F[3] = hll1(ap, am, FlS3, FrS3, UlS3, UrS3);
+    F[4] = hll1(ap, am, FlE, FrE, UlE, UrE);
+}
+
+/* _muscl_hll_kernel! (muscl.jl:181-215) for one pencil of primitives q[5][na]
+ * (rho, eint, u_normal, v_t1, v_t2) with stride `st`: fluxes at the nfi = na -
+ * 2 ng + 1 interfaces, F[5][nfi]. */
+static void flux_line(const double *const q[5], int64_t base, int64_t st, int64_t na, int ng,
+                      double g, double th, double small_rho, double *F)
+{
+    const int64_t nfi = na - 2 * ng + 1;
+    const double gm1 = g - 1.0;
+    for (int64_t gi = 0; gi < nfi; ++gi) {
+        const int64_t cl = ng + gi - 1; /* left cell of the interface, 0-based */
+#define Q(f, m) q[f][base + (m) * st]
+        double L[5], R[5];
+        for (int f = 0; f < 5; ++f) {
+            L[f] = plm_pt(Q(f, cl - 1), Q(f, cl), Q(f, cl + 1), th);
+            R[f] = plm_pt(Q(f, cl + 2), Q(f, cl + 1), Q(f, cl), th);
+        }
+#undef Q
+        L[0] = jl_max(L[0], small_rho);
+        R[0] = jl_max(R[0], small_rho);
+        double Fi[5];
+        hll5(L[0], L[1], L[2], L[3], L[4], R[0], R[1], R[2], R[3], R[4], g, gm1, Fi);
+        for (int f = 0; f < 5; ++f) F[f * nfi + gi] = Fi[f];
+    }
+}
+
+/* dU of one stage: prim = cons2prim(U) everywhere, dU = 0 + axis sweeps */
+static void muscl_L(const int64_t dims[3], int ng, double dt, double g, double th, double dx,
+                    double small_rho, double *const U[5], double *prim, double *dU, double *slab)
+{
+    const int64_t N = dims[0] * dims[1] * dims[2];
+    double *rho = prim, *eint = prim + N, *vx = prim + 2 * N, *vy = prim + 3 * N, *vz = prim + 4 * N;
+    for (int64_t i = 0; i < N; ++i) { /* _cons2prim_k! */
+        double d = U[0][i], u = U[1][i] / d, v = U[2][i] / d, w = U[3][i] / d;
+        rho[i] = d; vx[i] = u; vy[i] = v; vz[i] = w;
+        eint[i] = jl_max(U[4][i] / d - 0.5 * (u * u + v * v + w * w), small_rho);
+    }
+    memset(dU, 0, sizeof(double) * 5 * N);
+    const double dtdx = dt / dx;
+    const int64_t stride[3] = {1, dims[0], dims[0] * dims[1]};
+    for (int axis = 0; axis < 3; ++axis) {
+        const int64_t na = dims[axis], nfi = na - 2 * ng + 1, st = stride[axis];
+        /* cyclic roles (normal, t1, t2), muscl_grid.jl:236 */
+        const double *vu = axis == 0 ? vx : axis == 1 ? vy : vz;
+        const double *vv = axis == 0 ? vy : axis == 1 ? vz : vx;
+        const double *vw = axis == 0 ? vz : axis == 1 ? vx : vy;
+        const double *q[5] = {rho, eint, vu, vv, vw};
+        /* momentum slots receiving (normal, t1, t2) */
+        const int sn = 1 + axis, s1 = 1 + (axis + 1) % 3, s2 = 1 + (axis + 2) % 3;
+        const int slot[5] = {0, sn, s1, s2, 4};
+        double *F = malloc(sizeof(double) * 5 * nfi);
+        if (axis > 0) memset(slab, 0, sizeof(double) * 5 * N);
+        /* every pencil: the other two coordinates over their full (ghosted) range */
+        const int64_t o1 = axis == 0 ? 1 : 0, o2 = axis == 2 ? 1 : 2;
+        for (int64_t b = 0; b < dims[o2]; ++b)
+            for (int64_t a = 0; a < dims[o1]; ++a) {
+                const int64_t base = a * stride[o1] + b * stride[o2];
+                flux_line(q, base, st, na, ng, g, th, small_rho, F);
+                for (int64_t m = 0; m < na - 2 * ng; ++m) {
+                    const int64_t c = base + (ng + m) * st;
+                    for (int f = 0; f < 5; ++f) {
+                        const double du = -(F[f * nfi + m + 1] - F[f * nfi + m]) * dtdx;
+                        if (axis == 0) dU[slot[f] * N + c] += du;
+                        else slab[slot[f] * N + c] = du;
+                    }
+                }
+            }
+        if (axis > 0)
+            for (int64_t i = 0; i < 5 * N; ++i) dU[i] += slab[i];
+        free(F);
+    }
+}
+
+/* periodic ghost fill along x, then y, then z (ghost p < ng takes p + active,
+ * p >= ng + active takes p - active) */
+static void muscl_fill_periodic(const int64_t dims[3], int ng, double *const U[5])
+{
+    const int64_t stride[3] = {1, dims[0], dims[0] * dims[1]};
+    const int64_t N = dims[0] * dims[1] * dims[2];
+    for (int axis = 0; axis < 3; ++axis) {
+        const int64_t na = dims[axis], act = na - 2 * ng, st = stride[axis];
+        for (int64_t i = 0; i < N; ++i) {
+            const int64_t p = (i / st) % na;
+            int64_t src = -1;
+            if (p < ng) src = i + act * st;
+            else if (p >= ng + act) src = i - act * st;
+            if (src >= 0)
+                for (int f = 0; f < 5; ++f) U[f][i] = U[f][src];
+        }
+    }
+}
+
+/* One muscl_step_3d! on U = (D, S1, S2, S3, Tau), 5 x N field-major; bc 0:
+ * ghosts untouched (no bc! callback), 1: periodic fill before each stage. */
+void vo_muscl_step(const int64_t dims[3], int ng, double dt, double gamma, double theta,
+                   double dx, double small_rho, int bc, double *U)
+{
+    const int64_t N = dims[0] * dims[1] * dims[2];
+    double *U0 = malloc(sizeof(double) * 5 * N), *prim = malloc(sizeof(double) * 5 * N);
+    double *dU = malloc(sizeof(double) * 5 * N), *slab = malloc(sizeof(double) * 5 * N);
+    double *Uf[5];
+    for (int f = 0; f < 5; ++f) Uf[f] = U + f * N;
+    memcpy(U0, U, sizeof(double) * 5 * N);
+    if (bc == 1) muscl_fill_periodic(dims, ng, Uf);
+    muscl_L(dims, ng, dt, gamma, theta, dx, small_rho, Uf, prim, dU, slab);
+    for (int64_t i = 0; i < 5 * N; ++i) U[i] = U0[i] + dU[i];
+    if (bc == 1) muscl_fill_periodic(dims, ng, Uf);
+    muscl_L(dims, ng, dt, gamma, theta, dx, small_rho, Uf, prim, dU, slab);
+    for (int64_t i = 0; i < 5 * N; ++i) U[i] = 0.5 * (U0[i] + U[i] + dU[i]);
+    free(U0); free(prim); free(dU); free(slab);
+}
+
+/* The reference's certified 1-D flux line (muscl_flux_line!, muscl.jl:223-240)
+ * on one pencil of na primitives (rho, eint, vx, vy, vz), for tests. */
+void vo_muscl_flux_line(int64_t na, int ng, const double *prim, double gamma, double theta,
+                        double small_rho, double *F)
+{
+    const double *q[5] = {prim, prim + na, prim + 2 * na, prim + 3 * na, prim + 4 * na};
+    flux_line(q, 0, 1, na, ng, gamma, theta, small_rho, F);
+}

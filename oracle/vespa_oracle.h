@@ -83,6 +83,16 @@ double vo_compute_dt_gravity(const vo_grid *g, double G, const double *U);
 void vo_step_gravity(const vo_grid *g, const double *gacc, double *U, double *u0, double *acc,
                      double dt);
 
+/* lib/PPMKernels unsplit MUSCL step (muscl_step_3d!): U is 5 x N (D, S1, S2,
+ * S3, Tau) over dims[3] with ng ghost zones; bc 0 leaves ghosts untouched, 1
+ * fills them periodically before each stage. */
+void vo_muscl_step(const int64_t dims[3], int ng, double dt, double gamma, double theta,
+                   double dx, double small_rho, int bc, double *U);
+/* muscl_flux_line! on one pencil: prim is 5 x na (rho, eint, vx, vy, vz); F is
+ * 5 x (na - 2 ng + 1). */
+void vo_muscl_flux_line(int64_t na, int ng, const double *prim, double gamma, double theta,
+                        double small_rho, double *F);
+
 /* exact Riemann solver (src/exact_riemann.jl) */
 void vo_exact_riemann_star(const double *WL, const double *WR, double gamma, double *pu);
 void vo_exact_riemann_sample(const double *WL, const double *WR, double gamma, double s,
