@@ -251,6 +251,43 @@ int vb_gravity_accel(vb_grid *grid, double *g);
  * in the row form of _lap_csr_cpu! (325-334), the one the solver iterates. */
 int vb_gravity_laplacian(vb_grid *grid, const double *x, double *Ax);
 
+/* lib/PPMKernels' unsplit MUSCL step, muscl_step_3d! (lib/PPMKernels/src/
+ * muscl_grid.jl:314-380; Enzo HydroMethod=3): PLM with the minmod-theta
+ * limiter on (rho, eint, v), HLL fluxes, SSP-RK2, float64, on five conserved
+ * arrays D, S1, S2, S3, Tau (Tau = rho * specific total energy) of dims[3]
+ * cells, x fastest, including ng >= 2 ghost zones per side (each dim >=
+ * 2 ng + 1).  The active region per axis is ng .. dims - ng - 1 (0-based).
+ * Ghost zones: VB_MUSCL_BC_NONE leaves them as they are, as the reference does
+ * without a bc! callback; VB_MUSCL_BC_PERIODIC refills them from the opposite
+ * side of the active region before each stage (needs each dim >= 3 ng).
+ * Results are bit-identical to the reference's operation order. */
+typedef struct vb_muscl vb_muscl;
+enum { VB_MUSCL_BC_NONE = 0, VB_MUSCL_BC_PERIODIC = 1 };
+typedef struct {
+    double dt;
+    double gamma;
+    double theta;      /* limiter parameter (the reference's default 1.5) */
+    double dx;
+    double small_rho;  /* density and eint floor (default 1e-10) */
+    int32_t bc;        /* VB_MUSCL_BC_* */
+    int32_t flags;     /* must be 0 */
+} vb_muscl_params;
+/* Scratch for a grid of dims (and an owned state of 5 x N doubles, field-major). */
+int vb_muscl_create(vb_ctx *ctx, const int64_t dims[3], int32_t ng, vb_muscl **out);
+int vb_muscl_destroy(vb_muscl *m);
+int vb_muscl_upload(vb_muscl *m, const double *U);
+int vb_muscl_download(vb_muscl *m, double *U);
+/* device address of the owned state */
+int vb_muscl_state(vb_muscl *m, double **dU);
+/* one step of the owned state (synchronous) */
+int vb_muscl_step(vb_muscl *m, const vb_muscl_params *p);
+/* nsteps steps of the owned state, queued on the context's stream */
+int vb_muscl_run_async(vb_muscl *m, const vb_muscl_params *p, int64_t nsteps);
+/* one step of caller-owned device arrays of the handle's dims: the
+ * signature of muscl_step_3d!(D, S1, S2, S3, Tau, dims, ng; ...) */
+int vb_muscl_step_fields(vb_muscl *m, double *D, double *S1, double *S2, double *S3, double *Tau,
+                         const vb_muscl_params *p);
+
 /* Adjoint of the float64 SSP-RK2 step on a periodic grid (no counterpart in
  * the reference, which has no adjoint; it differentiates the map that
  * step!/evolve! apply, src/driver.jl:285-359,483-508).  Reverse mode, written

@@ -1,0 +1,390 @@
+// vb_muscl.cu -- lib/PPMKernels' unsplit MUSCL step (muscl_step_3d!,
+// lib/PPMKernels/src/muscl_grid.jl:314-380; Enzo HydroMethod=3): PLM with the
+// minmod-theta limiter on (rho, eint, v), the HLL Riemann flux, SSP-RK2, on
+// five conserved arrays (D, S1, S2, S3, Tau = rho * specific total energy)
+// with ng ghost zones per side.  The second scheme behind the library, beside
+// the hydro step of the main path.
+//
+// The reference sweeps the three axes over transposed slabs and adds each
+// axis's flux divergence into one zeroed dU.  Here one thread owns one cell
+// (ghost cells included): it rebuilds the two interface fluxes of each axis
+// along which it is active from the primitives at +-2 cells, and sums
+// dU = ((0 + du_x) + du_y) + du_z exactly as the reference's accumulation
+// reaches that cell (x in place; y and z through zero-filled slabs added over
+// the whole grid).  Every interface flux is evaluated by both of its cells with
+// the same operations, so the result is the reference's.  Compiled with
+// -fmad=false: bit-identical to the oracle's restatement.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "vb_internal.h"
+
+namespace vb {
+namespace {
+
+constexpr int MB = 256;
+
+struct MusclFields {
+    double *f[5];  // D, S1, S2, S3, Tau
+};
+
+struct MusclGeom {
+    int64_t n[3], stride[3], N;
+    int ng;
+    double gamma, theta, dtdx, small_rho;
+};
+
+// Julia's Base.min / max for floats: NaN propagates, the sign of x - y decides
+__device__ __forceinline__ double jmin(double x, double y)
+{
+    const double d = x - y;
+    if (isnan(x) || isnan(y)) return d;
+    return signbit(d) ? x : y;
+}
+__device__ __forceinline__ double jmax(double x, double y)
+{
+    const double d = x - y;
+    if (isnan(x) || isnan(y)) return d;
+    return signbit(d) ? y : x;
+}
+
+// _msign / _minmod3 / _plm_pt, muscl.jl:13-26 (Enzo's sign(0) = -1)
+__device__ __forceinline__ double msign(double x) { return x > 0.0 ? 1.0 : -1.0; }
+__device__ __forceinline__ double minmod3(double a, double b, double c)
+{
+    const double sa = msign(a), sb = msign(b), sc = msign(c);
+    return 0.25 * (sa + sb) * fabs(sa + sc) * jmin(fabs(a), jmin(fabs(b), fabs(c)));
+}
+__device__ __forceinline__ double plm_pt(double vm1, double v, double vp1, double th)
+{
+    return v + 0.5 * minmod3((v - vm1) * th, (vp1 - v) * th, 0.5 * (vp1 - vm1));
+}
+
+// _hll, muscl.jl:29-30
+__device__ __forceinline__ double hll1(double ap, double am, double fl, double fr, double ul, double ur)
+{
+    return (ap * fl + am * fr - ap * am * (ur - ul)) / (ap + am);
+}
+
+// HLL flux of primitive L/R states (rho, eint, u_normal, v, w): the first five
+// components of _hll6 (muscl.jl:57-78; identical to _hll5)
+__device__ __forceinline__ void hll5(const double L[5], const double R[5], double g, double gm1,
+                                     double F[5])
+{
+    const double h = 0.5;
+    const double rl = L[0], el = L[1], ul = L[2], vl = L[3], wl = L[4];
+    const double rr = R[0], er = R[1], ur = R[2], vr = R[3], wr = R[4];
+    const double v2l = ul * ul + vl * vl + wl * wl, pl = gm1 * rl * el, csl = sqrt(g * pl / rl);
+    const double etl = el + h * v2l;
+    const double UlS1 = rl * ul, UlS2 = rl * vl, UlS3 = rl * wl, UlE = rl * etl;
+    const double FlD = rl * ul, FlS1 = UlS1 * ul + pl, FlS2 = UlS2 * ul, FlS3 = UlS3 * ul;
+    const double FlE = (UlE + pl) * ul;
+    const double lpl = ul + csl, lml = ul - csl;
+    const double v2r = ur * ur + vr * vr + wr * wr, pr = gm1 * rr * er, csr = sqrt(g * pr / rr);
+    const double etr = er + h * v2r;
+    const double UrS1 = rr * ur, UrS2 = rr * vr, UrS3 = rr * wr, UrE = rr * etr;
+    const double FrD = rr * ur, FrS1 = UrS1 * ur + pr, FrS2 = UrS2 * ur, FrS3 = UrS3 * ur;
+    const double FrE = (UrE + pr) * ur;
+    const double lpr = ur + csr, lmr = ur - csr;
+    const double ap = jmax(0.0, jmax(lpl, lpr)), am = jmax(0.0, jmax(-lml, -lmr));
+    F[0] = hll1(ap, am, FlD, FrD, rl, rr);
+    F[1] = hll1(ap, am, FlS1, FrS1, UlS1, UrS1);
+    F[2] = hll1(ap, am, FlS2, FrS2, UlS2, UrS2);
+    F[3] = hll1(ap, am, FlS3, FrS3, UlS3, UrS3);
+    F[4] = hll1(ap, am, FlE, FrE, UlE, UrE);
+}
+
+// _cons2prim_k!, muscl_grid.jl:23-34: prim = (rho, eint, vx, vy, vz), eint
+// floored at small_rho
+__global__ void __launch_bounds__(MB) k_muscl_prim(MusclGeom m, MusclFields U, double *prim)
+{
+    const int64_t N = m.N;
+    for (int64_t i = (int64_t)blockIdx.x * MB + threadIdx.x; i < N; i += (int64_t)gridDim.x * MB) {
+        const double d = U.f[0][i], u = U.f[1][i] / d, v = U.f[2][i] / d, w = U.f[3][i] / d;
+        prim[i] = d;
+        prim[2 * N + i] = u;
+        prim[3 * N + i] = v;
+        prim[4 * N + i] = w;
+        prim[N + i] = jmax(U.f[4][i] / d - 0.5 * (u * u + v * v + w * w), m.small_rho);
+    }
+}
+
+// Flux through the interface between cells a (left) and a + st (right) along
+// `axis`, in the reference's flux-line form (_muscl_hll_kernel!, muscl.jl:
+// 181-215): the left state is cell a's right face, the right state is cell
+// a+st's left face taken as the right face of the reversed stencil.  Velocity
+// roles are cyclic (normal, t1, t2); F comes back in that frame.
+__device__ __forceinline__ void iface_flux(const MusclGeom &m, const double *__restrict__ prim,
+                                           int axis, int64_t a, int64_t st, double F[5])
+{
+    const int64_t N = m.N;
+    const int vq[3] = {2 + axis, 2 + (axis + 1) % 3, 2 + (axis + 2) % 3};  // prim rows: 2=vx..4=vz
+    const int row[5] = {0, 1, vq[0], vq[1], vq[2]};
+    double L[5], R[5];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+        const double *q = prim + (int64_t)row[f] * N;
+        const double qm1 = q[a - st], q0 = q[a], q1 = q[a + st], q2 = q[a + 2 * st];
+        L[f] = plm_pt(qm1, q0, q1, m.theta);
+        R[f] = plm_pt(q2, q1, q0, m.theta);
+    }
+    L[0] = jmax(L[0], m.small_rho);
+    R[0] = jmax(R[0], m.small_rho);
+    hll5(L, R, m.gamma, m.gamma - 1.0, F);
+}
+
+// One RK stage over every cell.  STAGE 1: U = U0 + dU; STAGE 2:
+// U = 0.5 (U0 + U + dU) (muscl_grid.jl:350-367).
+template <int STAGE>
+__global__ void __launch_bounds__(MB) k_muscl_stage(MusclGeom m, const double *__restrict__ prim,
+                                                   MusclFields U, const double *__restrict__ U0)
+{
+    const int64_t N = m.N;
+    for (int64_t i = (int64_t)blockIdx.x * MB + threadIdx.x; i < N; i += (int64_t)gridDim.x * MB) {
+        const int64_t c[3] = {i % m.n[0], (i / m.n[0]) % m.n[1], i / (m.n[0] * m.n[1])};
+        double dU[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            const bool active = c[axis] >= m.ng && c[axis] < m.n[axis] - m.ng;
+            double du[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // a zero-filled slab entry
+            if (active) {
+                const int64_t st = m.stride[axis];
+                double Flo[5], Fhi[5];
+                iface_flux(m, prim, axis, i - st, st, Flo);
+                iface_flux(m, prim, axis, i, st, Fhi);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) du[f] = -(Fhi[f] - Flo[f]) * m.dtdx;
+            }
+            if (axis == 0 && !active) continue;  // x adds in place over active cells only
+            // momentum rows receiving (normal, t1, t2)
+            const int slot[5] = {0, 1 + axis, 1 + (axis + 1) % 3, 1 + (axis + 2) % 3, 4};
+#pragma unroll
+            for (int f = 0; f < 5; ++f) dU[slot[f]] = dU[slot[f]] + du[f];
+        }
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            const double u0 = U0[f * N + i];
+            if constexpr (STAGE == 1) U.f[f][i] = u0 + dU[f];
+            else U.f[f][i] = 0.5 * (u0 + U.f[f][i] + dU[f]);
+        }
+    }
+}
+
+// periodic ghost fill along one axis: a ghost p < ng takes p + active, a ghost
+// p >= ng + active takes p - active (the sources are active along this axis)
+__global__ void __launch_bounds__(MB) k_muscl_fill(MusclGeom m, MusclFields U, int axis)
+{
+    const int64_t N = m.N, na = m.n[axis], act = na - 2 * m.ng, st = m.stride[axis];
+    for (int64_t i = (int64_t)blockIdx.x * MB + threadIdx.x; i < N; i += (int64_t)gridDim.x * MB) {
+        const int64_t p = (i / st) % na;
+        int64_t src = -1;
+        if (p < m.ng) src = i + act * st;
+        else if (p >= m.ng + act) src = i - act * st;
+        if (src >= 0)
+#pragma unroll
+            for (int f = 0; f < 5; ++f) U.f[f][i] = U.f[f][src];
+    }
+}
+
+__global__ void __launch_bounds__(MB) k_muscl_copy(int64_t N, MusclFields U, double *U0)
+{
+    for (int64_t i = (int64_t)blockIdx.x * MB + threadIdx.x; i < N; i += (int64_t)gridDim.x * MB)
+#pragma unroll
+        for (int f = 0; f < 5; ++f) U0[f * N + i] = U.f[f][i];
+}
+
+}  // namespace
+}  // namespace vb
+
+using vb::detail::fail;
+using vb::detail::use;
+
+struct vb_muscl {
+    vb_ctx *ctx = nullptr;
+    vb::MusclGeom m{};
+    double *U = nullptr;     // owned state, 5 x N
+    double *U0 = nullptr;    // step-start copy
+    double *prim = nullptr;  // primitives of the stage input
+};
+
+namespace {
+
+int check_params(const vb_muscl_params *p, const vb_muscl *mu)
+{
+    if (!p) return fail(VB_EINVAL, "null parameters");
+    if (p->flags != 0) return fail(VB_EINVAL, "flags must be 0");
+    if (p->bc != VB_MUSCL_BC_NONE && p->bc != VB_MUSCL_BC_PERIODIC)
+        return fail(VB_EINVAL, "unknown ghost-zone mode");
+    if (p->bc == VB_MUSCL_BC_PERIODIC)  // every ghost's periodic source is an active cell
+        for (int a = 0; a < 3; ++a)
+            if (mu->m.n[a] < 3 * (int64_t)mu->m.ng)
+                return fail(VB_EINVAL, "periodic ghost fill needs each dim >= 3 ng");
+    if (!std::isfinite(p->dt) || !(p->gamma > 1.0) || !std::isfinite(p->theta) ||
+        !(p->dx > 0.0) || !std::isfinite(p->small_rho))
+        return fail(VB_EINVAL, "dt, theta and small_rho must be finite, gamma > 1, dx > 0");
+    return VB_OK;
+}
+
+// one muscl_step_3d! on the five fields
+int queue_step(vb_muscl *mu, const vb::MusclFields &F, const vb_muscl_params *p)
+{
+    cudaStream_t s = mu->ctx->stream;
+    vb::MusclGeom m = mu->m;
+    m.gamma = p->gamma;
+    m.theta = p->theta;
+    m.dtdx = p->dt / p->dx;
+    m.small_rho = p->small_rho;
+    const unsigned grid = (unsigned)std::min<int64_t>((m.N + vb::MB - 1) / vb::MB, 148 * 16);
+    auto fill = [&]() {
+        if (p->bc != VB_MUSCL_BC_PERIODIC) return 0;
+        for (int a = 0; a < 3; ++a) vb::k_muscl_fill<<<grid, vb::MB, 0, s>>>(m, F, a);
+        return 3;
+    };
+    vb::k_muscl_copy<<<grid, vb::MB, 0, s>>>(m.N, F, mu->U0);
+    VB_CHECK_LAUNCH(mu->ctx, 1);
+    VB_CHECK_LAUNCH(mu->ctx, fill());
+    vb::k_muscl_prim<<<grid, vb::MB, 0, s>>>(m, F, mu->prim);
+    vb::k_muscl_stage<1><<<grid, vb::MB, 0, s>>>(m, mu->prim, F, mu->U0);
+    VB_CHECK_LAUNCH(mu->ctx, 2);
+    VB_CHECK_LAUNCH(mu->ctx, fill());
+    vb::k_muscl_prim<<<grid, vb::MB, 0, s>>>(m, F, mu->prim);
+    vb::k_muscl_stage<2><<<grid, vb::MB, 0, s>>>(m, mu->prim, F, mu->U0);
+    VB_CHECK_LAUNCH(mu->ctx, 2);
+    return VB_OK;
+}
+
+vb::MusclFields owned(vb_muscl *mu)
+{
+    vb::MusclFields F;
+    for (int f = 0; f < 5; ++f) F.f[f] = mu->U + f * mu->m.N;
+    return F;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vb_muscl_create(vb_ctx *ctx, const int64_t dims[3], int32_t ng, vb_muscl **out)
+{
+    if (!ctx || !dims || !out) return fail(VB_EINVAL, "null argument");
+    *out = nullptr;
+    if (ng < 2) return fail(VB_EINVAL, "ng must be at least 2 (the stencil reaches two cells)");
+    int64_t N = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (dims[a] < 2 * (int64_t)ng + 1) return fail(VB_EINVAL, "each dim needs 2 ng + 1 cells");
+        if (N > INT64_MAX / dims[a]) return fail(VB_EINVAL, "cell count overflows");
+        N *= dims[a];
+    }
+    int rc = use(ctx);
+    if (rc) return rc;
+    vb_muscl *mu = new vb_muscl;
+    mu->ctx = ctx;
+    mu->m.N = N;
+    mu->m.ng = ng;
+    int64_t st = 1;
+    for (int a = 0; a < 3; ++a) {
+        mu->m.n[a] = dims[a];
+        mu->m.stride[a] = st;
+        st *= dims[a];
+    }
+    const size_t bytes = sizeof(double) * 5 * (size_t)N;
+    cudaError_t e = cudaMalloc(&mu->U, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&mu->U0, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&mu->prim, bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(mu->U, 0, bytes, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(mu->U);
+        cudaFree(mu->U0);
+        cudaFree(mu->prim);
+        delete mu;
+        return fail(e == cudaErrorMemoryAllocation ? VB_ENOMEM : VB_ECUDA,
+                    std::string("muscl allocation: ") + cudaGetErrorString(e));
+    }
+    *out = mu;
+    return VB_OK;
+}
+
+int vb_muscl_destroy(vb_muscl *mu)
+{
+    if (!mu) return VB_OK;
+    cudaSetDevice(mu->ctx->device);
+    cudaStreamSynchronize(mu->ctx->stream);
+    cudaFree(mu->U);
+    cudaFree(mu->U0);
+    cudaFree(mu->prim);
+    delete mu;
+    return VB_OK;
+}
+
+int vb_muscl_upload(vb_muscl *mu, const double *U)
+{
+    if (!mu || !U) return fail(VB_EINVAL, "null argument");
+    int rc = use(mu->ctx);
+    if (rc) return rc;
+    VB_CUDA(cudaMemcpyAsync(mu->U, U, sizeof(double) * 5 * mu->m.N, cudaMemcpyHostToDevice,
+                            mu->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(mu->ctx->stream));
+    return VB_OK;
+}
+
+int vb_muscl_download(vb_muscl *mu, double *U)
+{
+    if (!mu || !U) return fail(VB_EINVAL, "null argument");
+    int rc = use(mu->ctx);
+    if (rc) return rc;
+    VB_CUDA(cudaMemcpyAsync(U, mu->U, sizeof(double) * 5 * mu->m.N, cudaMemcpyDeviceToHost,
+                            mu->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(mu->ctx->stream));
+    return VB_OK;
+}
+
+int vb_muscl_state(vb_muscl *mu, double **dU)
+{
+    if (!mu || !dU) return fail(VB_EINVAL, "null argument");
+    *dU = mu->U;
+    return VB_OK;
+}
+
+int vb_muscl_step(vb_muscl *mu, const vb_muscl_params *p)
+{
+    if (!mu) return fail(VB_EINVAL, "null handle");
+    int rc = check_params(p, mu);
+    if (!rc) rc = use(mu->ctx);
+    if (!rc) rc = queue_step(mu, owned(mu), p);
+    if (rc) return rc;
+    VB_CUDA(cudaStreamSynchronize(mu->ctx->stream));
+    return VB_OK;
+}
+
+int vb_muscl_run_async(vb_muscl *mu, const vb_muscl_params *p, int64_t nsteps)
+{
+    if (!mu) return fail(VB_EINVAL, "null handle");
+    if (nsteps < 0) return fail(VB_EINVAL, "nsteps < 0");
+    int rc = check_params(p, mu);
+    if (!rc) rc = use(mu->ctx);
+    for (int64_t k = 0; k < nsteps && !rc; ++k) rc = queue_step(mu, owned(mu), p);
+    return rc;
+}
+
+int vb_muscl_step_fields(vb_muscl *mu, double *D, double *S1, double *S2, double *S3, double *Tau,
+                         const vb_muscl_params *p)
+{
+    if (!mu || !D || !S1 || !S2 || !S3 || !Tau) return fail(VB_EINVAL, "null argument");
+    int rc = check_params(p, mu);
+    if (!rc) rc = use(mu->ctx);
+    if (rc) return rc;
+    vb::MusclFields F;
+    F.f[0] = D;
+    F.f[1] = S1;
+    F.f[2] = S2;
+    F.f[3] = S3;
+    F.f[4] = Tau;
+    rc = queue_step(mu, F, p);
+    if (rc) return rc;
+    VB_CUDA(cudaStreamSynchronize(mu->ctx->stream));
+    return VB_OK;
+}
+
+}  // extern "C"

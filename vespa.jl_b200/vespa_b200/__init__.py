@@ -11,6 +11,7 @@ from .amr import AmrMesh, AmrSimulation, RefinementPolicy
 from .adjoint import Adjoint, EvolveFunction, evolve_with_adjoint, rho2_integral, rho2_seed
 from .flux import AbstractFluxBackend, B200Flux, compute_face_fluxes
 from .gravity import GravityField, apply_laplacian, disable_gravity, enable_gravity, solve_poisson
+from .muscl import MusclGrid, muscl_step_3d
 from .problem import (BC, IdealHydro, Outflow, Periodic, Problem, Reflecting, cons2prim,
                       initial_primitive, initial_state, kelvin_helmholtz_problem, prim2cons,
                       riemann_box_problem, sedov_problem, smooth_random_problem,
@@ -25,6 +26,7 @@ __all__ = [
     "Adjoint", "EvolveFunction", "evolve_with_adjoint", "rho2_integral", "rho2_seed",
     "AbstractFluxBackend", "B200Flux", "compute_face_fluxes",
     "GravityField", "apply_laplacian", "disable_gravity", "enable_gravity", "solve_poisson",
+    "MusclGrid", "muscl_step_3d",
     "BC", "IdealHydro", "Outflow", "Periodic", "Problem", "Reflecting", "cons2prim",
     "initial_primitive", "initial_state", "kelvin_helmholtz_problem", "prim2cons",
     "riemann_box_problem", "sedov_problem", "smooth_random_problem", "sod_problem_defaults",

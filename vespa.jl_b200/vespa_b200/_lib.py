@@ -58,6 +58,19 @@ class GravityDesc(C.Structure):
     ]
 
 
+class MusclParams(C.Structure):
+    """vb_muscl_params"""
+    _fields_ = [
+        ("dt", C.c_double),
+        ("gamma", C.c_double),
+        ("theta", C.c_double),
+        ("dx", C.c_double),
+        ("small_rho", C.c_double),
+        ("bc", C.c_int32),
+        ("flags", C.c_int32),
+    ]
+
+
 # name -> (argtypes); every entry point returns int
 _VP = C.c_void_p
 _DP = C.POINTER(C.c_double)
@@ -113,6 +126,14 @@ SIGNATURES = {
     "vb_gravity_set_phi": [_VP, _DP],
     "vb_gravity_accel": [_VP, _DP],
     "vb_gravity_laplacian": [_VP, _DP, _DP],
+    "vb_muscl_create": [_VP, _I64P, C.c_int32, C.POINTER(_VP)],
+    "vb_muscl_destroy": [_VP],
+    "vb_muscl_upload": [_VP, _DP],
+    "vb_muscl_download": [_VP, _DP],
+    "vb_muscl_state": [_VP, C.POINTER(_VP)],
+    "vb_muscl_step": [_VP, C.POINTER(MusclParams)],
+    "vb_muscl_run_async": [_VP, C.POINTER(MusclParams), C.c_int64],
+    "vb_muscl_step_fields": [_VP, _VP, _VP, _VP, _VP, _VP, C.POINTER(MusclParams)],
     "vb_adjoint_create": [_VP, C.c_int64, C.c_int64, C.POINTER(_VP)],
     "vb_adjoint_destroy": [_VP],
     "vb_adjoint_forward": [_VP, C.c_double, C.c_int64, _DP, _I64P],
