@@ -53,11 +53,14 @@ def parse():
                     help="skip the KH 512^2 adjoint timing and finite-difference check")
     ap.add_argument("--no-gravity", action="store_true",
                     help="skip the 256^3 self-gravity run")
-    ap.add_argument("--workload", choices=["cube", "batch64", "plane", "adjoint", "amr", "gravity"],
+    ap.add_argument("--no-muscl", action="store_true",
+                    help="skip the 256^3 PPMKernels MUSCL run")
+    ap.add_argument("--workload", choices=["cube", "batch64", "plane", "adjoint", "amr", "gravity",
+                                           "muscl"],
                     default="cube",
-                    help="cube: the 256^3 headline line (with the plane, adjoint, AMR and "
-                         "gravity sections); batch64: 64 uneven Riemann boxes in one batch; plane, "
-                         "adjoint, amr, gravity: that section alone")
+                    help="cube: the 256^3 headline line (with the plane, adjoint, AMR, gravity "
+                         "and MUSCL sections); batch64: 64 uneven Riemann boxes in one batch; "
+                         "plane, adjoint, amr, gravity, muscl: that section alone")
     return ap.parse_args()
 
 
@@ -379,6 +382,7 @@ def run_ours(args, ranks: Ranks):
     amr = None if args.no_amr else amr_section(ctx, ranks)
     plane = None if args.no_plane else plane_section(ctx, ranks, K, W)
     gravity = None if args.no_gravity else gravity_section(ctx, ranks, min(K, 20), W)
+    muscl = None if args.no_muscl else muscl_section(ctx, ranks, min(K, 20), W)
 
     cpu = None
     if ranks.world == 1 and ranks.rank == 0 and not args.no_cpu_baseline:
@@ -423,6 +427,8 @@ def run_ours(args, ranks: Ranks):
         line["plane2d"] = plane
     if gravity is not None:
         line["gravity"] = gravity
+    if muscl is not None:
+        line["muscl"] = muscl
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -607,6 +613,60 @@ def gravity_section(ctx, ranks: Ranks, K: int, W: int, n=256, cpu_n=64):
     return out
 
 
+def muscl_section(ctx, ranks: Ranks, K: int, W: int, n=256, ng=3, cpu_n=48):
+    """lib/PPMKernels unsplit MUSCL (muscl_step_3d!, Enzo HydroMethod=3) on an
+    n^3 active region with ng ghost zones per side (periodic fill), the cube's
+    generator for the state, dt from CFL 0.4 of the initial state; K timed
+    steps after W warm-up steps.  Bytes the kernels move per cell and step:
+    copy U -> U0 (80), two primitive passes (160), stage 1 (prim, U0, write
+    U: 120), stage 2 (prim, U0, U, write U: 160) = 520 B.  CPU: the oracle's
+    serial restatement on a cpu_n^3 sample."""
+    import numpy as np
+    import vespa_b200 as vb
+    m = n + 2 * ng
+    dims = (m, m, m)
+    gamma = 5.0 / 3.0
+    prob = vb.smooth_random_problem((m, m, m), seed=vb.problem.DEFAULT_SEED + ranks.rank)
+    W5 = vb.problem.initial_primitive(prob)
+    rho, vel, p = W5[0], W5[1:4], W5[4]
+    etot = p / ((gamma - 1.0) * rho) + 0.5 * (vel ** 2).sum(axis=0)
+    U0 = np.ascontiguousarray(np.array([rho, rho * vel[0], rho * vel[1], rho * vel[2], rho * etot]))
+    cs = np.sqrt(gamma * p / rho)
+    dx = 1.0 / n
+    dt = 0.4 * dx / float(np.max(np.abs(vel).max(axis=0) + cs))
+    g = vb.MusclGrid(dims, ng, ctx=ctx)
+    g.upload(U0)
+    kw = dict(dt=dt, gamma=gamma, dx=dx, bc="periodic")
+    g.run_async(W, **kw)
+    ctx.synchronize()
+    ranks.barrier()
+    ctx.mark(14)
+    g.run_async(K, **kw)
+    ctx.mark(15)
+    ms = ranks.max(ctx.elapsed_ms(14, 15))
+    hbm, _ = measured_hbm()
+    gbs = 520 * m ** 3 / (ms / K / 1e3) / 1e9
+    out = {"config": f"3D {n}^3 active cells + {ng} periodic ghost zones per side, gamma 5/3, "
+                     f"theta 1.5, HLL, fixed dt = CFL 0.4 of the initial state",
+           "value": round(n ** 3 * ranks.world * K / (ms / 1e3) / 1e6, 1), "unit": UNIT,
+           "ms_per_step": round(ms / K, 4), "steps": K,
+           "achieved_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm, 4),
+           "bytes_per_cell_step": 520}
+    g.close()
+    if ranks.rank == 0:
+        from oracle import oracle as O
+        O.build()
+        mc = cpu_n + 2 * ng
+        Uc = np.ascontiguousarray(U0.reshape(5, m, m, m)[:, :mc, :mc, :mc].reshape(5, -1))
+        t0 = time.perf_counter()
+        O.muscl_step((mc, mc, mc), ng, Uc, dt, gamma, 1.5, dx, bc=1)
+        cs_ = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(cpu_n ** 3 / cs_ / 1e6, 3), "unit": UNIT, "cores": 1,
+                               "kind": "port", "sample": f"one step of a {cpu_n}^3 (+ghosts) "
+                                                         f"sample ({cs_:.2f} s), serial C oracle"}
+    return out
+
+
 def amr_section(ctx, ranks: Ranks, cpu_steps=60):
     """2D Sedov blast on the composite AMR mesh: 48^2 base, E = 1 in a 3-cell
     hot spot, reflecting walls, regrid every 4 steps refining above a density
@@ -721,6 +781,9 @@ def run_section(args, ranks: Ranks):
         sec = adjoint_section(ctx, ranks)
         metric, value = ("adjoint step / forward step, KH 512^2 float64",
                          sec["textured"]["adj_step_over_fwd_step"])
+    elif args.workload == "muscl":
+        sec = muscl_section(ctx, ranks, args.steps, args.warmup)
+        metric, value = "Mcell-updates/s 3D 256^3 PPMKernels unsplit MUSCL-HLL RK2 (fp64)", sec["value"]
     elif args.workload == "gravity":
         sec = gravity_section(ctx, ranks, min(args.steps, 20), args.warmup)
         metric, value = ("Mcell-updates/s 3D 256^3 with self-gravity (fp64, multigrid-preconditioned CG)",
@@ -742,7 +805,7 @@ def main():
             run_reference(args, ranks)
         elif args.workload == "batch64":
             run_batch64(args, ranks)
-        elif args.workload in ("plane", "adjoint", "amr", "gravity"):
+        elif args.workload in ("plane", "adjoint", "amr", "gravity", "muscl"):
             run_section(args, ranks)
         else:
             run_ours(args, ranks)
