@@ -9,6 +9,7 @@
 #include "vb_launch.h"
 #include "vb_stage_generic.cuh"
 #include "vb_stage_tiled3d.cuh"
+#include "vb_stage_tiled3d_f64.cuh"
 #include "vb_stage_tiled2d.cuh"
 
 namespace vb {
@@ -169,7 +170,7 @@ int launch_stage_tiled2d_fp64(const BoxDesc *hbox, int nitems, unsigned int *wor
 int launch_stage_tiled3d_fp64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
                               int nitems, unsigned int *work, int stage, cudaStream_t s)
 {
-    return launch_tiled3d<double, 2>(hbox, boxes, item_box, nitems, work, stage, s);
+    return launch_tiled3d_f64<2>(hbox, boxes, item_box, nitems, work, stage, s);
 }
 
 namespace {

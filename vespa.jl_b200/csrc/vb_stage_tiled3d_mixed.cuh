@@ -1,8 +1,8 @@
 // vb_stage_tiled3d_mixed.cuh -- VB_MIXED tiled 3D stage kernel.
 //
-// Same tiling, TMA pipeline and persistent work queue as k_stage_tiled3d
-// (16 x 16 column tiles marching z; see vb_stage_tiled3d.cuh), specialised
-// for float32 reconstruction and Riemann solves with float64 state:
+// 16 x 16 column tiles marching z with a TMA stage pipeline and a persistent
+// work queue (vb_stage_tiled3d.cuh), specialised for float32 reconstruction
+// and Riemann solves with float64 state:
 //   - primitives live in a ring of three float32 planes (k, k+1, k+2) whose
 //     layout puts the x/y halo and, at a non-periodic boundary, mirror ghost
 //     cells beside the interior, so every slope and face formula is the
