@@ -782,11 +782,12 @@ def run_section(args, ranks: Ranks):
         metric, value = ("adjoint step / forward step, KH 512^2 float64",
                          sec["textured"]["adj_step_over_fwd_step"])
     elif args.workload == "muscl":
-        sec = muscl_section(ctx, ranks, args.steps, args.warmup)
-        metric, value = "Mcell-updates/s 3D 256^3 PPMKernels unsplit MUSCL-HLL RK2 (fp64)", sec["value"]
+        sec = muscl_section(ctx, ranks, args.steps, args.warmup, n=args.n)
+        metric, value = (f"Mcell-updates/s 3D {args.n}^3 PPMKernels unsplit MUSCL-HLL RK2 (fp64)",
+                         sec["value"])
     elif args.workload == "gravity":
-        sec = gravity_section(ctx, ranks, min(args.steps, 20), args.warmup)
-        metric, value = ("Mcell-updates/s 3D 256^3 with self-gravity (fp64, multigrid-preconditioned CG)",
+        sec = gravity_section(ctx, ranks, min(args.steps, 20), args.warmup, n=args.n)
+        metric, value = (f"Mcell-updates/s 3D {args.n}^3 with self-gravity (fp64, multigrid-preconditioned CG)",
                          sec["fp64_mg"]["value"])
     else:
         sec = amr_section(ctx, ranks)
