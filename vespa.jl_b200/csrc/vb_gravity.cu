@@ -60,9 +60,11 @@ __device__ __forceinline__ int64_t gnb(const Geom &g, const GravP &P, int64_t li
 }
 
 // Visit this block's cells: rows of x (coordinates derived once per row), rows
-// strided over the GP blocks and x over the block's threads; 1D grids stride
-// cells directly.  A fixed order per thread, so the partial sums are
-// deterministic.
+// strided over the GP blocks and x over the block's threads; a row shorter
+// than half the block is shared with the next rows (thread t takes x = t % n0
+// of row t / n0 of each group of GB / n0 rows), so no thread idles on a short
+// row.  1D grids stride cells directly.  A fixed order per thread, so the
+// partial sums are deterministic.
 template <int ND, typename F>
 __device__ __forceinline__ void for_cells(const Geom &g, F &&f)
 {
@@ -73,9 +75,13 @@ __device__ __forceinline__ void for_cells(const Geom &g, F &&f)
         }
     } else {
         const int64_t n0 = g.n[0], nrow = g.ncell / n0;
-        for (int64_t row = blockIdx.x; row < nrow; row += GP) {
+        const int rpg = n0 >= GB / 2 ? 1 : GB / (int)n0;  // rows per group
+        const int rsub = rpg == 1 ? 0 : (int)threadIdx.x / (int)n0;
+        const int64_t cx0 = rpg == 1 ? threadIdx.x : (int)threadIdx.x - rsub * (int)n0;
+        if (rsub >= rpg) return;
+        for (int64_t row = (int64_t)blockIdx.x * rpg + rsub; row < nrow; row += (int64_t)GP * rpg) {
             const int64_t cy = row % g.n[1], cz = row / g.n[1];
-            for (int64_t cx = threadIdx.x; cx < n0; cx += GB) {
+            for (int64_t cx = cx0; cx < n0; cx += GB) {
                 const int64_t cc[3] = {cx, cy, cz};
                 f(row * n0 + cx, cc);
             }
@@ -114,34 +120,37 @@ __device__ __forceinline__ double lap_row(const Geom &g, const GravP &P, const d
     return s;
 }
 
-// Deterministic block sum of GB values (fixed tree).
-__device__ __forceinline__ double block_sum(double v, double *sh)
+// Deterministic sum over the block's threads (fixed tree: a shuffle tree in
+// each warp, then one over the warp sums), returned to every thread.  `sh`
+// holds at least NW + 1 doubles.
+template <int NTH>
+__device__ __forceinline__ double tree_sum(double v, double *sh)
 {
-    sh[threadIdx.x] = v;
-    __syncthreads();
+    constexpr int NW = NTH / 32;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 #pragma unroll
-    for (int s = GB / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + s];
-        __syncthreads();
-    }
-    const double r = sh[0];
+    for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+    if (l == 0) sh[w] = v;
     __syncthreads();
+    if (w == 0) {
+        double r = l < NW ? sh[l] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r = r + __shfl_down_sync(0xffffffffu, r, o);
+        if (l == 0) sh[NW] = r;
+    }
+    __syncthreads();
+    const double r = sh[NW];
+    __syncthreads();  // sh is free for the next sum
     return r;
 }
+
+__device__ __forceinline__ double block_sum(double v, double *sh) { return tree_sum<GB>(v, sh); }
 
 // Sum of the GP partials part[0..GP) by one block of 1024 threads (fixed tree).
 __device__ __forceinline__ double final_sum(const double *part, double *sh)
 {
     const int t = threadIdx.x;
-    sh[t] = t < GP ? part[t] : 0.0;
-    __syncthreads();
-    for (int s = 512; s > 0; s >>= 1) {
-        if (t < s) sh[t] = sh[t] + sh[t + s];
-        __syncthreads();
-    }
-    const double r = sh[0];
-    __syncthreads();
-    return r;
+    return tree_sum<1024>(t < GP ? part[t] : 0.0, sh);
 }
 
 // partials of sum(x * V) and sum(V) (the volume-weighted mean of a field)

@@ -6,19 +6,24 @@
 // the hydro step of the main path.
 //
 // The reference sweeps the three axes over transposed slabs and adds each
-// axis's flux divergence into one zeroed dU.  Here one thread owns one cell
-// (ghost cells included): it rebuilds the two interface fluxes of each axis
-// along which it is active from the primitives at +-2 cells, and sums
+// axis's flux divergence into one zeroed dU.  Here a CTA owns a 32 x 8 column
+// of cells (ghost cells included) and marches it along z.  The primitives of
+// five z-planes (the current one, its two stencil neighbours each side)
+// sit in a shared-memory ring with a two-cell x/y halo, filled by cp.async one
+// plane ahead.  Each plane, every interface flux the tile needs is evaluated
+// once: the x and y faces into shared memory, the z face in registers, where
+// it becomes the next plane's lower z face.  Each cell then sums
 // dU = ((0 + du_x) + du_y) + du_z exactly as the reference's accumulation
-// reaches that cell (x in place; y and z through zero-filled slabs added over
-// the whole grid).  Every interface flux is evaluated by both of its cells with
-// the same operations, so the result is the reference's.  Compiled with
-// -fmad=false: bit-identical to the oracle's restatement.
+// reaches it (x in place; y and z through zero-filled slabs added over the
+// whole grid).  A flux depends only on its four stencil cells, so evaluating
+// it once instead of twice changes no bit.  Compiled with -fmad=false:
+// bit-identical to the oracle's restatement.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 
 #include "vb_internal.h"
+#include "vb_tma.cuh"
 
 namespace vb {
 namespace {
@@ -110,65 +115,171 @@ __global__ void __launch_bounds__(MB) k_muscl_prim(MusclGeom m, MusclFields U, d
     }
 }
 
-// Flux through the interface between cells a (left) and a + st (right) along
-// `axis`, in the reference's flux-line form (_muscl_hll_kernel!, muscl.jl:
-// 181-215): the left state is cell a's right face, the right state is cell
-// a+st's left face taken as the right face of the reversed stencil.  Velocity
-// roles are cyclic (normal, t1, t2); F comes back in that frame.
-__device__ __forceinline__ void iface_flux(const MusclGeom &m, const double *__restrict__ prim,
-                                           int axis, int64_t a, int64_t st, double F[5])
+// Tile of one CTA: TX x TY cells of one z-plane, one thread per cell column.
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int PW = TX + 4, PH = TY + 4;  // plane window: 2-cell halo in x and y
+constexpr int PF = PW * PH;              // one primitive field of one plane
+constexpr int PS = 5 * PF;               // one ring slot: the five primitive fields
+constexpr int NSLOT = 5;                 // planes k-1 .. k+2 in use, k+3 landing
+constexpr int FXN = (TX + 1) * TY;       // x faces of one plane tile
+constexpr int FYN = TX * (TY + 1);       // y faces of one plane tile
+constexpr size_t TILE_SMEM = sizeof(double) * (NSLOT * PS + 5 * FXN + 5 * FYN);
+
+// HLL flux through one interface from the primitives of its four stencil
+// cells qm1, q0 | q1, q2 (field f of a cell at offset off[f]), in the
+// reference's flux-line form (_muscl_hll_kernel!, muscl.jl:181-215): the left
+// state is q0's right face, the right state is q1's left face taken as the
+// right face of the reversed stencil.  off[] lists (rho, eint, u_normal, t1,
+// t2); F comes back in that frame.
+__device__ __forceinline__ void face_flux(const double *qm1, const double *q0, const double *q1,
+                                          const double *q2, const int off[5], const MusclGeom &m,
+                                          double F[5])
 {
-    const int64_t N = m.N;
-    const int vq[3] = {2 + axis, 2 + (axis + 1) % 3, 2 + (axis + 2) % 3};  // prim rows: 2=vx..4=vz
-    const int row[5] = {0, 1, vq[0], vq[1], vq[2]};
     double L[5], R[5];
 #pragma unroll
     for (int f = 0; f < 5; ++f) {
-        const double *q = prim + (int64_t)row[f] * N;
-        const double qm1 = q[a - st], q0 = q[a], q1 = q[a + st], q2 = q[a + 2 * st];
-        L[f] = plm_pt(qm1, q0, q1, m.theta);
-        R[f] = plm_pt(q2, q1, q0, m.theta);
+        const double a = qm1[off[f]], b = q0[off[f]], c = q1[off[f]], d = q2[off[f]];
+        L[f] = plm_pt(a, b, c, m.theta);
+        R[f] = plm_pt(d, c, b, m.theta);
     }
     L[0] = jmax(L[0], m.small_rho);
     R[0] = jmax(R[0], m.small_rho);
     hll5(L, R, m.gamma, m.gamma - 1.0, F);
 }
 
-// One RK stage over every cell.  STAGE 1: U = U0 + dU; STAGE 2:
-// U = 0.5 (U0 + U + dU) (muscl_grid.jl:350-367).
-template <int STAGE>
-__global__ void __launch_bounds__(MB) k_muscl_stage(MusclGeom m, const double *__restrict__ prim,
-                                                   MusclFields U, const double *__restrict__ U0)
+// cp.async one primitive plane p (with its halo) into a ring slot; cells
+// outside the grid are left unwritten (no face that reads them is evaluated)
+__device__ __forceinline__ void load_plane(const MusclGeom &m, const double *__restrict__ prim,
+                                           double *slot, int64_t x0, int64_t y0, int64_t p)
 {
-    const int64_t N = m.N;
-    for (int64_t i = (int64_t)blockIdx.x * MB + threadIdx.x; i < N; i += (int64_t)gridDim.x * MB) {
-        const int64_t c[3] = {i % m.n[0], (i / m.n[0]) % m.n[1], i / (m.n[0] * m.n[1])};
-        double dU[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-        for (int axis = 0; axis < 3; ++axis) {
-            const bool active = c[axis] >= m.ng && c[axis] < m.n[axis] - m.ng;
-            double du[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // a zero-filled slab entry
-            if (active) {
-                const int64_t st = m.stride[axis];
-                double Flo[5], Fhi[5];
-                iface_flux(m, prim, axis, i - st, st, Flo);
-                iface_flux(m, prim, axis, i, st, Fhi);
-#pragma unroll
-                for (int f = 0; f < 5; ++f) du[f] = -(Fhi[f] - Flo[f]) * m.dtdx;
-            }
-            if (axis == 0 && !active) continue;  // x adds in place over active cells only
-            // momentum rows receiving (normal, t1, t2)
-            const int slot[5] = {0, 1 + axis, 1 + (axis + 1) % 3, 1 + (axis + 2) % 3, 4};
-#pragma unroll
-            for (int f = 0; f < 5; ++f) dU[slot[f]] = dU[slot[f]] + du[f];
-        }
-#pragma unroll
-        for (int f = 0; f < 5; ++f) {
-            const double u0 = U0[f * N + i];
-            if constexpr (STAGE == 1) U.f[f][i] = u0 + dU[f];
-            else U.f[f][i] = 0.5 * (u0 + U.f[f][i] + dU[f]);
-        }
+    if (p < 0 || p >= m.n[2]) return;
+    const int64_t nx = m.n[0], ny = m.n[1], N = m.N;
+    const double *plane = prim + p * nx * ny;
+    for (int e = threadIdx.x; e < PS; e += NT) {
+        const int f = e / PF, rc = e - f * PF, r = rc / PW, c = rc - r * PW;
+        const int64_t x = x0 - 2 + c, y = y0 - 2 + r;
+        if (x >= 0 && x < nx && y >= 0 && y < ny) cp_async8(slot + e, plane + f * N + y * nx + x);
     }
+}
+
+// One RK stage over the cells of one 32 x 8 column, planes [k0, k0 + kz).
+// STAGE 1: U = U0 + dU; STAGE 2: U = 0.5 (U0 + U + dU) (muscl_grid.jl:350-367).
+template <int STAGE>
+__global__ void __launch_bounds__(NT, 2) k_muscl_tile(MusclGeom m, const double *__restrict__ prim,
+                                                      MusclFields U, const double *__restrict__ U0,
+                                                      int kz)
+{
+    extern __shared__ __align__(16) double smem[];
+    double *const ring = smem, *const fx = smem + NSLOT * PS, *const fy = fx + 5 * FXN;
+    const int t = threadIdx.x, tx = t % TX, ty = t / TX;
+    const int64_t nx = m.n[0], ny = m.n[1], nz = m.n[2], ng = m.ng, N = m.N;
+    const int64_t x0 = (int64_t)blockIdx.x * TX, y0 = (int64_t)blockIdx.y * TY;
+    const int64_t k0 = (int64_t)blockIdx.z * kz, k1 = k0 + kz < nz ? k0 + kz : nz;
+    const int64_t x = x0 + tx, y = y0 + ty;
+    const bool in = x < nx && y < ny;
+    const bool act_x = x >= ng && x < nx - ng, act_y = y >= ng && y < ny - ng;
+    // a face between cells c and c + 1 along an axis of n cells is needed iff
+    // one of the two is active; its stencil c - 1 .. c + 2 is then in the grid
+    auto face_ok = [&](int64_t c, int64_t n) { return c >= ng - 1 && c <= n - ng - 1; };
+    auto slot = [&](int64_t p) { return ring + (int)((p + NSLOT) % NSLOT) * PS; };  // p >= -2
+    const int own = (ty + 2) * PW + tx + 2;  // this column's cell in a plane window
+    const int zoff[5] = {0, PF, 4 * PF, 2 * PF, 3 * PF};  // rho, eint, vz | vx, vy
+
+    for (int64_t p = k0 - 2; p <= k0 + 2; ++p) load_plane(m, prim, slot(p), x0, y0, p);
+    cp_async_commit();
+    cp_async_wait_group<0>();
+    __syncthreads();
+    double flo[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // z flux through this cell's lower face
+    if (in && face_ok(k0 - 1, nz))
+        face_flux(slot(k0 - 2) + own, slot(k0 - 1) + own, slot(k0) + own, slot(k0 + 1) + own, zoff,
+                  m, flo);
+    __syncthreads();  // slot of plane k0 - 2 is free
+    if (k0 + 3 <= k1 + 1) load_plane(m, prim, slot(k0 + 3), x0, y0, k0 + 3);
+    cp_async_commit();
+
+    for (int64_t k = k0; k < k1; ++k) {
+        cp_async_wait_group<1>();  // plane k + 2 has landed (k + 3 may be in flight)
+        __syncthreads();
+        const double *const pk = slot(k);
+        double fhi[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        if (in && face_ok(k, nz))
+            face_flux(slot(k - 1) + own, pk + own, slot(k + 1) + own, slot(k + 2) + own, zoff, m,
+                      fhi);
+        // the plane's x faces (33 per row) and y faces (9 per column), spread
+        // over the CTA
+        for (int it = t; it < FXN + FYN; it += NT) {
+            const double *c0;
+            double *out;
+            int st, ostr;
+            bool ok;
+            int off[5] = {0, PF, 2 * PF, 3 * PF, 4 * PF};  // x: vx | vy, vz
+            if (it < FXN) {
+                const int r = it / (TX + 1), j = it - r * (TX + 1);  // face x0-1+j | x0+j
+                ok = face_ok(x0 - 1 + j, nx) && y0 + r < ny;
+                c0 = pk + (r + 2) * PW + j + 1;
+                st = 1;
+                out = fx + it;
+                ostr = FXN;
+            } else {
+                const int i2 = it - FXN, r = i2 / TX, j = i2 - r * TX;  // face y0-1+r | y0+r
+                ok = face_ok(y0 - 1 + r, ny) && x0 + j < nx;
+                c0 = pk + (r + 1) * PW + j + 2;
+                st = PW;
+                out = fy + i2;
+                ostr = FYN;
+                off[2] = 3 * PF;  // y: vy | vz, vx
+                off[3] = 4 * PF;
+                off[4] = 2 * PF;
+            }
+            if (ok) {
+                double F[5];
+                face_flux(c0 - st, c0, c0 + st, c0 + 2 * st, off, m, F);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) out[f * ostr] = F[f];
+            }
+        }
+        __syncthreads();  // faces visible; slot of plane k - 1 is free
+        if (k + 4 <= k1 + 1) load_plane(m, prim, slot(k + 4), x0, y0, k + 4);
+        cp_async_commit();
+
+        if (in) {
+            const bool act_z = k >= ng && k < nz - ng;
+            double dU[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            if (act_x) {  // x adds in place over active cells only; S1 is normal
+                const double *lo = fx + ty * (TX + 1) + tx;
+#pragma unroll
+                for (int f = 0; f < 5; ++f)
+                    dU[f] = dU[f] + -(lo[f * FXN + 1] - lo[f * FXN]) * m.dtdx;
+            }
+            {  // y: a zero-filled slab entry where inactive; (S2, S3, S1) rotated
+                const double *lo = fy + ty * TX + tx;
+                const int slot_y[5] = {0, 2, 3, 1, 4};
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    const double du = act_y ? -(lo[f * FYN + TX] - lo[f * FYN]) * m.dtdx : 0.0;
+                    dU[slot_y[f]] = dU[slot_y[f]] + du;
+                }
+            }
+            {  // z: (S3, S1, S2) rotated
+                const int slot_z[5] = {0, 3, 1, 2, 4};
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    const double du = act_z ? -(fhi[f] - flo[f]) * m.dtdx : 0.0;
+                    dU[slot_z[f]] = dU[slot_z[f]] + du;
+                }
+            }
+            const int64_t i = (k * ny + y) * nx + x;
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                const double u0 = U0[f * N + i];
+                if constexpr (STAGE == 1) U.f[f][i] = u0 + dU[f];
+                else U.f[f][i] = 0.5 * (u0 + U.f[f][i] + dU[f]);
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < 5; ++f) flo[f] = fhi[f];
+    }
+    cp_async_wait_group<0>();  // nothing in flight when the CTA retires
 }
 
 // periodic ghost fill along one axis: a ghost p < ng takes p + active, a ghost
@@ -226,6 +337,24 @@ int check_params(const vb_muscl_params *p, const vb_muscl *mu)
     return VB_OK;
 }
 
+// z-planes per CTA: the fewest waves of 2 CTAs per SM, each wave's length
+// the chunk plus the three-plane prologue (ring fill and the first lower face)
+int choose_kz(int64_t tiles, int64_t nz)
+{
+    int64_t best_kz = nz, best = INT64_MAX;
+    for (int64_t nch = 1; nch <= nz && nch <= 65535; ++nch) {
+        const int64_t kz = (nz + nch - 1) / nch;
+        if ((nz + kz - 1) / kz != nch) continue;
+        const int64_t waves = (tiles * nch + 2 * 148 - 1) / (2 * 148);
+        const int64_t cost = waves * (kz + 3);
+        if (cost < best) {
+            best = cost;
+            best_kz = kz;
+        }
+    }
+    return (int)best_kz;
+}
+
 // one muscl_step_3d! on the five fields
 int queue_step(vb_muscl *mu, const vb::MusclFields &F, const vb_muscl_params *p)
 {
@@ -236,6 +365,9 @@ int queue_step(vb_muscl *mu, const vb::MusclFields &F, const vb_muscl_params *p)
     m.dtdx = p->dt / p->dx;
     m.small_rho = p->small_rho;
     const unsigned grid = (unsigned)std::min<int64_t>((m.N + vb::MB - 1) / vb::MB, 148 * 16);
+    const int64_t gx = (m.n[0] + vb::TX - 1) / vb::TX, gy = (m.n[1] + vb::TY - 1) / vb::TY;
+    const int kz = choose_kz(gx * gy, m.n[2]);
+    const dim3 tgrid((unsigned)gx, (unsigned)gy, (unsigned)((m.n[2] + kz - 1) / kz));
     auto fill = [&]() {
         if (p->bc != VB_MUSCL_BC_PERIODIC) return 0;
         for (int a = 0; a < 3; ++a) vb::k_muscl_fill<<<grid, vb::MB, 0, s>>>(m, F, a);
@@ -245,11 +377,11 @@ int queue_step(vb_muscl *mu, const vb::MusclFields &F, const vb_muscl_params *p)
     VB_CHECK_LAUNCH(mu->ctx, 1);
     VB_CHECK_LAUNCH(mu->ctx, fill());
     vb::k_muscl_prim<<<grid, vb::MB, 0, s>>>(m, F, mu->prim);
-    vb::k_muscl_stage<1><<<grid, vb::MB, 0, s>>>(m, mu->prim, F, mu->U0);
+    vb::k_muscl_tile<1><<<tgrid, vb::NT, vb::TILE_SMEM, s>>>(m, mu->prim, F, mu->U0, kz);
     VB_CHECK_LAUNCH(mu->ctx, 2);
     VB_CHECK_LAUNCH(mu->ctx, fill());
     vb::k_muscl_prim<<<grid, vb::MB, 0, s>>>(m, F, mu->prim);
-    vb::k_muscl_stage<2><<<grid, vb::MB, 0, s>>>(m, mu->prim, F, mu->U0);
+    vb::k_muscl_tile<2><<<tgrid, vb::NT, vb::TILE_SMEM, s>>>(m, mu->prim, F, mu->U0, kz);
     VB_CHECK_LAUNCH(mu->ctx, 2);
     return VB_OK;
 }
@@ -278,6 +410,14 @@ int vb_muscl_create(vb_ctx *ctx, const int64_t dims[3], int32_t ng, vb_muscl **o
     }
     int rc = use(ctx);
     if (rc) return rc;
+    for (cudaError_t e : {cudaFuncSetAttribute(vb::k_muscl_tile<1>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)vb::TILE_SMEM),
+                          cudaFuncSetAttribute(vb::k_muscl_tile<2>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)vb::TILE_SMEM)})
+        if (e != cudaSuccess)
+            return fail(VB_ECUDA, std::string("muscl shared memory: ") + cudaGetErrorString(e));
     vb_muscl *mu = new vb_muscl;
     mu->ctx = ctx;
     mu->m.N = N;

@@ -93,6 +93,12 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// wait until at most N of this thread's committed groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // Fast single-precision helpers for the VB_MIXED Riemann solver.
 __device__ __forceinline__ float rcp_approx(float x)
