@@ -618,9 +618,11 @@ def muscl_section(ctx, ranks: Ranks, K: int, W: int, n=256, ng=3, cpu_n=48):
     n^3 active region with ng ghost zones per side (periodic fill), the cube's
     generator for the state, dt from CFL 0.4 of the initial state; K timed
     steps after W warm-up steps.  Bytes the kernels move per cell and step:
-    copy U -> U0 (80), two primitive passes (160), stage 1 (prim, U0, write
-    U: 120), stage 2 (prim, U0, U, write U: 160) = 520 B.  CPU: the oracle's
-    serial restatement on a cpu_n^3 sample."""
+    first preparation pass (read U, write U0 and the primitives: 120), stage 1
+    (prim, U0, write U: 120), second preparation pass (read U, write the
+    primitives: 80), stage 2 (prim, U0, U, write U: 160) = 480 B (ghost fills
+    add a few percent).  CPU: the oracle's serial restatement on a cpu_n^3
+    sample."""
     import numpy as np
     import vespa_b200 as vb
     m = n + 2 * ng
@@ -645,13 +647,13 @@ def muscl_section(ctx, ranks: Ranks, K: int, W: int, n=256, ng=3, cpu_n=48):
     ctx.mark(15)
     ms = ranks.max(ctx.elapsed_ms(14, 15))
     hbm, _ = measured_hbm()
-    gbs = 520 * m ** 3 / (ms / K / 1e3) / 1e9
+    gbs = 480 * m ** 3 / (ms / K / 1e3) / 1e9
     out = {"config": f"3D {n}^3 active cells + {ng} periodic ghost zones per side, gamma 5/3, "
                      f"theta 1.5, HLL, fixed dt = CFL 0.4 of the initial state",
            "value": round(n ** 3 * ranks.world * K / (ms / 1e3) / 1e6, 1), "unit": UNIT,
            "ms_per_step": round(ms / K, 4), "steps": K,
            "achieved_gbs": round(gbs, 1), "hbm_frac": round(gbs / hbm, 4),
-           "bytes_per_cell_step": 520}
+           "bytes_per_cell_step": 480}
     g.close()
     if ranks.rank == 0:
         from oracle import oracle as O

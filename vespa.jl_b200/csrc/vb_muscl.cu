@@ -54,12 +54,16 @@ __device__ __forceinline__ double jmax(double x, double y)
     return signbit(d) ? y : x;
 }
 
-// _msign / _minmod3 / _plm_pt, muscl.jl:13-26 (Enzo's sign(0) = -1)
-__device__ __forceinline__ double msign(double x) { return x > 0.0 ? 1.0 : -1.0; }
+// _msign / _minmod3 / _plm_pt, muscl.jl:13-26 (Enzo's sign(0) = -1; NaN -> -1)
+// 0.25 (sa + sb) |sa + sc| with signs sa, sb, sc = +-1 (sign(x) = x > 0 ? 1 :
+// -1) is exactly +-1 when the three signs agree, a zero carrying sa's sign
+// when sa = sb != sc, and +0 when sa != sb; multiplying that factor by the
+// smallest magnitude rounds exactly as the reference's product does.
 __device__ __forceinline__ double minmod3(double a, double b, double c)
 {
-    const double sa = msign(a), sb = msign(b), sc = msign(c);
-    return 0.25 * (sa + sb) * fabs(sa + sc) * jmin(fabs(a), jmin(fabs(b), fabs(c)));
+    const bool pa = a > 0.0, pb = b > 0.0, pc = c > 0.0;
+    const double f = pa != pb ? 0.0 : pa != pc ? (pa ? 0.0 : -0.0) : (pa ? 1.0 : -1.0);
+    return f * jmin(fabs(a), jmin(fabs(b), fabs(c)));
 }
 __device__ __forceinline__ double plm_pt(double vm1, double v, double vp1, double th)
 {
@@ -100,19 +104,47 @@ __device__ __forceinline__ void hll5(const double L[5], const double R[5], doubl
     F[4] = hll1(ap, am, FlE, FrE, UlE, UrE);
 }
 
-// _cons2prim_k!, muscl_grid.jl:23-34: prim = (rho, eint, vx, vy, vz), eint
-// floored at small_rho
-__global__ void __launch_bounds__(MB) k_muscl_prim(MusclGeom m, MusclFields U, double *prim)
+// Per stage, before the tile pass, one pass over every cell (block 32 x 8,
+// grid z = planes):
+//  - COPY: U0 = U (the step-start state, ghosts as they were);
+//  - FILL: a ghost takes the value of its periodic image, the cell whose
+//    every ghost coordinate p moved by +-active into the active range (what
+//    the three axis fills x, y, z in turn leave in it; the image is active,
+//    so no thread reads a cell another thread writes);
+//  - primitives of the resulting U (_cons2prim_k!, muscl_grid.jl:23-34):
+//    prim = (rho, eint, vx, vy, vz), eint floored at small_rho.
+template <bool COPY, bool FILL>
+__global__ void __launch_bounds__(MB) k_muscl_prep(MusclGeom m, MusclFields U, double *U0, double *prim)
 {
-    const int64_t N = m.N;
-    for (int64_t i = (int64_t)blockIdx.x * MB + threadIdx.x; i < N; i += (int64_t)gridDim.x * MB) {
-        const double d = U.f[0][i], u = U.f[1][i] / d, v = U.f[2][i] / d, w = U.f[3][i] / d;
-        prim[i] = d;
-        prim[2 * N + i] = u;
-        prim[3 * N + i] = v;
-        prim[4 * N + i] = w;
-        prim[N + i] = jmax(U.f[4][i] / d - 0.5 * (u * u + v * v + w * w), m.small_rho);
+    const int64_t c[3] = {(int64_t)blockIdx.x * 32 + threadIdx.x % 32,
+                          (int64_t)blockIdx.y * 8 + threadIdx.x / 32, (int64_t)blockIdx.z};
+    if (c[0] >= m.n[0] || c[1] >= m.n[1]) return;
+    const int64_t N = m.N, i = c[0] + c[1] * m.stride[1] + c[2] * m.stride[2];
+    int64_t src = i;
+    if constexpr (FILL) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int64_t act = m.n[a] - 2 * m.ng;
+            if (c[a] < m.ng) src += act * m.stride[a];
+            else if (c[a] >= m.ng + act) src -= act * m.stride[a];
+        }
     }
+    double u[5];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) u[f] = U.f[f][src];
+    if constexpr (COPY) {
+#pragma unroll
+        for (int f = 0; f < 5; ++f) U0[f * N + i] = src == i ? u[f] : U.f[f][i];
+    }
+    if (src != i)
+#pragma unroll
+        for (int f = 0; f < 5; ++f) U.f[f][i] = u[f];
+    const double d = u[0], vx = u[1] / d, vy = u[2] / d, vz = u[3] / d;
+    prim[i] = d;
+    prim[2 * N + i] = vx;
+    prim[3 * N + i] = vy;
+    prim[4 * N + i] = vz;
+    prim[N + i] = jmax(u[4] / d - 0.5 * (vx * vx + vy * vy + vz * vz), m.small_rho);
 }
 
 // Tile of one CTA: TX x TY cells of one z-plane, one thread per cell column.
@@ -282,29 +314,6 @@ __global__ void __launch_bounds__(NT, 2) k_muscl_tile(MusclGeom m, const double 
     cp_async_wait_group<0>();  // nothing in flight when the CTA retires
 }
 
-// periodic ghost fill along one axis: a ghost p < ng takes p + active, a ghost
-// p >= ng + active takes p - active (the sources are active along this axis)
-__global__ void __launch_bounds__(MB) k_muscl_fill(MusclGeom m, MusclFields U, int axis)
-{
-    const int64_t N = m.N, na = m.n[axis], act = na - 2 * m.ng, st = m.stride[axis];
-    for (int64_t i = (int64_t)blockIdx.x * MB + threadIdx.x; i < N; i += (int64_t)gridDim.x * MB) {
-        const int64_t p = (i / st) % na;
-        int64_t src = -1;
-        if (p < m.ng) src = i + act * st;
-        else if (p >= m.ng + act) src = i - act * st;
-        if (src >= 0)
-#pragma unroll
-            for (int f = 0; f < 5; ++f) U.f[f][i] = U.f[f][src];
-    }
-}
-
-__global__ void __launch_bounds__(MB) k_muscl_copy(int64_t N, MusclFields U, double *U0)
-{
-    for (int64_t i = (int64_t)blockIdx.x * MB + threadIdx.x; i < N; i += (int64_t)gridDim.x * MB)
-#pragma unroll
-        for (int f = 0; f < 5; ++f) U0[f * N + i] = U.f[f][i];
-}
-
 }  // namespace
 }  // namespace vb
 
@@ -364,23 +373,20 @@ int queue_step(vb_muscl *mu, const vb::MusclFields &F, const vb_muscl_params *p)
     m.theta = p->theta;
     m.dtdx = p->dt / p->dx;
     m.small_rho = p->small_rho;
-    const unsigned grid = (unsigned)std::min<int64_t>((m.N + vb::MB - 1) / vb::MB, 148 * 16);
+    const dim3 pgrid((unsigned)((m.n[0] + 31) / 32), (unsigned)((m.n[1] + 7) / 8), (unsigned)m.n[2]);
     const int64_t gx = (m.n[0] + vb::TX - 1) / vb::TX, gy = (m.n[1] + vb::TY - 1) / vb::TY;
     const int kz = choose_kz(gx * gy, m.n[2]);
     const dim3 tgrid((unsigned)gx, (unsigned)gy, (unsigned)((m.n[2] + kz - 1) / kz));
-    auto fill = [&]() {
-        if (p->bc != VB_MUSCL_BC_PERIODIC) return 0;
-        for (int a = 0; a < 3; ++a) vb::k_muscl_fill<<<grid, vb::MB, 0, s>>>(m, F, a);
-        return 3;
-    };
-    vb::k_muscl_copy<<<grid, vb::MB, 0, s>>>(m.N, F, mu->U0);
-    VB_CHECK_LAUNCH(mu->ctx, 1);
-    VB_CHECK_LAUNCH(mu->ctx, fill());
-    vb::k_muscl_prim<<<grid, vb::MB, 0, s>>>(m, F, mu->prim);
+    if (p->bc == VB_MUSCL_BC_PERIODIC)
+        vb::k_muscl_prep<true, true><<<pgrid, vb::MB, 0, s>>>(m, F, mu->U0, mu->prim);
+    else
+        vb::k_muscl_prep<true, false><<<pgrid, vb::MB, 0, s>>>(m, F, mu->U0, mu->prim);
     vb::k_muscl_tile<1><<<tgrid, vb::NT, vb::TILE_SMEM, s>>>(m, mu->prim, F, mu->U0, kz);
     VB_CHECK_LAUNCH(mu->ctx, 2);
-    VB_CHECK_LAUNCH(mu->ctx, fill());
-    vb::k_muscl_prim<<<grid, vb::MB, 0, s>>>(m, F, mu->prim);
+    if (p->bc == VB_MUSCL_BC_PERIODIC)
+        vb::k_muscl_prep<false, true><<<pgrid, vb::MB, 0, s>>>(m, F, mu->U0, mu->prim);
+    else
+        vb::k_muscl_prep<false, false><<<pgrid, vb::MB, 0, s>>>(m, F, mu->U0, mu->prim);
     vb::k_muscl_tile<2><<<tgrid, vb::NT, vb::TILE_SMEM, s>>>(m, mu->prim, F, mu->U0, kz);
     VB_CHECK_LAUNCH(mu->ctx, 2);
     return VB_OK;
@@ -406,6 +412,8 @@ int vb_muscl_create(vb_ctx *ctx, const int64_t dims[3], int32_t ng, vb_muscl **o
     for (int a = 0; a < 3; ++a) {
         if (dims[a] < 2 * (int64_t)ng + 1) return fail(VB_EINVAL, "each dim needs 2 ng + 1 cells");
         if (N > INT64_MAX / dims[a]) return fail(VB_EINVAL, "cell count overflows");
+        if (dims[a] > (a == 0 ? INT32_MAX : a == 1 ? 8 * 65535 : 65535))
+            return fail(VB_EINVAL, "dims exceed the launch grid (ny <= 524280, nz <= 65535)");
         N *= dims[a];
     }
     int rc = use(ctx);
