@@ -545,8 +545,9 @@ def gravity_section(ctx, ranks: Ranks, K: int, W: int, n=256, cpu_n=64):
     default), whose iterations stream 88 B/cell (matvec r p w Ap, update r phi
     p r Ap w phi r, direction r p w p), and with the multigrid preconditioner
     (precond = :mg, ext/mg_pcg.jl); (b) K evolve! steps with gravity after W
-    warm-up steps (one warm-started solve per step, stages on the cell-centric
-    kernel): both precisions with the preconditioner, float64 with plain CG.
+    warm-up steps (one warm-started solve per step, stages on the tiled
+    kernels with the source): both precisions with the preconditioner, float64
+    with plain CG.
     CPU: the oracle's plain CG on a cpu_n^3 sample of (a), serial."""
     import numpy as np
     import vespa_b200 as vb
@@ -592,7 +593,7 @@ def gravity_section(ctx, ranks: Ranks, K: int, W: int, n=256, cpu_n=64):
         ms = ranks.max(ctx.elapsed_ms(12, 13))
         out[f"{prec}_{pc}"] = {"value": round(n ** 3 * ranks.world * K / (ms / 1e3) / 1e6, 1),
                                "unit": UNIT, "ms_per_step": round(ms / K, 4), "steps": K,
-                               "stages": "cell-centric kernel with the gravity source"}
+                               "stages": f"{sim.kernel} kernel with the gravity source"}
         sim.close()
     if ranks.rank == 0:
         from oracle import oracle as O

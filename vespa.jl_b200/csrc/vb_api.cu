@@ -265,7 +265,8 @@ int sync_box(vb_grid *gr)
 int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout)
 {
     double *bf = gr->bflux_on ? gr->bflux : nullptr;
-    if (gr->tiled && !bf && !gr->grav) {
+    const bool grav = gr->grav != nullptr;  // self-gravity: 3D tiled kernels carry the source
+    if (gr->tiled && !bf && (!grav || gr->g.nd == 3)) {
         int rc = sync_box(gr);
         if (rc) return rc;
         const int64_t items = box_items(gr->g, gr->kz);
@@ -280,9 +281,9 @@ int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout
         }
         int n = gr->precision == VB_MIXED
                     ? vb::launch_stage_tiled3d_mixed(&gr->box, nullptr, nullptr, (int)items, work,
-                                                     st, gr->ctx->stream)
+                                                     st, gr->ctx->stream, grav)
                     : vb::launch_stage_tiled3d_fp64(&gr->box, nullptr, nullptr, (int)items, work,
-                                                    st, gr->ctx->stream);
+                                                    st, gr->ctx->stream, grav);
         VB_CHECK_LAUNCH(gr->ctx, n);
         return VB_OK;
     }

@@ -30,6 +30,7 @@ namespace {
 
 constexpr int GB = 256;  // threads per block
 constexpr int GP = 592;  // blocks (= partial sums) per reduction pass: 4 per SM, fixed
+constexpr int GP_SM = 4;  // the GP blocks fit in one wave only at <= 64 registers a thread
 constexpr int GRAPH_ITERS = 8;
 
 struct GravCtrl {
@@ -79,11 +80,19 @@ __device__ __forceinline__ void for_cells(const Geom &g, F &&f)
         const int rsub = rpg == 1 ? 0 : (int)threadIdx.x / (int)n0;
         const int64_t cx0 = rpg == 1 ? threadIdx.x : (int)threadIdx.x - rsub * (int)n0;
         if (rsub >= rpg) return;
-        for (int64_t row = (int64_t)blockIdx.x * rpg + rsub; row < nrow; row += (int64_t)GP * rpg) {
-            const int64_t cy = row % g.n[1], cz = row / g.n[1];
+        // row = cz * n1 + cy, advanced by `step` rows without a division per row
+        const int64_t n1 = g.n[1], step = (int64_t)GP * rpg, sy = step % n1, sz = step / n1;
+        int64_t row = (int64_t)blockIdx.x * rpg + rsub, cy = row % n1, cz = row / n1;
+        for (; row < nrow; row += step) {
             for (int64_t cx = cx0; cx < n0; cx += GB) {
                 const int64_t cc[3] = {cx, cy, cz};
                 f(row * n0 + cx, cc);
+            }
+            cy += sy;
+            cz += sz;
+            if (cy >= n1) {
+                cy -= n1;
+                ++cz;
             }
         }
     }
@@ -100,6 +109,16 @@ __device__ __forceinline__ double lap_row(const Geom &g, const GravP &P, const d
 {
     const double xc = x[lin];
     double s = 0.0;
+    bool inner = true;  // every neighbour inside the grid: the row lists the lo
+#pragma unroll          // faces z, y, x, then the hi faces x, y, z
+    for (int d = 0; d < ND; ++d) inner = inner && cc[d] >= 1 && cc[d] + 1 < g.n[d];
+    if (inner) {
+#pragma unroll
+        for (int d = ND - 1; d >= 0; --d) s = s + P.coef[d] * (xc - x[lin - g.stride[d]]);
+#pragma unroll
+        for (int d = 0; d < ND; ++d) s = s + P.coef[d] * (xc - x[lin + g.stride[d]]);
+        return s;
+    }
 #pragma unroll
     for (int d = ND - 1; d >= 0; --d) {
         const int64_t nb = gnb(g, P, lin, cc[d], d, false);
@@ -154,7 +173,7 @@ __device__ __forceinline__ double final_sum(const double *part, double *sh)
 }
 
 // partials of sum(x * V) and sum(V) (the volume-weighted mean of a field)
-__global__ void __launch_bounds__(GB) k_meanpart(Geom g, const double *__restrict__ x, double *part)
+__global__ void __launch_bounds__(GB, GP_SM) k_meanpart(Geom g, const double *__restrict__ x, double *part)
 {
     __shared__ double sh[GB];
     double s = 0.0, v = 0.0;
@@ -183,7 +202,7 @@ __global__ void __launch_bounds__(1024) k_mean_final(const double *part, GravCtr
 }
 
 // _rhs_flat_kernel!, src/gravity.jl:215-231: b = -4 pi G (rho - rhobar) V
-__global__ void __launch_bounds__(GB) k_rhs(Geom g, GravP P, const double *__restrict__ U, double *b,
+__global__ void __launch_bounds__(GB, GP_SM) k_rhs(Geom g, GravP P, const double *__restrict__ U, double *b,
                                            const GravCtrl *gc)
 {
     const double rhobar = P.project_mean ? gc->rhobar : 0.0;
@@ -193,7 +212,7 @@ __global__ void __launch_bounds__(GB) k_rhs(Geom g, GravP P, const double *__res
 
 // CG start, src/gravity.jl:272-279: r = b - A phi, p = r; partials of r.r and b.b
 template <int ND>
-__global__ void __launch_bounds__(GB) k_cg_init(Geom g, GravP P, const double *__restrict__ phi,
+__global__ void __launch_bounds__(GB, GP_SM) k_cg_init(Geom g, GravP P, const double *__restrict__ phi,
                                                const double *__restrict__ b, double *r, double *p,
                                                double *part)
 {
@@ -232,7 +251,7 @@ __global__ void __launch_bounds__(1024) k_cg_init_final(const double *part, Grav
 
 // Ap = A p; partials of p.Ap
 template <int ND>
-__global__ void __launch_bounds__(GB) k_cg_matvec(Geom g, GravP P, const double *__restrict__ p,
+__global__ void __launch_bounds__(GB, GP_SM) k_cg_matvec(Geom g, GravP P, const double *__restrict__ p,
                                                  double *Ap, double *part, const GravCtrl *gc)
 {
     __shared__ double sh[GB];
@@ -262,7 +281,7 @@ __global__ void __launch_bounds__(1024) k_cg_alpha(const double *part, GravCtrl 
 }
 
 // phi += alpha p; r -= alpha Ap; partials of r.r
-__global__ void __launch_bounds__(GB) k_cg_update(Geom g, double *phi, const double *__restrict__ p,
+__global__ void __launch_bounds__(GB, GP_SM) k_cg_update(Geom g, double *phi, const double *__restrict__ p,
                                                  double *r, const double *__restrict__ Ap,
                                                  double *part, const GravCtrl *gc)
 {
@@ -299,7 +318,7 @@ __global__ void __launch_bounds__(1024) k_cg_beta(const double *part, GravCtrl *
 }
 
 // p = r + beta p
-__global__ void __launch_bounds__(GB) k_cg_dir(Geom g, double *p, const double *__restrict__ r,
+__global__ void __launch_bounds__(GB, GP_SM) k_cg_dir(Geom g, double *p, const double *__restrict__ r,
                                               const GravCtrl *gc)
 {
     if (gc->done) return;
@@ -308,7 +327,7 @@ __global__ void __launch_bounds__(GB) k_cg_dir(Geom g, double *p, const double *
         p[i] = r[i] + beta * p[i];
 }
 
-__global__ void __launch_bounds__(GB) k_sub_mean(Geom g, double *phi, const GravCtrl *gc)
+__global__ void __launch_bounds__(GB, GP_SM) k_sub_mean(Geom g, double *phi, const GravCtrl *gc)
 {
     const double mu = gc->mu;
     for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < g.ncell; i += (int64_t)GP * GB)
@@ -319,7 +338,7 @@ __global__ void __launch_bounds__(GB) k_sub_mean(Geom g, double *phi, const Grav
 // face distances; across a wall the neighbour value is the cell's own and the
 // distance half a width
 template <int ND>
-__global__ void __launch_bounds__(GB) k_accel(Geom g, GravP P, const double *__restrict__ phi,
+__global__ void __launch_bounds__(GB, GP_SM) k_accel(Geom g, GravP P, const double *__restrict__ phi,
                                              double *gacc)
 {
     for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
@@ -336,7 +355,7 @@ __global__ void __launch_bounds__(GB) k_accel(Geom g, GravP P, const double *__r
 }
 
 template <int ND>
-__global__ void __launch_bounds__(GB) k_lap(Geom g, GravP P, const double *__restrict__ x, double *out)
+__global__ void __launch_bounds__(GB, GP_SM) k_lap(Geom g, GravP P, const double *__restrict__ x, double *out)
 {
     for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) { out[i] = lap_row<ND>(g, P, x, i, cc); });
 }
@@ -356,7 +375,7 @@ constexpr double MG_OMEGA = 0.8;
 
 // diag(A): the row's coefficients summed in the row's order; 1 for an empty row
 template <int ND>
-__global__ void __launch_bounds__(GB) k_diag(Geom g, GravP P, double *diag)
+__global__ void __launch_bounds__(GB, GP_SM) k_diag(Geom g, GravP P, double *diag)
 {
     for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
         double s = 0.0;
@@ -384,7 +403,7 @@ __global__ void __launch_bounds__(GB) k_diag(Geom g, GravP P, double *diag)
 // one damped-Jacobi sweep on A (_matvec! then _csr_jacobi!, mg_pcg.jl:148-150):
 // xout = x + omega (rhs - A x) / diag; xin == nullptr stands for x = 0
 template <int ND>
-__global__ void __launch_bounds__(GB) k_ajac(Geom g, GravP P, const double *__restrict__ xin,
+__global__ void __launch_bounds__(GB, GP_SM) k_ajac(Geom g, GravP P, const double *__restrict__ xin,
                                             const double *__restrict__ rhs,
                                             const double *__restrict__ diag, double *xout,
                                             const GravCtrl *gc)
@@ -400,7 +419,7 @@ __global__ void __launch_bounds__(GB) k_ajac(Geom g, GravP P, const double *__re
 // mr = rhs - A x, and the base-grid right-hand side (0 + mr: the scatter onto
 // a zeroed base grid, one cell per base cell on a uniform mesh)
 template <int ND>
-__global__ void __launch_bounds__(GB) k_aresid(Geom g, GravP P, const double *__restrict__ x,
+__global__ void __launch_bounds__(GB, GP_SM) k_aresid(Geom g, GravP P, const double *__restrict__ x,
                                               const double *__restrict__ rhs, double *mr, double *tb,
                                               const GravCtrl *gc)
 {
@@ -415,23 +434,47 @@ __global__ void __launch_bounds__(GB) k_aresid(Geom g, GravP P, const double *__
 __device__ __forceinline__ int mg_wrap(int a, int n) { return a < 0 ? n - 1 : (a >= n ? 0 : a); }
 
 // _mgk_jacobi! (mg_pcg.jl:21-31): phi = (1 - w) phiold + w (sum_nb + h^2 b) / 6
-__global__ void __launch_bounds__(GB) k_mg_jacobi(int n, double h2, const double *__restrict__ phiold,
+// for cell i of the periodic n^3 level
+__device__ __forceinline__ double mg_jacobi_cell(int n, int i, double h2, const double *phiold,
+                                                 const double *__restrict__ b)
+{
+    const int x = i % n, y = (i / n) % n, z = i / (n * n);
+    const int nn = n * n;
+    const double s = phiold[i - x + mg_wrap(x - 1, n)] + phiold[i - x + mg_wrap(x + 1, n)] +
+                     phiold[i - y * n + mg_wrap(y - 1, n) * n] + phiold[i - y * n + mg_wrap(y + 1, n) * n] +
+                     phiold[i - z * nn + mg_wrap(z - 1, n) * nn] + phiold[i - z * nn + mg_wrap(z + 1, n) * nn];
+    return (1.0 - MG_OMEGA) * phiold[i] + MG_OMEGA * (s + h2 * b[i]) / 6.0;
+}
+
+__global__ void __launch_bounds__(GB, GP_SM) k_mg_jacobi(int n, double h2, const double *__restrict__ phiold,
                                                  const double *__restrict__ b, double *phi,
                                                  const GravCtrl *gc)
 {
     if (gc->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n * n * n) return;
-    const int x = i % n, y = (i / n) % n, z = i / (n * n);
-    const int nn = n * n;
-    const double s = phiold[i - x + mg_wrap(x - 1, n)] + phiold[i - x + mg_wrap(x + 1, n)] +
-                     phiold[i - y * n + mg_wrap(y - 1, n) * n] + phiold[i - y * n + mg_wrap(y + 1, n) * n] +
-                     phiold[i - z * nn + mg_wrap(z - 1, n) * nn] + phiold[i - z * nn + mg_wrap(z + 1, n) * nn];
-    phi[i] = (1.0 - MG_OMEGA) * phiold[i] + MG_OMEGA * (s + h2 * b[i]) / 6.0;
+    phi[i] = mg_jacobi_cell(n, i, h2, phiold, b);
+}
+
+// `sweeps` (even) Jacobi sweeps of a small level in one block, alternating
+// e -> t -> e, with a block barrier between sweeps: the same values as
+// `sweeps` launches of k_mg_jacobi
+__global__ void __launch_bounds__(GB, GP_SM) k_mg_jacobi_block(int n, double h2, int sweeps, double *e,
+                                                       const double *__restrict__ b, double *t,
+                                                       const GravCtrl *gc)
+{
+    if (gc->done) return;
+    const int nc = n * n * n;
+    for (int k = 0; k < sweeps; ++k) {
+        const double *src = (k & 1) ? t : e;
+        double *dst = (k & 1) ? e : t;
+        for (int i = threadIdx.x; i < nc; i += GB) dst[i] = mg_jacobi_cell(n, i, h2, src, b);
+        __syncthreads();
+    }
 }
 
 // _mgk_residual! (33-43): r = b - (6 phi - sum_nb) / h^2
-__global__ void __launch_bounds__(GB) k_mg_residual(int n, double invh2, const double *__restrict__ phi,
+__global__ void __launch_bounds__(GB, GP_SM) k_mg_residual(int n, double invh2, const double *__restrict__ phi,
                                                    const double *__restrict__ b, double *r,
                                                    const GravCtrl *gc)
 {
@@ -447,7 +490,7 @@ __global__ void __launch_bounds__(GB) k_mg_residual(int n, double invh2, const d
 }
 
 // _mgk_restrict! (45-53): coarse = mean of the 8 fine children; coarse e = 0
-__global__ void __launch_bounds__(GB) k_mg_restrict(int nc, const double *__restrict__ rf, double *bc,
+__global__ void __launch_bounds__(GB, GP_SM) k_mg_restrict(int nc, const double *__restrict__ rf, double *bc,
                                                    double *ec, const GravCtrl *gc)
 {
     if (gc->done) return;
@@ -463,7 +506,7 @@ __global__ void __launch_bounds__(GB) k_mg_restrict(int nc, const double *__rest
 
 // _mgk_prolong_add! (55-66): trilinear cell-centred prolongation (weights 3/4,
 // 1/4, periodic) added into the fine level
-__global__ void __launch_bounds__(GB) k_mg_prolong_add(int nc, const double *__restrict__ phic,
+__global__ void __launch_bounds__(GB, GP_SM) k_mg_prolong_add(int nc, const double *__restrict__ phic,
                                                       double *phif, const GravCtrl *gc)
 {
     if (gc->done) return;
@@ -486,7 +529,7 @@ __global__ void __launch_bounds__(GB) k_mg_prolong_add(int nc, const double *__r
     phif[i] = phif[i] + v;
 }
 
-__global__ void __launch_bounds__(GB) k_fill0(int64_t n, double *e, const GravCtrl *gc)
+__global__ void __launch_bounds__(GB, GP_SM) k_fill0(int64_t n, double *e, const GravCtrl *gc)
 {
     if (gc->done) return;
     for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < n; i += (int64_t)gridDim.x * GB)
@@ -494,7 +537,7 @@ __global__ void __launch_bounds__(GB) k_fill0(int64_t n, double *e, const GravCt
 }
 
 // partials of sum(e) over the base grid (the correction's mean)
-__global__ void __launch_bounds__(GB) k_sumpart(int64_t n, const double *__restrict__ e, double *part,
+__global__ void __launch_bounds__(GB, GP_SM) k_sumpart(int64_t n, const double *__restrict__ e, double *part,
                                                const GravCtrl *gc)
 {
     __shared__ double sh[GB];
@@ -514,7 +557,7 @@ __global__ void __launch_bounds__(1024) k_sum_final(const double *part, int64_t 
 }
 
 // z += (e - mean) / Vbase + 0 * mr / diag  (_mgk_gather! with gamma = 0, then x .+= mc)
-__global__ void __launch_bounds__(GB) k_mg_gather_add(int64_t n, const double *__restrict__ e,
+__global__ void __launch_bounds__(GB, GP_SM) k_mg_gather_add(int64_t n, const double *__restrict__ e,
                                                      const double *__restrict__ mr,
                                                      const double *__restrict__ diag, double Vbase,
                                                      double *z, const GravCtrl *gc)
@@ -528,7 +571,7 @@ __global__ void __launch_bounds__(GB) k_mg_gather_add(int64_t n, const double *_
 }
 
 // PCG start after z = M^-1 r: p = z; partials of r.z
-__global__ void __launch_bounds__(GB) k_pcg_start(Geom g, const double *__restrict__ r,
+__global__ void __launch_bounds__(GB, GP_SM) k_pcg_start(Geom g, const double *__restrict__ r,
                                                  const double *__restrict__ z, double *p, double *part)
 {
     __shared__ double sh[GB];
@@ -562,7 +605,7 @@ __global__ void __launch_bounds__(1024) k_pcg_check(const double *part, GravCtrl
 }
 
 // partials of r.z (after the preconditioner)
-__global__ void __launch_bounds__(GB) k_pcg_rz(Geom g, const double *__restrict__ r,
+__global__ void __launch_bounds__(GB, GP_SM) k_pcg_rz(Geom g, const double *__restrict__ r,
                                               const double *__restrict__ z, double *part,
                                               const GravCtrl *gc)
 {
@@ -679,7 +722,15 @@ int queue_precond(vb_grid *gr, vb_gravity *gv)
         vb::k_mg_restrict<<<mg_blocks((int64_t)c.n * c.n * c.n), vb::GB, 0, s>>>(c.n, l.r, c.b, c.e, gv->gc);
         VB_CHECK_LAUNCH(gr->ctx, 2);
     }
-    VB_CHECK_LAUNCH(gr->ctx, jacobi(gv->lev[L - 1], 32));  // coarsest: 2 pre + 30 sweeps
+    {  // coarsest: 2 pre + 30 sweeps, in one block when the level is small
+        const auto &l = gv->lev[L - 1];
+        if ((int64_t)l.n * l.n * l.n <= 16 * vb::GB) {
+            vb::k_mg_jacobi_block<<<1, vb::GB, 0, s>>>(l.n, l.h * l.h, 32, l.e, l.b, l.t, gv->gc);
+            VB_CHECK_LAUNCH(gr->ctx, 1);
+        } else {
+            VB_CHECK_LAUNCH(gr->ctx, jacobi(l, 32));
+        }
+    }
     for (int k = L - 2; k >= 0; --k) {
         const auto &l = gv->lev[k], &c = gv->lev[k + 1];
         vb::k_mg_prolong_add<<<mg_blocks((int64_t)l.n * l.n * l.n), vb::GB, 0, s>>>(c.n, c.e, l.e, gv->gc);
@@ -951,6 +1002,7 @@ int vb_gravity_enable(vb_grid *gr, const vb_gravity_desc *d)
     }
     gr->g.grav_g = gv->gacc;
     gr->g.grav_G = d->G;
+    gr->box_kz = -1;          // the tiled kernels' box descriptor carries the geometry
     gr->invdt_valid = false;  // the free-fall limiter joins the CFL maximum
     return VB_OK;
 }
@@ -966,6 +1018,7 @@ int vb_gravity_disable(vb_grid *gr)
     gr->grav = nullptr;
     gr->g.grav_g = nullptr;
     gr->g.grav_G = 0.0;
+    gr->box_kz = -1;
     gr->invdt_valid = false;
     return VB_OK;
 }

@@ -168,9 +168,9 @@ int launch_stage_tiled2d_fp64(const BoxDesc *hbox, int nitems, unsigned int *wor
 }
 
 int launch_stage_tiled3d_fp64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
-                              int nitems, unsigned int *work, int stage, cudaStream_t s)
+                              int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav)
 {
-    return launch_tiled3d_f64<2>(hbox, boxes, item_box, nitems, work, stage, s);
+    return launch_tiled3d_f64<2>(hbox, boxes, item_box, nitems, work, stage, s, grav);
 }
 
 namespace {

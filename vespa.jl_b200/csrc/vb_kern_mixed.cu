@@ -24,9 +24,9 @@ int launch_generic(const Geom &g, const double *Uin, const double *U0, double *U
 }  // namespace
 
 int launch_stage_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
-                               int nitems, unsigned int *work, int stage, cudaStream_t s)
+                               int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav)
 {
-    return launch_tiled3d_mixed<2>(hbox, boxes, item_box, nitems, work, stage, s);
+    return launch_tiled3d_mixed<2>(hbox, boxes, item_box, nitems, work, stage, s, grav);
 }
 
 int launch_stage_tiled2d_mixed(const BoxDesc *hbox, int nitems, unsigned int *work, int stage,

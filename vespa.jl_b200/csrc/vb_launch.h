@@ -66,8 +66,10 @@ int launch_hllc_faces(int64_t nf, const double *WL, const double *WR, const int3
 // Tiled stage.  hbox (host pointer) set: a single box passed by value; else a
 // device box table `boxes` with `item_box` mapping each global work item to
 // its box.  `work` holds the two stage cursors (reset by the dt kernels).
+// grav: the self-gravity source and free-fall dt term (single boxes only).
 int launch_stage_tiled3d_fp64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
-                              int nitems, unsigned int *work, int stage, cudaStream_t s);
+                              int nitems, unsigned int *work, int stage, cudaStream_t s,
+                              bool grav = false);
 // Tiled 2D stage (single box by value).
 int launch_stage_tiled2d_fp64(const BoxDesc *hbox, int nitems, unsigned int *work, int stage,
                               cudaStream_t s);
@@ -81,7 +83,8 @@ int launch_advance(Ctrl *ctrl, cudaStream_t s);
 
 // vb_kern_mixed.cu
 int launch_stage_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
-                               int nitems, unsigned int *work, int stage, cudaStream_t s);
+                               int nitems, unsigned int *work, int stage, cudaStream_t s,
+                               bool grav = false);
 int launch_stage_mixed(const Geom &g, int stage, const double *Uin, const double *U0,
                        double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s);
 

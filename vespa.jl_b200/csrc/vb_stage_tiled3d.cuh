@@ -77,7 +77,9 @@ __device__ __forceinline__ void prefetch_l1(const void *p)
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
-// compute_dt's per-cell term of a new state, exactly as src/driver.jl:178-185
+// compute_dt's per-cell term of a new state, exactly as src/driver.jl:178-185;
+// GRAV: then the free-fall rate of the cell (src/gravity.jl:439-441)
+template <bool GRAV = false>
 __device__ __forceinline__ double cfl_term_exact(const double un[5], const Geom &g, double m)
 {
     double W[5];
@@ -85,7 +87,9 @@ __device__ __forceinline__ double cfl_term_exact(const double un[5], const Geom 
     const double cs = sound_speed(W, g.gamma);
     m = nan_max(m, (fabs(W[1]) + cs) / g.w[0]);
     m = nan_max(m, (fabs(W[2]) + cs) / g.w[1]);
-    return nan_max(m, (fabs(W[3]) + cs) / g.w[2]);
+    m = nan_max(m, (fabs(W[3]) + cs) / g.w[2]);
+    if constexpr (GRAV) m = nan_max(m, gravity_invdt(g.grav_G, W[0]));
+    return m;
 }
 
 // The same over x and y only (2D grids: compute_dt loops d in 1:N)

@@ -54,7 +54,7 @@ __device__ __forceinline__ void face_states(const double *wk, const int o[4], do
 
 }  // namespace t3d
 
-template <int NS, int STAGE, bool BATCH>
+template <int NS, int STAGE, bool BATCH, bool GRAV = false>
 __global__ void __launch_bounds__(256, 2)
 k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restrict__ boxes,
                     const int *__restrict__ item_box, int nitems, unsigned int *work)
@@ -329,7 +329,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
             double Wn[5];
             consume(q, Wn, 2);
             double cf = 0.0;
-            if constexpr (STAGE == 2) cf = cfl_term_exact(unp, g, invdt);
+            if constexpr (STAGE == 2) cf = cfl_term_exact<GRAV>(unp, g, invdt);
             if (z_early) zsolve(k, w0 + o_c, w1 + o_c, Wn, Fzhi);
             else halo_c2p(q);
             if constexpr (STAGE == 2)
@@ -357,6 +357,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
         double un[5];
         const double *pin = Uin + lin, *p0 = U0 + lin;
         double *po = Uout + lin;
+        double acc[5];  // GRAV: the flux sums, completed by the gravity source
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
             const double gxl = S.gx[f][ty * (TX + 1) + tx];
@@ -382,6 +383,10 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
                 if (cz == LO_AFTER) a -= gzl;
             }
             Fzlo[f] = Fzhi[f];
+            if constexpr (GRAV) {
+                acc[f] = a;
+                continue;
+            }
             if constexpr (STAGE == 1) {
                 un[f] = __ldg(pin) - invV * a;
             } else {
@@ -392,13 +397,25 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
             p0 += g.ncell;
             po += g.ncell;
         }
+        if constexpr (GRAV) {  // the source from the stage state, after the fluxes
+            double u[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) u[f] = __ldg(pin + f * g.ncell);
+            gravity_source<3>(g, lin, u, acc);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                if constexpr (STAGE == 1) un[f] = u[f] - invV * acc[f];
+                else un[f] = 0.5 * p0[f * g.ncell] + 0.5 * (u[f] - invV * acc[f]);
+                po[f * g.ncell] = un[f];
+            }
+        }
         lin += plane_cells;
         if constexpr (STAGE == 2) {
 #pragma unroll
             for (int f = 0; f < 5; ++f) unp[f] = un[f];
         }
     }
-    if constexpr (STAGE == 2) invdt = cfl_term_exact(unp, g, invdt);  // the item's last plane
+    if constexpr (STAGE == 2) invdt = cfl_term_exact<GRAV>(unp, g, invdt);  // the item's last plane
     qb += nplanes;
     if (timed_out && t == 0) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
     if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);  // this box's CFL max
@@ -407,21 +424,28 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
 
 template <int NS>
 int launch_tiled3d_f64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
-                       int nitems, unsigned int *work, int stage, cudaStream_t s)
+                       int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav)
 {
     const size_t smem = sizeof(t3d::Smem<NS>);
-    static int res1 = 0, resb = 0;
+    static int res1 = 0, resb = 0, resg = 0;
     if (!res1) res1 = persistent_blocks(k_stage_tiled3d_f64<NS, 1, false>,
                                         k_stage_tiled3d_f64<NS, 2, false>, smem);
     if (!resb) resb = persistent_blocks(k_stage_tiled3d_f64<NS, 1, true>,
                                         k_stage_tiled3d_f64<NS, 2, true>, smem);
-    const int resident = hbox ? res1 : resb;
+    if (!resg) resg = persistent_blocks(k_stage_tiled3d_f64<NS, 1, false, true>,
+                                        k_stage_tiled3d_f64<NS, 2, false, true>, smem);
+    if (grav && !hbox) return -1;  // gravity: single boxes only
+    const int resident = grav ? resg : hbox ? res1 : resb;
     if (resident <= 0 || nitems <= 0) return -1;
     const unsigned grid = (unsigned)(nitems < resident ? nitems : resident);
     BoxDesc box0;
     if (hbox) box0 = *hbox;
     else std::memset(&box0, 0, sizeof box0);
-    if (hbox && stage == 1)
+    if (grav && stage == 1)
+        k_stage_tiled3d_f64<NS, 1, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (grav)
+        k_stage_tiled3d_f64<NS, 2, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (hbox && stage == 1)
         k_stage_tiled3d_f64<NS, 1, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
     else if (hbox)
         k_stage_tiled3d_f64<NS, 2, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);

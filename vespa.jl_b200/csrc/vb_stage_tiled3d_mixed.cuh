@@ -106,6 +106,20 @@ __device__ __forceinline__ float cfl_term(const double un[5], double gamma, floa
     return (t > m || t != t) ? t : m;
 }
 
+// cfl_term and, GRAV, the cell's free-fall rate (src/gravity.jl:439-441,
+// float64, folded into the float32 maximum)
+template <bool GRAV>
+__device__ __forceinline__ float cfl_mixed(const double un[5], const Geom &g, float gf, float iw0,
+                                           float iw1, float iw2, float m)
+{
+    float r = cfl_term(un, g.gamma, gf, iw0, iw1, iw2, m);
+    if constexpr (GRAV) {
+        const float t = (float)gravity_invdt(g.grav_G, un[0]);
+        r = (t > r || t != t) ? t : r;
+    }
+    return r;
+}
+
 // the same over x and y only (2D grids)
 __device__ __forceinline__ double cfl_term2d(const double un[5], const Geom &g, double m)
 {
@@ -162,7 +176,7 @@ __device__ __forceinline__ void store_pair(double (*gx)[TY * (TX + 1)], double (
 
 }  // namespace t3m
 
-template <int NS, int STAGE, bool BATCH>
+template <int NS, int STAGE, bool BATCH, bool GRAV = false>
 __global__ void __launch_bounds__(256, 2)
 k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__restrict__ boxes,
                       const int *__restrict__ item_box, int nitems, unsigned int *work)
@@ -441,7 +455,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
             float Wn[5];
             consume(q, Wn, 2);
             float cf = 0.f;
-            if constexpr (STAGE == 2) cf = cfl_term(unp, gamma, gf, iw0, iw1, iw2, invdtf);
+            if constexpr (STAGE == 2) cf = cfl_mixed<GRAV>(unp, g, gf, iw0, iw1, iw2, invdtf);
             if (z_early) {
                 zsolve(k, w0 + o_c, w1 + o_c, Wn, Fzhi);
             } else {
@@ -471,6 +485,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         const bool interior = cx == LO_BEFORE && cy == LO_BEFORE && cz == LO_BEFORE;
         double un[5];
         double *po = Uout + lin;
+        double acc[5];  // GRAV: the flux sums, completed by the gravity source
         cp_async_wait_all();  // this thread's own epilogue inputs have landed
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
@@ -500,6 +515,10 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
                 if (cz == LO_AFTER) a -= gz0;
             }
             fzl[f] = Fzhi[f];
+            if constexpr (GRAV) {
+                acc[f] = a;
+                continue;
+            }
             if constexpr (STAGE == 1) {
                 un[f] = __fma_rn(-invV, a, S.ep[0][f][t]);
             } else {
@@ -509,6 +528,18 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
             *po = un[f];
             po += g.ncell;
         }
+        if constexpr (GRAV) {  // the source from the stage state, after the fluxes
+            double u[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) u[f] = S.ep[0][f][t];
+            gravity_source<3>(g, lin, u, acc);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                if constexpr (STAGE == 1) un[f] = __fma_rn(-invV, acc[f], u[f]);
+                else un[f] = __fma_rn(0.5, S.ep[1][f][t], __dmul_rn(0.5, __fma_rn(-invV, acc[f], u[f])));
+                po[f * g.ncell] = un[f];
+            }
+        }
         lin += plane_cells;
         if constexpr (STAGE == 2) {
 #pragma unroll
@@ -516,7 +547,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         }
     }
     if constexpr (STAGE == 2)  // the item's last plane
-        invdt = (double)cfl_term(unp, gamma, gf, iw0, iw1, iw2, invdtf);
+        invdt = (double)cfl_mixed<GRAV>(unp, g, gf, iw0, iw1, iw2, invdtf);
     qb += nplanes;
     if (timed_out && t == 0) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
     if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);  // this box's CFL max
@@ -525,21 +556,28 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
 
 template <int NS>
 int launch_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
-                         int nitems, unsigned int *work, int stage, cudaStream_t s)
+                         int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav)
 {
     const size_t smem = sizeof(t3m::Smem<NS>);
-    static int res1 = 0, resb = 0;
+    static int res1 = 0, resb = 0, resg = 0;
     if (!res1) res1 = persistent_blocks(k_stage_tiled3d_mixed<NS, 1, false>,
                                         k_stage_tiled3d_mixed<NS, 2, false>, smem);
     if (!resb) resb = persistent_blocks(k_stage_tiled3d_mixed<NS, 1, true>,
                                         k_stage_tiled3d_mixed<NS, 2, true>, smem);
-    const int resident = hbox ? res1 : resb;
+    if (!resg) resg = persistent_blocks(k_stage_tiled3d_mixed<NS, 1, false, true>,
+                                        k_stage_tiled3d_mixed<NS, 2, false, true>, smem);
+    if (grav && !hbox) return -1;  // gravity: single boxes only
+    const int resident = grav ? resg : hbox ? res1 : resb;
     if (resident <= 0 || nitems <= 0) return -1;
     const unsigned grid = (unsigned)(nitems < resident ? nitems : resident);
     BoxDesc box0;
     if (hbox) box0 = *hbox;
     else std::memset(&box0, 0, sizeof box0);
-    if (hbox && stage == 1)
+    if (grav && stage == 1)
+        k_stage_tiled3d_mixed<NS, 1, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (grav)
+        k_stage_tiled3d_mixed<NS, 2, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (hbox && stage == 1)
         k_stage_tiled3d_mixed<NS, 1, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
     else if (hbox)
         k_stage_tiled3d_mixed<NS, 2, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
