@@ -561,7 +561,7 @@ def gravity_section(ctx, ranks: Ranks, K: int, W: int, n=256, cpu_n=64):
                      "(a) cold solve of a white-noise density U[0.5, 1.5), tol 1e-8; "
                      "(b) the cube's smooth random state, CFL 0.4, solve per step (tol 1e-8)"}
     hbm, _ = measured_hbm()
-    for pc in ("none", "mg"):
+    for pc in ("mg", "none"):
         sim = vb.Simulation(mesh, prob, precision="fp64", ctx=ctx, initial=Un)
         grav = vb.enable_gravity(sim, G=1.0, tol=1e-8, maxiter=5000, precond=pc)
         vb.solve_poisson(sim, grav)  # warm-up (captures the iteration graph)
