@@ -234,7 +234,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
         if (gl) {
             double gst[5];
             ghost_state<double>(loz, bz_lo, 2, gst);
-            tiled_hllc<double, 3>(gst, loz, gamma, Fzlo);
+            tiled_hllc<3>(gst, loz, gamma, Fzlo);
         } else {
             const bool gll = !perz && k0 - 2 < 0;
             double hzm[5];
@@ -243,7 +243,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
                 const double wl = gll ? ((bz_lo == BC_REFLECTING && f == 3) ? -Wb[f] : Wb[f]) : Wa[f];
                 hzm[f] = face_val(Wb[f], 0.5, limited_slope<double>(wl, Wb[f], Wc[f]));
             }
-            tiled_hllc<double, 3>(hzm, loz, gamma, Fzlo);
+            tiled_hllc<3>(hzm, loz, gamma, Fzlo);
         }
     }
 
@@ -266,7 +266,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
 #pragma unroll
             for (int f = 0; f < 5; ++f) hz1[f] = hz[f];
         }
-        tiled_hllc<double, 3>(hz, zr, gamma, Fzhi);
+        tiled_hllc<3>(hz, zr, gamma, Fzhi);
 #pragma unroll
         for (int f = 0; f < 5; ++f) hz[f] = hz1[f];
     };
@@ -274,11 +274,11 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
     auto xy_faces = [&](const double *w0) {
         double L[5], R[5], F[5];
         face_states(w0, ox, L, R);
-        tiled_hllc<double, 1>(L, R, gamma, F);
+        tiled_hllc<1>(L, R, gamma, F);
 #pragma unroll
         for (int f = 0; f < 5; ++f) S.gx[f][ty * (TX + 1) + tx] = ax * F[f];
         face_states(w0, oy, L, R);
-        tiled_hllc<double, 2>(L, R, gamma, F);
+        tiled_hllc<2>(L, R, gamma, F);
 #pragma unroll
         for (int f = 0; f < 5; ++f) S.gy[f][ty * TX + tx] = ay * F[f];
     };
@@ -289,13 +289,13 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
         if (warp == 7) {
             const int ex[4] = {wrow(TX - 2, j), wrow(TX - 1, j), wxs(TX, j), wxs(TX + 1, j)};
             face_states(w0, ex, L, R);
-            tiled_hllc<double, 1>(L, R, gamma, F);
+            tiled_hllc<1>(L, R, gamma, F);
 #pragma unroll
             for (int f = 0; f < 5; ++f) S.gx[f][j * (TX + 1) + TX] = ax * F[f];
         } else {
             const int ey[4] = {wrow(j, TY - 2), wrow(j, TY - 1), wrow(j, TY), wrow(j, TY + 1)};
             face_states(w0, ey, L, R);
-            tiled_hllc<double, 2>(L, R, gamma, F);
+            tiled_hllc<2>(L, R, gamma, F);
 #pragma unroll
             for (int f = 0; f < 5; ++f) S.gy[f][TY * TX + j] = ay * F[f];
         }
