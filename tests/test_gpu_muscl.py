@@ -58,6 +58,19 @@ def test_step_bit_identical_to_oracle(vb, oracle, case):
     assert_bit_identical(g.state(), U)
 
 
+def test_long_z_chunks_bit_identical_to_oracle(vb, oracle):
+    """A grid large enough for multi-plane z chunks (about 20 planes per CTA,
+    the five-plane ring wrapping several times), periodic ghosts."""
+    dims = (134, 70, 128)
+    U0 = random_state(dims, 4)
+    g = vb.MusclGrid(dims, NG)
+    g.upload(U0)
+    g.step(dt=DT, gamma=GAMMA, theta=THETA, dx=DX, bc="periodic")
+    U = U0.copy()
+    oracle.muscl_step(dims, NG, U, DT, GAMMA, THETA, DX, bc=1)
+    assert_bit_identical(g.state(), U)
+
+
 def test_step_fields_on_caller_arrays_equals_owned_state(vb):
     """vb_muscl_step_fields on five device arrays the caller owns (here torch
     tensors) does what vb_muscl_step does on the handle's own state."""
