@@ -687,6 +687,9 @@ def amr_section(ctx, ranks: Ranks, cpu_steps=60):
     pol = A.RefinementPolicy(0.2, 4, 4)
     out = {"config": "2D Sedov 48^2 base, r0 = 3 cells, gamma 1.4, reflecting, CFL 0.3, "
                      "RefinementPolicy(refine_above=0.2, max_level=4, every=4), t_end = 0.05, float64"}
+    import gc
+    gc.collect()
+    gc.disable()  # the host drives this run: no collector pauses inside it
     sampler = ClockSampler(ranks.local)
     sampler.start()
     for sub in (False, True):
@@ -722,6 +725,7 @@ def amr_section(ctx, ranks: Ranks, cpu_steps=60):
         out["subcycled" if sub else "single_rate"] = entry
         sim.close()
     out["clocks"] = sampler.stop()
+    gc.enable()
     # the oracle on the first cpu_steps steps of the same run (host, 1 thread)
     if ranks.rank == 0:
         from oracle import oracle as O

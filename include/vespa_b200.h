@@ -272,7 +272,9 @@ typedef struct {
     int32_t bc;        /* VB_MUSCL_BC_* */
     int32_t flags;     /* must be 0 */
 } vb_muscl_params;
-/* Scratch for a grid of dims (and an owned state of 5 x N doubles, field-major). */
+/* Scratch for a grid of dims (and an owned state of 5 x N doubles, field-major).
+ * ng >= 2; each dim >= 2 ng + 1; dims[1] <= 524280 and dims[2] <= 65535 (launch
+ * grid); VB_EINVAL otherwise. */
 int vb_muscl_create(vb_ctx *ctx, const int64_t dims[3], int32_t ng, vb_muscl **out);
 int vb_muscl_destroy(vb_muscl *m);
 int vb_muscl_upload(vb_muscl *m, const double *U);
