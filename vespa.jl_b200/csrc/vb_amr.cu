@@ -62,7 +62,8 @@ struct vb_amr {
     int64_t hcap = 0;
     uint64_t *hkey = nullptr;
     int *hval = nullptr;
-    // small device words: [0] error bits, [1] changed, [2] max level, [3] scan total, [4] tags
+    // small device words: [0] error bits, [1] unused, [2] max level, [3] scan total, [4] tags,
+    // [8, 8 + BAL_GROUP) marks changed by each balance pass of a group
     int *word = nullptr, *hword = nullptr;
     vb::Ctrl *ctrl = nullptr, *hctrl = nullptr;
     double *partials = nullptr, *totals = nullptr, *htot = nullptr;
@@ -120,9 +121,12 @@ int alloc_leaf_buffers(vb_amr *a, int64_t c)
     return VB_OK;
 }
 
+constexpr int NWORD = 16;     // device words per mesh (see vb_amr::word)
+constexpr int BAL_GROUP = 4;  // balance passes queued per host read
+
 int sync_words(vb_amr *a)
 {
-    VB_CUDA(cudaMemcpyAsync(a->hword, a->word, sizeof(int) * 8, cudaMemcpyDeviceToHost,
+    VB_CUDA(cudaMemcpyAsync(a->hword, a->word, sizeof(int) * NWORD, cudaMemcpyDeviceToHost,
                             a->ctx->stream));
     VB_CUDA(cudaStreamSynchronize(a->ctx->stream));
     return VB_OK;
@@ -159,7 +163,7 @@ int build_tables(vb_amr *a)
         if (rc) return rc;
         a->hcap = hc;
     }
-    VB_CUDA(cudaMemsetAsync(a->word, 0, sizeof(int) * 8, s));
+    VB_CUDA(cudaMemsetAsync(a->word, 0, sizeof(int) * NWORD, s));
     vb::AmrTopo t = topo(a);
     VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_hash_build(t, a->hkey, a->hval, a->word, s));
     VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_kinds(t, a->kind, a->rep, a->fcnt, s));
@@ -224,24 +228,32 @@ int build_tables(vb_amr *a)
 }
 
 // Refine the leaves marked in a->tag (with 2:1 balance), remap the state and
-// rebuild the tables.
-int refine_marked(vb_amr *a)
+// rebuild the tables.  Balance passes queue in groups of BAL_GROUP, each pass
+// gated on the previous one having changed a mark (the group's first pass on
+// `gate`, the tag count, when given), and the leaf count is queued behind the
+// group: one host read settles both unless the group's last pass still
+// changed marks (then another group runs and the count is redone).
+int refine_marked(vb_amr *a, const int *gate = nullptr, int64_t *ntag = nullptr)
 {
     cudaStream_t s = a->ctx->stream;
     vb::AmrTopo t = topo(a);
-    for (int pass = 0;; ++pass) {
-        if (pass > 2 * vb::AMR_MAX_LEVEL + 4) return fail(VB_ECUDA, "AMR balance did not converge");
-        VB_CUDA(cudaMemsetAsync(a->word + 1, 0, sizeof(int), s));
-        VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_balance(t, a->tag, a->word + 1, s));
+    int *flags = a->word + 8;
+    for (int group = 0;; ++group) {
+        if (group * BAL_GROUP > 2 * vb::AMR_MAX_LEVEL + 4)
+            return fail(VB_ECUDA, "AMR balance did not converge");
+        VB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * BAL_GROUP, s));
+        for (int p = 0; p < BAL_GROUP; ++p) {
+            const int *g = p > 0 ? flags + p - 1 : (group == 0 ? gate : nullptr);
+            VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_balance(t, a->tag, flags + p, g, s));
+        }
+        VB_CUDA(cudaMemsetAsync(a->word + 2, 0, sizeof(int), s));
+        VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_count_children(t, a->tag, a->cnt, a->word + 2, s));
+        VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->cnt, a->n, a->fbase, a->bsum, a->word + 3, s));
         int rc = sync_words(a);
         if (rc) return rc;
-        if (!a->hword[1]) break;
+        if (group == 0 && ntag) *ntag = a->hword[4];
+        if (!a->hword[8 + BAL_GROUP - 1]) break;  // a pass of the group changed nothing
     }
-    VB_CUDA(cudaMemsetAsync(a->word + 2, 0, sizeof(int), s));
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_count_children(t, a->tag, a->cnt, a->word + 2, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->cnt, a->n, a->fbase, a->bsum, a->word + 3, s));
-    int rc = sync_words(a);
-    if (rc) return rc;
     const int64_t n_new = a->hword[3];
     const int maxlev = a->hword[2];
     if (n_new == a->n) return VB_OK;  // nothing refined
@@ -275,7 +287,7 @@ int refine_marked(vb_amr *a)
         a->U = Unew;
         a->lev = lev_new;
         a->cx = cx_new;
-        rc = alloc_leaf_buffers(a, cap_new);
+        const int rc = alloc_leaf_buffers(a, cap_new);
         if (rc) return rc;
     } else {
         // same capacity: emit into the spare buffers and swap
@@ -382,11 +394,9 @@ int regrid(vb_amr *a, double above, int maxl, int64_t *ntag)
     VB_CUDA(cudaMemsetAsync(a->word + 4, 0, sizeof(int), st));
     VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_tag(a->dev, a->U, above, maxl, a->tag, nullptr,
                                                a->word + 4, st));
-    int rc = sync_words(a);
-    if (rc) return rc;
-    if (ntag) *ntag = a->hword[4];
-    if (!a->hword[4]) return VB_OK;
-    return refine_marked(a);
+    // no host read of the tag count: with none tagged the balance passes skip
+    // and the leaf count comes back unchanged
+    return refine_marked(a, a->word + 4, ntag);
 }
 
 }  // namespace
@@ -444,8 +454,8 @@ int vb_amr_create(vb_ctx *ctx, const vb_problem_desc *d, vb_amr **out)
     std::memset(a->hctrl, 0, sizeof(vb::Ctrl));
     a->hctrl->tfinal = INFINITY;
     a->hctrl->step_limit = LLONG_MAX;
-    e = cudaMalloc(&a->word, sizeof(int) * 8);
-    if (e == cudaSuccess) e = cudaMallocHost(&a->hword, sizeof(int) * 8);
+    e = cudaMalloc(&a->word, sizeof(int) * NWORD);
+    if (e == cudaSuccess) e = cudaMallocHost(&a->hword, sizeof(int) * NWORD);
     if (e != cudaSuccess) {
         release(a);
         delete a;

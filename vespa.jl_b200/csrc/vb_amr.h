@@ -61,7 +61,8 @@ struct AmrAreas {
 
 int amr_scan(const int *in, int n, int *out, int *bsum, int *total, cudaStream_t s);
 int launch_amr_hash_build(const AmrTopo &t, uint64_t *keys, int *vals, int *err, cudaStream_t s);
-int launch_amr_balance(const AmrTopo &t, uint8_t *mark, int *changed, cudaStream_t s);
+int launch_amr_balance(const AmrTopo &t, uint8_t *mark, int *changed, const int *gate,
+                       cudaStream_t s);
 int launch_amr_count_children(const AmrTopo &t, const uint8_t *mark, int *cnt, int *maxlev,
                               cudaStream_t s);
 int launch_amr_emit(const AmrTopo &t, const uint8_t *mark, const int *off, int *lev_new,

@@ -123,9 +123,13 @@ __global__ void k_hash_insert(AmrTopo t, uint64_t *keys, int *vals, int *err)
     atomicOr(err, 1);
 }
 
-// refine marks of coarser face neighbours of marked leaves (one pass)
-__global__ void k_balance(AmrTopo t, uint8_t *mark, int *changed)
+// refine marks of coarser face neighbours of marked leaves (one pass); the
+// pass does nothing when `gate` is set and zero (the previous pass changed no
+// mark, or nothing was tagged), so passes queue without a host check between
+// them.  The closure reached is the same whatever the order of the marks.
+__global__ void k_balance(AmrTopo t, uint8_t *mark, int *changed, const int *gate)
 {
+    if (gate && *gate == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= t.n || !mark[i]) return;
     const int l = t.lev[i];
@@ -403,9 +407,10 @@ int launch_amr_hash_build(const AmrTopo &t, uint64_t *keys, int *vals, int *err,
     return 2;
 }
 
-int launch_amr_balance(const AmrTopo &t, uint8_t *mark, int *changed, cudaStream_t s)
+int launch_amr_balance(const AmrTopo &t, uint8_t *mark, int *changed, const int *gate,
+                       cudaStream_t s)
 {
-    k_balance<<<nblk(t.n, 256), 256, 0, s>>>(t, mark, changed);
+    k_balance<<<nblk(t.n, 256), 256, 0, s>>>(t, mark, changed, gate);
     return 1;
 }
 
