@@ -83,6 +83,32 @@ __device__ __forceinline__ void for_cells(const Geom &g, F &&f)
         // row = cz * n1 + cy, advanced by `step` rows without a division per row
         const int64_t n1 = g.n[1], step = (int64_t)GP * rpg, sy = step % n1, sz = step / n1;
         int64_t row = (int64_t)blockIdx.x * rpg + rsub, cy = row % n1, cz = row / n1;
+        if (n0 <= GB) {
+            // one cell per row and thread: two rows per pass, in the same
+            // order, so that the loads of both are in flight together
+            if (cx0 >= n0) return;
+            for (; row + step < nrow; row += 2 * step) {
+                int64_t cy2 = cy + sy, cz2 = cz + sz;
+                if (cy2 >= n1) {
+                    cy2 -= n1;
+                    ++cz2;
+                }
+                const int64_t c1[3] = {cx0, cy, cz}, c2[3] = {cx0, cy2, cz2};
+                f(row * n0 + cx0, c1);
+                f((row + step) * n0 + cx0, c2);
+                cy = cy2 + sy;
+                cz = cz2 + sz;
+                if (cy >= n1) {
+                    cy -= n1;
+                    ++cz;
+                }
+            }
+            if (row < nrow) {
+                const int64_t c1[3] = {cx0, cy, cz};
+                f(row * n0 + cx0, c1);
+            }
+            return;
+        }
         for (; row < nrow; row += step) {
             for (int64_t cx = cx0; cx < n0; cx += GB) {
                 const int64_t cc[3] = {cx, cy, cz};
@@ -252,7 +278,7 @@ __global__ void __launch_bounds__(1024) k_cg_init_final(const double *part, Grav
 // Ap = A p; partials of p.Ap
 template <int ND>
 __global__ void __launch_bounds__(GB, GP_SM) k_cg_matvec(Geom g, GravP P, const double *__restrict__ p,
-                                                 double *Ap, double *part, const GravCtrl *gc)
+                                                 double *__restrict__ Ap, double *part, const GravCtrl *gc)
 {
     __shared__ double sh[GB];
     if (gc->done) return;
@@ -405,7 +431,7 @@ __global__ void __launch_bounds__(GB, GP_SM) k_diag(Geom g, GravP P, double *dia
 template <int ND>
 __global__ void __launch_bounds__(GB, GP_SM) k_ajac(Geom g, GravP P, const double *__restrict__ xin,
                                             const double *__restrict__ rhs,
-                                            const double *__restrict__ diag, double *xout,
+                                            const double *__restrict__ diag, double *__restrict__ xout,
                                             const GravCtrl *gc)
 {
     if (gc->done) return;
@@ -420,8 +446,8 @@ __global__ void __launch_bounds__(GB, GP_SM) k_ajac(Geom g, GravP P, const doubl
 // a zeroed base grid, one cell per base cell on a uniform mesh)
 template <int ND>
 __global__ void __launch_bounds__(GB, GP_SM) k_aresid(Geom g, GravP P, const double *__restrict__ x,
-                                              const double *__restrict__ rhs, double *mr, double *tb,
-                                              const GravCtrl *gc)
+                                              const double *__restrict__ rhs, double *__restrict__ mr,
+                                              double *__restrict__ tb, const GravCtrl *gc)
 {
     if (gc->done) return;
     for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
