@@ -326,6 +326,7 @@ struct vb_muscl {
     double *U = nullptr;     // owned state, 5 x N
     double *U0 = nullptr;    // step-start copy
     double *prim = nullptr;  // primitives of the stage input
+    int kz = 1;              // z-planes per CTA of the tile pass (fixed by dims)
 };
 
 namespace {
@@ -375,7 +376,7 @@ int queue_step(vb_muscl *mu, const vb::MusclFields &F, const vb_muscl_params *p)
     m.small_rho = p->small_rho;
     const dim3 pgrid((unsigned)((m.n[0] + 31) / 32), (unsigned)((m.n[1] + 7) / 8), (unsigned)m.n[2]);
     const int64_t gx = (m.n[0] + vb::TX - 1) / vb::TX, gy = (m.n[1] + vb::TY - 1) / vb::TY;
-    const int kz = choose_kz(gx * gy, m.n[2]);
+    const int kz = mu->kz;
     const dim3 tgrid((unsigned)gx, (unsigned)gy, (unsigned)((m.n[2] + kz - 1) / kz));
     if (p->bc == VB_MUSCL_BC_PERIODIC)
         vb::k_muscl_prep<true, true><<<pgrid, vb::MB, 0, s>>>(m, F, mu->U0, mu->prim);
@@ -436,6 +437,7 @@ int vb_muscl_create(vb_ctx *ctx, const int64_t dims[3], int32_t ng, vb_muscl **o
         mu->m.stride[a] = st;
         st *= dims[a];
     }
+    mu->kz = choose_kz(((dims[0] + vb::TX - 1) / vb::TX) * ((dims[1] + vb::TY - 1) / vb::TY), dims[2]);
     const size_t bytes = sizeof(double) * 5 * (size_t)N;
     cudaError_t e = cudaMalloc(&mu->U, bytes);
     if (e == cudaSuccess) e = cudaMalloc(&mu->U0, bytes);
