@@ -426,35 +426,62 @@ __global__ void __launch_bounds__(GB, GP_SM) k_diag(Geom g, GravP P, double *dia
     });
 }
 
+// (A x)[i] on the periodic n^3 grid of the multigrid preconditioner, in the
+// same CSR row order as lap_row (lo faces of lower cells z, y, x; hi faces
+// x, y, z, a 1-cell axis twice; lo faces wrapped to a higher index x, y, z),
+// with 32-bit indices: the same bits as lap_row<3> on that grid.
+__device__ __forceinline__ double lap_cube(int n, const GravP &P, const double *__restrict__ x, int i)
+{
+    const int c[3] = {i % n, (i / n) % n, i / (n * n)};
+    const int st[3] = {1, n, n * n};
+    const double xc = x[i];
+    double s = 0.0;
+#pragma unroll
+    for (int d = 2; d >= 0; --d)
+        if (c[d] > 0) s = s + P.coef[d] * (xc - x[i - st[d]]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int nb = c[d] < n - 1 ? i + st[d] : i - (n - 1) * st[d];
+        s = s + P.coef[d] * (xc - x[nb]);
+        if (nb == i) s = s + P.coef[d] * (xc - x[nb]);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        if (c[d] == 0 && n > 1) s = s + P.coef[d] * (xc - x[i + (n - 1) * st[d]]);
+    return s;
+}
+
 // one damped-Jacobi sweep on A (_matvec! then _csr_jacobi!, mg_pcg.jl:148-150):
-// xout = x + omega (rhs - A x) / diag; xin == nullptr stands for x = 0
-template <int ND>
-__global__ void __launch_bounds__(GB, GP_SM) k_ajac(Geom g, GravP P, const double *__restrict__ xin,
-                                            const double *__restrict__ rhs,
-                                            const double *__restrict__ diag, double *__restrict__ xout,
-                                            const GravCtrl *gc)
+// xout = x + omega (rhs - A x) / diag, xin == nullptr standing for x = 0; one
+// thread per cell of the periodic cube
+__global__ void __launch_bounds__(GB) k_ajac_cube(int n, GravP P, const double *__restrict__ xin,
+                                                 const double *__restrict__ rhs,
+                                                 const double *__restrict__ diag,
+                                                 double *__restrict__ xout, const GravCtrl *gc)
 {
     if (gc->done) return;
-    for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
-        const double ax = xin ? lap_row<ND>(g, P, xin, i, cc) : 0.0;
-        const double xv = xin ? xin[i] : 0.0;
-        xout[i] = xv + MG_OMEGA * (rhs[i] - ax) / diag[i];
-    });
+    const int i = blockIdx.x * GB + threadIdx.x;
+    if (i >= n * n * n) return;
+    const double ax = xin ? lap_cube(n, P, xin, i) : 0.0;
+    const double xv = xin ? xin[i] : 0.0;
+    xout[i] = xv + MG_OMEGA * (rhs[i] - ax) / diag[i];
 }
 
 // mr = rhs - A x, and the base-grid right-hand side (0 + mr: the scatter onto
-// a zeroed base grid, one cell per base cell on a uniform mesh)
-template <int ND>
-__global__ void __launch_bounds__(GB, GP_SM) k_aresid(Geom g, GravP P, const double *__restrict__ x,
-                                              const double *__restrict__ rhs, double *__restrict__ mr,
-                                              double *__restrict__ tb, const GravCtrl *gc)
+// a zeroed base grid, one base cell per cell on a uniform mesh), whose
+// correction e starts at zero; one thread per cell of the periodic cube
+__global__ void __launch_bounds__(GB) k_aresid_cube(int n, GravP P, const double *__restrict__ x,
+                                                   const double *__restrict__ rhs,
+                                                   double *__restrict__ mr, double *__restrict__ tb,
+                                                   double *__restrict__ te, const GravCtrl *gc)
 {
     if (gc->done) return;
-    for_cells<ND>(g, [&](int64_t i, const int64_t cc[3]) {
-        const double m = rhs[i] - lap_row<ND>(g, P, x, i, cc);
-        mr[i] = m;
-        tb[i] = 0.0 + m;
-    });
+    const int i = blockIdx.x * GB + threadIdx.x;
+    if (i >= n * n * n) return;
+    const double m = rhs[i] - lap_cube(n, P, x, i);
+    mr[i] = m;
+    tb[i] = 0.0 + m;
+    te[i] = 0.0;
 }
 
 __device__ __forceinline__ int mg_wrap(int a, int n) { return a < 0 ? n - 1 : (a >= n ? 0 : a); }
@@ -553,13 +580,6 @@ __global__ void __launch_bounds__(GB, GP_SM) k_mg_prolong_add(int nc, const doub
             for (int c = 0; c < 2; ++c)
                 v = v + w[a] * w[b] * w[c] * phic[ic[a] + nc * (jc[b] + nc * kc[c])];
     phif[i] = phif[i] + v;
-}
-
-__global__ void __launch_bounds__(GB, GP_SM) k_fill0(int64_t n, double *e, const GravCtrl *gc)
-{
-    if (gc->done) return;
-    for (int64_t i = (int64_t)blockIdx.x * GB + threadIdx.x; i < n; i += (int64_t)gridDim.x * GB)
-        e[i] = 0.0;
 }
 
 // partials of sum(e) over the base grid (the correction's mean)
@@ -718,16 +738,17 @@ int queue_precond(vb_grid *gr, vb_gravity *gv)
     cudaStream_t s = gr->ctx->stream;
     const vb::Geom &g = gr->g;
     const vb::GravP &P = gv->P;
+    // the preconditioner runs on periodic cubes only: one thread per cell
+    const int n = (int)g.n[0];
+    const unsigned nb = mg_blocks((int64_t)n * n * n);
     auto ajac = [&](const double *xin, double *xout) {
-        vb::k_ajac<3><<<vb::GP, vb::GB, 0, s>>>(g, P, xin, gv->r, gv->diag, xout, gv->gc);
+        vb::k_ajac_cube<<<nb, vb::GB, 0, s>>>(n, P, xin, gv->r, gv->diag, xout, gv->gc);
         return 1;
     };
     VB_CHECK_LAUNCH(gr->ctx, ajac(nullptr, gv->z2));  // pre-smooth from z = 0
     VB_CHECK_LAUNCH(gr->ctx, ajac(gv->z2, gv->z));
     auto &top = gv->lev[0];
-    vb::k_aresid<3><<<vb::GP, vb::GB, 0, s>>>(g, P, gv->z, gv->r, gv->mr, top.b, gv->gc);
-    VB_CHECK_LAUNCH(gr->ctx, 1);
-    vb::k_fill0<<<vb::GP, vb::GB, 0, s>>>((int64_t)top.n * top.n * top.n, top.e, gv->gc);
+    vb::k_aresid_cube<<<nb, vb::GB, 0, s>>>(n, P, gv->z, gv->r, gv->mr, top.b, top.e, gv->gc);
     VB_CHECK_LAUNCH(gr->ctx, 1);
     // V-cycle: down the levels, then back up
     const int L = (int)gv->lev.size();
