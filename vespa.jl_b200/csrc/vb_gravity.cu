@@ -165,6 +165,32 @@ __device__ __forceinline__ double lap_row(const Geom &g, const GravP &P, const d
     return s;
 }
 
+// (A x)[i] on a periodic n^3 grid (the multigrid preconditioner's, and the CG
+// matvec's when the grid is such a cube), in the
+// same CSR row order as lap_row (lo faces of lower cells z, y, x; hi faces
+// x, y, z, a 1-cell axis twice; lo faces wrapped to a higher index x, y, z),
+// with 32-bit indices: the same bits as lap_row<3> on that grid.
+__device__ __forceinline__ double lap_cube(int n, const GravP &P, const double *__restrict__ x, int i)
+{
+    const int c[3] = {i % n, (i / n) % n, i / (n * n)};
+    const int st[3] = {1, n, n * n};
+    const double xc = x[i];
+    double s = 0.0;
+#pragma unroll
+    for (int d = 2; d >= 0; --d)
+        if (c[d] > 0) s = s + P.coef[d] * (xc - x[i - st[d]]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int nb = c[d] < n - 1 ? i + st[d] : i - (n - 1) * st[d];
+        s = s + P.coef[d] * (xc - x[nb]);
+        if (nb == i) s = s + P.coef[d] * (xc - x[nb]);
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        if (c[d] == 0 && n > 1) s = s + P.coef[d] * (xc - x[i + (n - 1) * st[d]]);
+    return s;
+}
+
 // Deterministic sum over the block's threads (fixed tree: a shuffle tree in
 // each warp, then one over the warp sums), returned to every thread.  `sh`
 // holds at least NW + 1 doubles.
@@ -288,6 +314,39 @@ __global__ void __launch_bounds__(GB, GP_SM) k_cg_matvec(Geom g, GravP P, const 
         Ap[i] = a;
         s = s + p[i] * a;
     });
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// k_cg_matvec on the periodic cube (lap_cube, the same row sums), one thread
+// per cell; each block's p.Ap partial goes to cpart[block]
+__global__ void __launch_bounds__(GB) k_cg_matvec_cube(int n, GravP P, const double *__restrict__ p,
+                                                      double *__restrict__ Ap, double *cpart,
+                                                      const GravCtrl *gc)
+{
+    __shared__ double sh[GB / 32 + 1];
+    if (gc->done) return;
+    const int i = blockIdx.x * GB + threadIdx.x;
+    double s = 0.0;
+    if (i < n * n * n) {
+        const double a = lap_cube(n, P, p, i);
+        Ap[i] = a;
+        s = p[i] * a;
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) cpart[blockIdx.x] = s;
+}
+
+// fold nb block partials into the GP partials the one-block final sums read:
+// block b sums its fixed contiguous range of cpart (a fixed tree)
+__global__ void __launch_bounds__(GB, GP_SM) k_fold_parts(const double *__restrict__ cpart, int nb,
+                                                         double *part, const GravCtrl *gc)
+{
+    __shared__ double sh[GB / 32 + 1];
+    if (gc->done) return;
+    const int per = (nb + GP - 1) / GP, lo = blockIdx.x * per, hi = min(nb, lo + per);
+    double s = 0.0;
+    for (int j = lo + (int)threadIdx.x; j < hi; j += GB) s = s + cpart[j];
     s = block_sum(s, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
@@ -424,31 +483,6 @@ __global__ void __launch_bounds__(GB, GP_SM) k_diag(Geom g, GravP P, double *dia
         }
         diag[i] = s == 0.0 ? 1.0 : s;
     });
-}
-
-// (A x)[i] on the periodic n^3 grid of the multigrid preconditioner, in the
-// same CSR row order as lap_row (lo faces of lower cells z, y, x; hi faces
-// x, y, z, a 1-cell axis twice; lo faces wrapped to a higher index x, y, z),
-// with 32-bit indices: the same bits as lap_row<3> on that grid.
-__device__ __forceinline__ double lap_cube(int n, const GravP &P, const double *__restrict__ x, int i)
-{
-    const int c[3] = {i % n, (i / n) % n, i / (n * n)};
-    const int st[3] = {1, n, n * n};
-    const double xc = x[i];
-    double s = 0.0;
-#pragma unroll
-    for (int d = 2; d >= 0; --d)
-        if (c[d] > 0) s = s + P.coef[d] * (xc - x[i - st[d]]);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const int nb = c[d] < n - 1 ? i + st[d] : i - (n - 1) * st[d];
-        s = s + P.coef[d] * (xc - x[nb]);
-        if (nb == i) s = s + P.coef[d] * (xc - x[nb]);
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-        if (c[d] == 0 && n > 1) s = s + P.coef[d] * (xc - x[i + (n - 1) * st[d]]);
-    return s;
 }
 
 // one damped-Jacobi sweep on A (_matvec! then _csr_jacobi!, mg_pcg.jl:148-150):
@@ -687,6 +721,10 @@ struct vb_gravity {
     vb::GravP P{};
     double *phi = nullptr, *b = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr;
     double *gacc = nullptr, *part = nullptr;
+    // periodic cube (n^3, n <= 1024, phi periodic on every side): the
+    // one-thread-per-cell matvec and its per-block partials
+    int cube_n = 0;
+    double *cpart = nullptr;
     vb::GravCtrl *gc = nullptr;   // device
     vb::GravCtrl *hgc = nullptr;  // pinned host mirror
     cudaGraphExec_t gexec = nullptr;
@@ -714,11 +752,28 @@ namespace {
                  : (kern<3><<<vb::GP, vb::GB, 0, s>>>(__VA_ARGS__), 1))
 
 // One CG iteration (five launches; each returns at once after convergence).
+inline unsigned mg_blocks(int64_t n) { return (unsigned)((n + vb::GB - 1) / vb::GB); }
+
+// Ap = A p and the GP partials of p.Ap; evaluates to the launch count
+int queue_matvec(vb_grid *gr, vb_gravity *gv)
+{
+    cudaStream_t s = gr->ctx->stream;
+    const vb::Geom &g = gr->g;
+    if (gv->cube_n) {
+        const int n = gv->cube_n;
+        const unsigned nb = mg_blocks((int64_t)n * n * n);
+        vb::k_cg_matvec_cube<<<nb, vb::GB, 0, s>>>(n, gv->P, gv->p, gv->Ap, gv->cpart, gv->gc);
+        vb::k_fold_parts<<<vb::GP, vb::GB, 0, s>>>(gv->cpart, (int)nb, gv->part, gv->gc);
+        return 2;
+    }
+    return ND_DISPATCH(g.nd, vb::k_cg_matvec, g, gv->P, gv->p, gv->Ap, gv->part, gv->gc);
+}
+
 int queue_iteration(vb_grid *gr, vb_gravity *gv)
 {
     cudaStream_t s = gr->ctx->stream;
     const vb::Geom &g = gr->g;
-    VB_CHECK_LAUNCH(gr->ctx, ND_DISPATCH(g.nd, vb::k_cg_matvec, g, gv->P, gv->p, gv->Ap, gv->part, gv->gc));
+    VB_CHECK_LAUNCH(gr->ctx, queue_matvec(gr, gv));
     vb::k_cg_alpha<<<1, 1024, 0, s>>>(gv->part, gv->gc);
     VB_CHECK_LAUNCH(gr->ctx, 1);
     vb::k_cg_update<<<vb::GP, vb::GB, 0, s>>>(g, gv->phi, gv->p, gv->r, gv->Ap, gv->part, gv->gc);
@@ -729,8 +784,6 @@ int queue_iteration(vb_grid *gr, vb_gravity *gv)
     VB_CHECK_LAUNCH(gr->ctx, 1);
     return VB_OK;
 }
-
-inline unsigned mg_blocks(int64_t n) { return (unsigned)((n + vb::GB - 1) / vb::GB); }
 
 // z = M^-1 r (one composite-smoothed two-level cycle)
 int queue_precond(vb_grid *gr, vb_gravity *gv)
@@ -799,7 +852,7 @@ int queue_pcg_iteration(vb_grid *gr, vb_gravity *gv)
 {
     cudaStream_t s = gr->ctx->stream;
     const vb::Geom &g = gr->g;
-    vb::k_cg_matvec<3><<<vb::GP, vb::GB, 0, s>>>(g, gv->P, gv->p, gv->Ap, gv->part, gv->gc);
+    VB_CHECK_LAUNCH(gr->ctx, queue_matvec(gr, gv));
     vb::k_cg_alpha<<<1, 1024, 0, s>>>(gv->part, gv->gc);
     vb::k_cg_update<<<vb::GP, vb::GB, 0, s>>>(g, gv->phi, gv->p, gv->r, gv->Ap, gv->part, gv->gc);
     vb::k_pcg_check<<<1, 1024, 0, s>>>(gv->part, gv->gc);
@@ -859,6 +912,7 @@ void free_gravity(vb_gravity *gv)
     cudaFree(gv->Ap);
     cudaFree(gv->gacc);
     cudaFree(gv->part);
+    cudaFree(gv->cpart);
     cudaFree(gv->gc);
     cudaFreeHost(gv->hgc);
     cudaFree(gv->z);
@@ -1006,6 +1060,20 @@ int vb_gravity_enable(vb_grid *gr, const vb_gravity_desc *d)
         std::memset(gv->hgc, 0, sizeof(vb::GravCtrl));
     }
     gv->P = P;
+    {
+        bool cube = g.nd == 3 && g.n[0] == g.n[1] && g.n[1] == g.n[2] && g.n[0] <= 1024;
+        for (int a = 0; a < 3; ++a) cube = cube && P.per_lo[a] && P.per_hi[a];
+        gv->cube_n = cube ? (int)g.n[0] : 0;
+        if (cube && !gv->cpart) {
+            const cudaError_t e = cudaMalloc(&gv->cpart, sizeof(double) * mg_blocks(g.ncell));
+            if (e != cudaSuccess) {
+                gv->cube_n = 0;
+                if (!gr->grav) free_gravity(gv);
+                return fail(e == cudaErrorMemoryAllocation ? VB_ENOMEM : VB_ECUDA,
+                            std::string("gravity allocation: ") + cudaGetErrorString(e));
+            }
+        }
+    }
     gv->maxiter = d->maxiter;
     gv->tol = d->tol;
     gr->grav = gv;
