@@ -115,3 +115,21 @@ def test_compute_face_fluxes_rejects_other_backends():
     F = np.zeros((2, 5))
     with pytest.raises(TypeError):
         vb.compute_face_fluxes(object(), 1.4, F, F.copy(), F.copy(), [1, 2])
+
+
+def test_bench_reference_arm_prints_the_contract_line():
+    """bench.py --impl reference (the oracle on the host cores) runs without a
+    GPU and prints one JSON line with the reference arm's keys."""
+    import json
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1",
+                          "--warmup", "0"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
+    assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] in ("port", "reference") and d["cpu_baseline"]["cores"] >= 1
+    assert d["unit"] == "Mcell-updates/s" and d["steps"] == 1
