@@ -212,7 +212,7 @@ int make_geom(const vb_problem_desc *d, vb::Geom *out)
 
 // Box-table entry of a tiled grid (host side).
 vb::BoxDesc make_box(const vb::TiledMaps &mU, const vb::TiledMaps &mU1, const vb::Geom &g,
-                     double *U, double *U1, vb::Ctrl *ctrl, int kz, int item0)
+                     double *U, double *U1, vb::Ctrl *ctrl, int kz, int item0, bool taper)
 {
     vb::BoxDesc b;
     std::memset(&b, 0, sizeof b);
@@ -233,15 +233,17 @@ vb::BoxDesc make_box(const vb::TiledMaps &mU, const vb::TiledMaps &mU1, const vb
     } else {
         b.ntx = (int)(g.n[0] / 16);
         b.ntiles = (int)((g.n[0] / 16) * (g.n[1] / 16));
+        b.nch = vb::chunk_count((int)g.n[2], kz, taper, &b.nchu);
     }
     b.item0 = item0;
     return b;
 }
 
-int64_t box_items(const vb::Geom &g, int kz)
+int64_t box_items(const vb::Geom &g, int kz, bool taper)
 {
     if (g.nd == 2) return (g.n[0] / 256) * ((g.n[1] + kz - 1) / kz);
-    return (g.n[0] / 16) * (g.n[1] / 16) * ((g.n[2] + kz - 1) / kz);
+    int nchu = 0;
+    return (g.n[0] / 16) * (g.n[1] / 16) * vb::chunk_count((int)g.n[2], kz, taper, &nchu);
 }
 
 }  // namespace detail
@@ -257,7 +259,8 @@ using vb::detail::make_box;
 int sync_box(vb_grid *gr)
 {
     if (gr->box_kz == gr->kz) return VB_OK;
-    gr->box = make_box(gr->maps_U, gr->maps_U1, gr->g, gr->U, gr->U1, gr->ctrl, gr->kz, 0);
+    gr->box = make_box(gr->maps_U, gr->maps_U1, gr->g, gr->U, gr->U1, gr->ctrl, gr->kz, 0,
+                       gr->precision == VB_MIXED);
     gr->box_kz = gr->kz;
     return VB_OK;
 }
@@ -269,7 +272,7 @@ int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout
     if (gr->tiled && !bf && (!grav || gr->g.nd == 3)) {
         int rc = sync_box(gr);
         if (rc) return rc;
-        const int64_t items = box_items(gr->g, gr->kz);
+        const int64_t items = box_items(gr->g, gr->kz, gr->precision == VB_MIXED);
         if (items > 0x7fffffff) return fail(VB_ENOTSUP, "too many tiled work items");
         unsigned int *work = gr->ctrl->work;  // device address of the cursors
         if (gr->g.nd == 2) {

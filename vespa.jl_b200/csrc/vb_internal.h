@@ -59,8 +59,8 @@ int make_geom(const vb_problem_desc *d, Geom *g);
 int encode_maps(TiledMaps *m, const double *base, const Geom &g);
 // box-table entry and item count of a tiled grid
 BoxDesc make_box(const TiledMaps &mU, const TiledMaps &mU1, const Geom &g, double *U, double *U1,
-                 Ctrl *ctrl, int kz, int item0);
-int64_t box_items(const Geom &g, int kz);
+                 Ctrl *ctrl, int kz, int item0, bool taper = false);
+int64_t box_items(const Geom &g, int kz, bool taper = false);
 // default z-chunk of a tiled box (batches)
 int default_kz(const Geom &g);
 // automatic kernel choice and default chunk of a single grid

@@ -117,8 +117,8 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
     const int local = item - B.item0;
     const int tile = local % ntiles;
     const int x0 = (tile % ntx) * TX, y0 = (tile / ntx) * TY;
-    const int k0 = (local / ntiles) * kz;
-    const int k1 = min(nz, k0 + kz);
+    int k0, k1;
+    chunk_span(nz, kz, B.nchu, local / ntiles, k0, k1);
     const int nplanes = (k1 - k0) + 4;
     const bool xlo_bnd = !perx && x0 == 0, xhi_bnd = !perx && x0 + TX == nx;
     const bool ylo_bnd = !pery && y0 == 0, yhi_bnd = !pery && y0 + TY == ny;
