@@ -109,9 +109,11 @@ int vb_hllc_faces_device_async(vb_ctx *ctx, int64_t nf, const double *dWL, const
  * GPU that loads the library holds that array (about 7.75 MiB) until exit.
  * Runs on the calling thread's current device and `stream` (a cudaStream_t,
  * NULL for the default stream) and returns after the results are in F.
- * The first call on a device looks up the array's device address; make that
- * call before any stream capture.  All calls share the array: calls whose
- * work overlaps on the GPU race and must be serialised by the caller. */
+ * The first call on a device looks up the array's device address in the
+ * current context (again whenever a later call finds another context current,
+ * e.g. after cudaDeviceReset); make that first call before any stream capture.
+ * All calls share the array: calls whose work overlaps on the GPU race and
+ * must be serialised by the caller. */
 #define VB_NOALLOC_MAX_FACES 65536
 int vb_hllc_faces_noalloc(int64_t nf, const double *WL, const double *WR, const int32_t *axis,
                           double gamma, double *F, void *stream);

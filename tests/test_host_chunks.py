@@ -2,8 +2,9 @@
 vespa.jl_b200/csrc/vb_launch.h), checked on the host: compiled by nvcc as
 host code and run without a GPU.  Every (nz, kz) must give contiguous chunks
 covering [0, nz) exactly once, none longer than kz; the uniform form must be
-the plain ceil(nz / kz) chunks; the tapered form must end on a piece of at
-most 8 planes."""
+the plain ceil(nz / kz) chunks; with kz >= 16 the tapered form's tail pieces
+must have at least 8 planes (all of nz when nz < 8) and its last piece fewer
+than 16."""
 import os
 import shutil
 import subprocess
@@ -34,6 +35,11 @@ int main()
                         std::printf("BAD %d %d %d chunk %d [%d, %d)\n", nz, kz, taper, c, k0, k1);
                         return 1;
                     }
+                    const int minp = nz < 8 ? nz : 8;
+                    if (taper && kz >= 16 && c >= nchu && k1 - k0 < minp) {
+                        std::printf("BAD short tail piece %d %d chunk %d: %d\n", nz, kz, c, k1 - k0);
+                        return 1;
+                    }
                     prev = k1;
                     last = k1 - k0;
                 }
@@ -45,7 +51,7 @@ int main()
                     std::printf("BAD uniform count %d %d: %d\n", nz, kz, n);
                     return 1;
                 }
-                if (taper && last > 8) {
+                if (taper && kz >= 16 && last >= 16) {
                     std::printf("BAD taper end %d %d: %d\n", nz, kz, last);
                     return 1;
                 }

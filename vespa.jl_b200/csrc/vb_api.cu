@@ -656,6 +656,12 @@ int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
         gr->kz = kz;
         rc = ensure_cfl(gr);
         if (!rc) rc = queue_steps(gr, 1);  // warm-up
+        // capture this chunk's step graph before the timed region, so that
+        // only graph replays are timed (capture and instantiation are host
+        // work that would leave the stream idle between the events)
+        if (!rc && nsteps >= GRAPH_STEPS && !gr->grav &&
+            (!gr->gexec || gr->gkey != graph_key(gr)))
+            rc = capture_steps(gr);
         if (rc) break;
         cudaEventRecord(e0, s);
         rc = queue_steps(gr, nsteps);

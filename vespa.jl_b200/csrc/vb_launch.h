@@ -37,13 +37,15 @@ struct alignas(64) BoxDesc {
 // z chunks of a 3D box, in queue order: nchu chunks of kz planes (the last
 // one cut at nz), then, in the tapered form, the remaining planes (between kz
 // and 2 kz of them, or all nz when nz <= 2 kz) in halving pieces of at most kz
-// and at least 8 planes, so that the work queue ends on short items and the
-// blocks finish together.  The tapered form is used by single VB_MIXED grids
-// (measured 2 % faster at 256^3); the float64 and batch launches keep the
-// uniform chunks.
+// planes: a remainder of 16 planes or more gives up half of itself (rounded
+// down), a smaller one is taken whole.  With kz >= 16 every piece then has 8
+// to kz planes and the last one fewer than 16, so that the work queue ends on
+// short items and the blocks finish together.  The tapered form is used by
+// single VB_MIXED grids (measured 2 % faster at 256^3); the float64 and batch
+// launches keep the uniform chunks.
 __host__ __device__ inline int chunk_tail_piece(int r, int kz)
 {
-    const int p = r > 8 ? (r + 1) / 2 : r;
+    const int p = r >= 16 ? r / 2 : r;
     return p < kz ? p : kz;
 }
 __host__ __device__ inline void chunk_span(int nz, int kz, int nchu, int c, int &k0, int &k1)

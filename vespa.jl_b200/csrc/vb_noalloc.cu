@@ -17,10 +17,15 @@
 // once) race on the array and must be serialised by the caller.
 //
 // In host code the array's name is only a host-side stand-in, not a device
-// address, so the device address is looked up with cudaGetSymbolAddress, once
-// per device with that device current, on the first call made on that device.
-// That first call should come before any stream capture.
-#include <atomic>
+// address, so the device address is looked up with cudaGetSymbolAddress, with
+// the device current, on the first call made on that device.  The address
+// belongs to the device's current CUDA context (the module holding the array
+// is loaded per context), so it is cached together with that context's
+// process-unique id (cuCtxGetId) and looked up again when a call finds a
+// different context current: after cudaDeviceReset, or under a caller's own
+// context.  That first call on a device (or in a new context) should come
+// before any stream capture.
+#include <mutex>
 #include <string>
 
 #include "../../include/vespa_b200.h"
@@ -37,7 +42,41 @@ constexpr size_t kScratchBytes = 3 * kStateBytes + kAxisBytes;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
-std::atomic<void *> g_scratch_addr[kMaxDevices];
+// per device: the array's address and the id of the context it belongs to
+// (ctx_id 0 = not looked up yet)
+struct ScratchSlot {
+    void *addr = nullptr;
+    unsigned long long ctx_id = 0;
+};
+ScratchSlot g_scratch[kMaxDevices];
+std::mutex g_scratch_mu;
+
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry-point
+// lookup (the library does not link libcuda directly)
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext *);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long *);
+
+// id of the calling thread's current context; false when none is current
+bool current_context_id(unsigned long long *id)
+{
+    static PfnCtxGetCurrent get_current = nullptr;
+    static PfnCtxGetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess && a &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess && b) {
+            get_current = (PfnCtxGetCurrent)a;
+            get_id = (PfnCtxGetId)b;
+        }
+    });
+    if (!get_current || !get_id) return false;
+    CUcontext c = nullptr;
+    return get_current(&c) == CUDA_SUCCESS && c && get_id(c, id) == CUDA_SUCCESS && *id != 0;
+}
 
 int fail(int code, const std::string &msg)
 {
@@ -66,13 +105,25 @@ extern "C" int vb_hllc_faces_noalloc(int64_t nf, const double *WL, const double 
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(VB_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return fail(VB_ENOTSUP, "device ordinal above 63");
-    // once per device, with that device current: the array's device address
-    void *base = g_scratch_addr[dev].load(std::memory_order_acquire);
-    if (!base) {
-        e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
-        if (e != cudaSuccess || !base)
-            return fail(VB_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch_addr[dev].store(base, std::memory_order_release);
+    // once per device and context, with that device current: the array's
+    // device address.  With no context current yet on this thread, the lookup
+    // itself binds the device's primary context.
+    void *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_mu);
+        ScratchSlot &slot = g_scratch[dev];
+        unsigned long long ctx_id = 0;
+        if (current_context_id(&ctx_id) && slot.addr && slot.ctx_id == ctx_id) {
+            base = slot.addr;
+        } else {
+            e = cudaGetSymbolAddress(&base, g_noalloc_scratch);
+            if (e != cudaSuccess || !base)
+                return fail(VB_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            if (!current_context_id(&ctx_id))
+                return fail(VB_ECUDA, "cuCtxGetCurrent/cuCtxGetId: no current context");
+            slot.addr = base;
+            slot.ctx_id = ctx_id;
+        }
     }
 
     cudaStream_t s = (cudaStream_t)stream;
