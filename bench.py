@@ -33,6 +33,14 @@ METRIC = ("Mcell-updates/s 3D 256³ PLM+HLLC RK2 (fp64 vs fp32/fp64 split); %HBM
 UNIT = "Mcell-updates/s"
 FALLBACK_HBM_GBS = 6650.0
 BYTES_PER_CELL_STAGE = {1: 80, 2: 120}  # 5 float64 fields: stage 1 R(U)+W(U1), stage 2 R(U1)+R(U)+W(U)
+
+
+def workload(n: int) -> str:
+    """The headline workload's name, printed identically by both arms."""
+    return (f"3D {n}^3 periodic PLM/minmod+HLLC SSP-RK2, gamma 5/3, CFL 0.4, "
+            "dt recomputed each step")
+
+
 DATA = ("synthetic: seeded smooth random periodic state (rho = 1 + 0.3 x mean of 8 random sine "
         "modes, velocity components uniform in [-0.5, 0.5], p = 1 + 0.2 U[-1, 1]); no dataset")
 
@@ -53,6 +61,8 @@ def parse():
                     help="skip the KH 512^2 adjoint timing and finite-difference check")
     ap.add_argument("--no-gravity", action="store_true",
                     help="skip the 256^3 self-gravity run")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the 64-box batch run")
     ap.add_argument("--no-muscl", action="store_true",
                     help="skip the 256^3 PPMKernels MUSCL run")
     ap.add_argument("--workload", choices=["cube", "batch64", "plane", "adjoint", "amr", "gravity",
@@ -290,8 +300,9 @@ def run_reference(args, ranks: Ranks):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(el / args.steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
-        "config": {"workload": f"3D periodic PLM/minmod+HLLC SSP-RK2, {n}^3 sample per step of the "
-                               f"256^3 workload (CPU-bounded), CFL 0.4, gamma 5/3",
+        "config": {"workload": workload(args.n),
+                   "sample": f"each timed step advances a {n}^3 box of the same generator "
+                             f"(CPU-bounded sample of the {args.n}^3 workload)",
                    "cells_per_step": n ** 3, "parallelism": f"{nthreads} host threads"},
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": nthreads,
                          "kind": "port",
@@ -372,14 +383,21 @@ def run_ours(args, ranks: Ranks):
         bytes_launch = BYTES_PER_CELL_STAGE[2] * cells
         achieved = bytes_launch / (d["ms_stage2"] / 1e3) / 1e9
         traffic = ncu_traffic(kname, cells)
+        b1 = BYTES_PER_CELL_STAGE[1] * cells
+        a1 = b1 / (d["ms_stage1"] / 1e3) / 1e9
         return {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
                 "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "peak_source": hbm_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": bytes_launch,
-                "step_hbm_frac": round(200 * cells / (d["ms"] / K / 1e3) / 1e9 / hbm, 4)}
+                "step_hbm_frac": round(200 * cells / (d["ms"] / K / 1e3) / 1e9 / hbm, 4),
+                "stage1": {"kernel": kname.replace("stage2", "stage1"),
+                           "achieved": round(a1, 1), "frac": round(a1 / hbm, 4),
+                           "algorithmic_bytes_per_launch": b1,
+                           "traffic": ncu_traffic(kname.replace("stage2", "stage1"), cells)}}
 
     # the latency-bound AMR run goes before the adjoint's host-bound
     # finite-difference loop, after which it measured up to 2x slower
+    batch64 = None if args.no_batch else batch64_section(ctx, ranks, K, W)
     amr = None if args.no_amr else amr_section(ctx, ranks)
     adjoint = None if args.no_adjoint else adjoint_section(ctx, ranks)
     plane = None if args.no_plane else plane_section(ctx, ranks, K, W)
@@ -398,8 +416,7 @@ def run_ours(args, ranks: Ranks):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 reconstruction+HLLC / f64 state, accumulation, reductions",
         "data": DATA,
-        "config": {"workload": f"3D {n}^3 periodic PLM/minmod+HLLC SSP-RK2, gamma 5/3, CFL 0.4, "
-                               "dt recomputed on device each step",
+        "config": {"workload": workload(n),
                    "cells_per_gpu": cells, "precision": "mixed", "kernel": mixed["kernel"],
                    "tile": f"16x16 columns, z chunk {mixed['kz']} (autotuned)",
                    "l2": "inputs larger than L2 (671 MB per state buffer)",
@@ -421,6 +438,8 @@ def run_ours(args, ranks: Ranks):
         "gpu_launches": mixed["launches"],
         "clocks": clocks,
     }
+    if batch64:
+        line["batch64"] = batch64
     if adjoint:
         line["adjoint"] = adjoint
     if amr:
@@ -745,14 +764,17 @@ def amr_section(ctx, ranks: Ranks, cpu_steps=60):
     return out
 
 
-def run_batch64(args, ranks: Ranks):
+BATCH_DATA = ("synthetic: 64 seeded planar two-state Riemann problems, rho in [0.1, 10], "
+              "|u| <= 2, p in [0.01, 10], gamma 1.4, outflow; cube sides from "
+              "{32,48,64,96,128,192,256}")
+
+
+def batch64_section(ctx, ranks: Ranks, K: int, W: int):
     """64 independent 3D Riemann boxes (cube sides drawn from {32..256}), mixed
     precision, stepped as one batch: one persistent launch per stage for all
     boxes, the K timed steps replayed as one CUDA graph."""
     import vespa_b200 as vb
     from vespa_b200 import problem as P
-    K, W = args.steps, args.warmup
-    ctx = vb.Context(ranks.local)
     probs = [P.riemann_box_problem(i, seed=P.DEFAULT_SEED + 1000 * ranks.rank) for i in range(64)]
     batch = vb.Batch(probs, precision="mixed", ctx=ctx)
     cells = batch.ncell()
@@ -767,23 +789,38 @@ def run_batch64(args, ranks: Ranks):
     ms = ranks.max(ctx.elapsed_ms(0, 1))
     launches = ctx.launch_count - l0
     total = ranks.sum(float(cells))
+    batch.close()
+    hbm, hbm_kind = measured_hbm()
+    return {"value": round(total * K / (ms / 1e3) / 1e6, 1), "unit": UNIT,
+            "ms_per_step": round(ms / K, 4), "steps": K, "warmup": W,
+            "cells_per_gpu": cells, "boxes": 64,
+            "sides": sorted({p.dims[0] for p in probs}),
+            "step_hbm_frac": round(200 * cells / (ms / K / 1e3) / 1e9 / hbm, 4),
+            "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_kind, "gpu_launches": launches,
+            "precision": "mixed", "data": BATCH_DATA,
+            "what": "per-box CFL dt; finalise, stage 1, stage 2 and advance per step for all "
+                    "boxes; the K timed steps replay one CUDA graph"}
+
+
+def run_batch64(args, ranks: Ranks):
+    """--workload batch64: the batch section alone, as its own JSON line."""
+    import vespa_b200 as vb
+    K, W = args.steps, args.warmup
+    ctx = vb.Context(ranks.local)
+    sec = batch64_section(ctx, ranks, K, W)
     if ranks.rank != 0:
         return
-    value = total * K / (ms / 1e3) / 1e6
-    hbm, hbm_kind = measured_hbm()
     line = {
         "metric": "Mcell-updates/s, 64 uneven 3D Riemann boxes batched, PLM+HLLC RK2, mixed",
-        "value": round(value, 1), "unit": UNIT, "n_gpus": ranks.world, "steps": K, "warmup": W,
-        "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 reconstruction+HLLC / f64 state", "data": (
-            "synthetic: 64 seeded planar two-state Riemann problems, rho in [0.1, 10], |u| <= 2, "
-            "p in [0.01, 10], gamma 1.4, outflow; cube sides from {32,48,64,96,128,192,256}"),
+        "value": sec["value"], "unit": UNIT, "n_gpus": ranks.world, "steps": K, "warmup": W,
+        "ms_per_step": sec["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 reconstruction+HLLC / f64 state",
+        "data": BATCH_DATA,
         "config": {"workload": "batch of 64 uneven boxes, per-box CFL dt, CUDA-graph replay",
-                   "cells_per_gpu": cells, "boxes": 64,
+                   "cells_per_gpu": sec["cells_per_gpu"], "boxes": 64,
                    "parallelism": f"independent batch per GPU x{ranks.world}"},
-        "step_hbm_frac": round(200 * cells / (ms / K / 1e3) / 1e9 / hbm, 4),
-        "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_kind,
-        "gpu_launches": launches,
+        "step_hbm_frac": sec["step_hbm_frac"], "hbm_peak_gbs": sec["hbm_peak_gbs"],
+        "hbm_peak_source": sec["hbm_peak_source"], "gpu_launches": sec["gpu_launches"],
     }
     print(json.dumps(line), flush=True)
 

@@ -132,9 +132,11 @@ int vb_grid_device_state(vb_grid *grid, double **dU);
  * per-face loop has no launch shape).  VB_OPT_KERNEL: VB_KERNEL_AUTO picks the
  * tiled 3D kernel when the grid allows it (nx, ny multiples of 16, nz >= 2),
  * VB_KERNEL_CELL forces the cell-centric kernel, VB_KERNEL_TILED requires the
- * tiled one.  VB_OPT_TILE_KZ: z planes per tiled work item.  Results do not
- * depend on either knob. */
-enum { VB_OPT_KERNEL = 1, VB_OPT_TILE_KZ = 2 };
+ * tiled one.  VB_OPT_TILE_KZ: z planes per tiled work item.
+ * VB_OPT_TILE_TAPER: -1 (default) tapers the 3D work queue's last z chunks
+ * for VB_MIXED grids only, 0 keeps uniform chunks, 1 tapers in either
+ * precision.  Results do not depend on any of these knobs. */
+enum { VB_OPT_KERNEL = 1, VB_OPT_TILE_KZ = 2, VB_OPT_TILE_TAPER = 3 };
 enum { VB_KERNEL_AUTO = 0, VB_KERNEL_CELL = 1, VB_KERNEL_TILED = 2 };
 int vb_grid_set_option(vb_grid *grid, int option, int64_t value);
 int vb_grid_get_option(const vb_grid *grid, int option, int64_t *value);
@@ -153,6 +155,13 @@ int vb_grid_get_time(vb_grid *grid, double *t, int64_t *step);
 /* compute_dt(sim), src/driver.jl:169-199: cfl / max over cells and axes of
  * (|v_d| + c) / w_d; +Inf when the gas is at rest. */
 int vb_compute_dt(vb_grid *grid, double *dt);
+/* No counterpart in the reference: a self-test of the failure path.  Runs one
+ * block that waits, bounded by limit_ns (1 us .. 10 s), on an mbarrier that
+ * nothing completes, then takes the tiled stage kernels' abandon path, which
+ * raises the grid's timeout flag; the call returns VB_ETIMEOUT exactly as a
+ * stage whose TMA load never arrived would, clears the flag and leaves the
+ * state and clock untouched. */
+int vb_grid_selftest_wait(vb_grid *grid, int64_t limit_ns);
 /* step!(sim, dt), src/driver.jl:333-359: one SSP-RK2 step, advances t. */
 int vb_step(vb_grid *grid, double dt);
 /* evolve!(sim), src/driver.jl:483-508: steps with dt = min(compute_dt,

@@ -68,3 +68,41 @@ def test_batch_rejects_untileable_boxes(vb):
     with pytest.raises(vb.VespaB200Error) as e:
         vb.Batch([bad])
     assert e.value.status == 6
+
+
+def test_seeded_64_box_batch_equals_single_runs_and_oracle(vb, oracle):
+    """The benchmark's batch (64 seeded Riemann boxes, sides from
+    {32, ..., 256}, about 282 M cells): after 3 mixed-precision steps every
+    box equals its single-grid run bit for bit; in float64 every box of side
+    64 or less equals the oracle bit for bit."""
+    probs = [P.riemann_box_problem(i, seed=P.DEFAULT_SEED) for i in range(64)]
+    assert len({p.dims[0] for p in probs}) >= 5  # the draw spans the side list
+    steps = 3
+    batch = vb.Batch(probs, precision="mixed")
+    batch.run_steps(steps)
+    for i, p in enumerate(probs):
+        U0 = P.initial_state(p)
+        sim = vb.Simulation(vb.B200Mesh(p.dims, p.domain), p, precision="mixed", initial=U0)
+        sim.set_kernel("tiled")
+        vb.evolve(sim, tfinal=math.inf, max_steps=steps)
+        assert batch.time(i) == (sim.t, steps), i
+        a = batch.state(i)
+        b = sim.state()
+        sim.close()
+        assert np.array_equal(a, b), (i, p.dims, float(np.abs(a - b).max()))
+    batch.close()
+
+    batch = vb.Batch(probs, precision="fp64")
+    batch.run_steps(steps)
+    checked = 0
+    for i, p in enumerate(probs):
+        if p.dims[0] > 64:
+            continue
+        U = P.initial_state(p)
+        t, n = oracle.evolve(oracle.grid_from_problem(p), U, math.inf, max_steps=steps, mode=1)
+        assert batch.time(i) == (t, n), i
+        a = batch.state(i)
+        assert np.array_equal(a, U), (i, p.dims, float(np.abs(a - U).max()))
+        checked += 1
+    batch.close()
+    assert checked >= 10

@@ -87,3 +87,29 @@ def test_batch_rejects_boxes_the_tiled_kernel_cannot_take(vb):
     with pytest.raises(vb.VespaB200Error) as e:
         vb.Batch([good, bad])
     assert "VB_ENOTSUP" in str(e.value)
+
+
+def test_bounded_wait_gives_up_and_reports_a_timeout(vb, oracle):
+    """The failure path of the tiled kernels' TMA stage waits, made to run out
+    without faulting anything: a block waits (limit 1 ms) on an mbarrier that
+    nothing completes, takes the stage kernels' abandon path and raises the
+    grid's timeout flag; the host returns VB_ETIMEOUT, the state and clock are
+    untouched, and the grid (and context) keep working afterwards."""
+    from vespa_b200 import _lib
+    prob = P.smooth_random_problem((32, 32, 16), seed=5)
+    U0 = P.initial_state(prob)
+    sim = make_sim(prob, U0)
+    sim.set_kernel("tiled")
+    rc = _lib.load().vb_grid_selftest_wait(sim.handle, 1_000_000)
+    assert rc == _lib.VB_ETIMEOUT
+    assert "gave up" in _lib.last_error()
+    assert sim.t == 0.0 and sim.step == 0
+    assert np.array_equal(sim.state(), U0)
+    vb.evolve(sim, max_steps=2)  # no stale flag: the next steps run and match the oracle
+    U = U0.copy()
+    t, n = oracle.evolve(oracle.grid_from_problem(prob), U, math.inf, max_steps=2, mode=1)
+    assert sim.step == n == 2 and sim.t == t
+    assert_bit_identical(sim.state(), U)
+    with pytest.raises(vb.VespaB200Error) as e:
+        _lib.call("vb_grid_selftest_wait", sim.handle, 0)
+    assert e.value.status == _lib.VB_EINVAL

@@ -255,13 +255,21 @@ using vb::detail::box_items;
 using vb::detail::encode_maps;
 using vb::detail::make_box;
 
-// Refresh the grid's box descriptor after kz (or the maps) changed.
+// Whether the grid's 3D work queue uses tapered z chunks (VB_OPT_TILE_TAPER;
+// by default single VB_MIXED grids do).
+bool grid_taper(const vb_grid *gr)
+{
+    return gr->taper < 0 ? gr->precision == VB_MIXED : gr->taper != 0;
+}
+
+// Refresh the grid's box descriptor after kz, the taper (or the maps) changed.
 int sync_box(vb_grid *gr)
 {
-    if (gr->box_kz == gr->kz) return VB_OK;
-    gr->box = make_box(gr->maps_U, gr->maps_U1, gr->g, gr->U, gr->U1, gr->ctrl, gr->kz, 0,
-                       gr->precision == VB_MIXED);
+    const int tp = grid_taper(gr) ? 1 : 0;
+    if (gr->box_kz == gr->kz && gr->box_taper == tp) return VB_OK;
+    gr->box = make_box(gr->maps_U, gr->maps_U1, gr->g, gr->U, gr->U1, gr->ctrl, gr->kz, 0, tp != 0);
     gr->box_kz = gr->kz;
+    gr->box_taper = tp;
     return VB_OK;
 }
 
@@ -272,7 +280,7 @@ int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout
     if (gr->tiled && !bf && (!grav || gr->g.nd == 3)) {
         int rc = sync_box(gr);
         if (rc) return rc;
-        const int64_t items = box_items(gr->g, gr->kz, gr->precision == VB_MIXED);
+        const int64_t items = box_items(gr->g, gr->kz, grid_taper(gr));
         if (items > 0x7fffffff) return fail(VB_ENOTSUP, "too many tiled work items");
         unsigned int *work = gr->ctrl->work;  // device address of the cursors
         if (gr->g.nd == 2) {
@@ -350,7 +358,8 @@ constexpr int64_t GRAPH_STEPS = 8;
 
 uint64_t graph_key(const vb_grid *gr)
 {
-    return (gr->tiled ? 1u : 0u) | (gr->bflux_on ? 2u : 0u) | ((uint64_t)gr->kz << 2);
+    return (gr->tiled ? 1u : 0u) | (gr->bflux_on ? 2u : 0u) | (grid_taper(gr) ? 4u : 0u) |
+           ((uint64_t)gr->kz << 3);
 }
 
 // Capture GRAPH_STEPS steps into the grid's graph for its current configuration.
@@ -727,6 +736,10 @@ int vb_grid_set_option(vb_grid *gr, int option, int64_t value)
             return fail(VB_EINVAL, "the chunk must be in 1..nz (3D) or 1..ny (2D)");
         gr->kz = (int)value;
         return VB_OK;
+    case VB_OPT_TILE_TAPER:
+        if (value < -1 || value > 1) return fail(VB_EINVAL, "taper must be -1 (auto), 0 or 1");
+        gr->taper = (int)value;
+        return VB_OK;
     default:
         return fail(VB_EINVAL, "unknown option");
     }
@@ -738,6 +751,7 @@ int vb_grid_get_option(const vb_grid *gr, int option, int64_t *value)
     switch (option) {
     case VB_OPT_KERNEL: *value = gr->tiled ? VB_KERNEL_TILED : VB_KERNEL_CELL; return VB_OK;
     case VB_OPT_TILE_KZ: *value = gr->kz; return VB_OK;
+    case VB_OPT_TILE_TAPER: *value = grid_taper(gr) ? 1 : 0; return VB_OK;
     default: return fail(VB_EINVAL, "unknown option");
     }
 }
@@ -843,6 +857,24 @@ int vb_compute_dt(vb_grid *gr, double *dt)
     }
     *dt = invdt == 0.0 ? INFINITY : gr->g.cfl / invdt;
     return VB_OK;
+}
+
+int vb_grid_selftest_wait(vb_grid *gr, int64_t limit_ns)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    if (limit_ns < 1000 || limit_ns > 10000000000LL)
+        return fail(VB_EINVAL, "limit_ns must be in [1e3, 1e10]");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    VB_CHECK_LAUNCH(gr->ctx, vb::launch_wait_selftest(gr->ctrl, (uint64_t)limit_ns, gr->ctx->stream));
+    rc = pull_ctrl(gr);
+    if (rc) return rc;
+    if (!(gr->hctrl->flags & vb::CTRL_F_TIMEOUT)) return fail(VB_ECUDA, "the self-test wait did not give up");
+    // report as a stage would, and leave the grid usable
+    gr->hctrl->flags &= ~vb::CTRL_F_TIMEOUT;
+    rc = push_ctrl(gr);
+    if (rc) return rc;
+    return fail(VB_ETIMEOUT, "a bounded device wait (TMA stage load) gave up");
 }
 
 int vb_step(vb_grid *gr, double dt)

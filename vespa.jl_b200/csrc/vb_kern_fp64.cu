@@ -224,7 +224,33 @@ __global__ void k_advance(Ctrl *ctrl)
     }
 }
 
+// Failure-path self-test: the tiled kernels' bounded stage wait on an
+// mbarrier that nothing will ever complete (no copy is issued, so nothing is
+// in flight), then the same block-uniform decision and abandon path as a
+// stage kernel whose TMA load never arrived.  Touches no state.
+__global__ void k_wait_selftest(Ctrl *ctrl, uint64_t limit_ns)
+{
+    __shared__ uint64_t bar;
+    __shared__ int stall_sh;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        stall_sh = 0;
+    }
+    __syncthreads();
+    if (!mbar_wait(&bar, 0, limit_ns)) stall_sh = 1;  // phase 0 never completes
+    __syncthreads();
+    if (stall_sh) stage_abandon<1>(&bar, 0, 0, 0, ctrl);  // no stage planes in flight
+}
+
 }  // namespace
+
+int launch_wait_selftest(Ctrl *ctrl, uint64_t limit_ns, cudaStream_t s)
+{
+    if (!ctrl || limit_ns == 0) return -1;
+    k_wait_selftest<<<1, 64, 0, s>>>(ctrl, limit_ns);
+    return 1;
+}
 
 int launch_finalize_boxes(const BoxDesc *boxes, int nbox, unsigned int *work, cudaStream_t s)
 {

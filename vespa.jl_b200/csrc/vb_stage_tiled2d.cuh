@@ -66,11 +66,13 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
     t2::Smem<T, NS> &S = *reinterpret_cast<t2::Smem<T, NS> *>(smem_raw);
     __shared__ double red[32];
     __shared__ int item_sh;
+    __shared__ int stall_sh;  // a stage load's bounded wait gave up
     const int t = threadIdx.x;
 
     if (t == 0) {
         for (int s = 0; s < NS; ++s) mbar_init(&S.bar[s], 1);
         fence_mbar_init();
+        stall_sh = 0;
     }
     __syncthreads();
 
@@ -106,7 +108,6 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
         return (bc == BC_REFLECTING && f == 1 + axis) ? -w : w;
     };
 
-    bool timed_out = false;
     int qb = 0;
     double invdt = 0.0;
     for (;;) {
@@ -142,7 +143,7 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
     }
     auto consume = [&](int q, T Wown[5], bool halo) {
         const int b = (qb + q) % NS;
-        if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) timed_out = true;
+        if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) stall_sh = 1;
         const double *u = S.u[b];
         double uu[5];
 #pragma unroll
@@ -164,19 +165,29 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
             issue(q + NS);
         }
     };
+    // after the barrier that follows consume(q): uniform across the block
+    auto stalled = [&](int q) -> bool {
+        if (!stall_sh) return false;
+        stage_abandon<NS>(S.bar, qb, q, nrows, ctrl);
+        return true;
+    };
 
     T Wa[5], Wb[5], Wy0[5], Wy1[5], Wy2[5];
     consume(0, Wa, false);
     __syncthreads();
+    if (stalled(0)) return;
     release(0);
     consume(1, Wb, false);
     __syncthreads();
+    if (stalled(1)) return;
     release(1);
     consume(2, Wy0, true);
     __syncthreads();
+    if (stalled(2)) return;
     release(2);
     consume(3, Wy1, true);
     __syncthreads();
+    if (stalled(3)) return;
     release(3);
 
     // y state entering row r0: hi face value of r0 and the flux through r0-1/2
@@ -248,6 +259,7 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
 #pragma unroll
         for (int f = 0; f < 5; ++f) S.w[f][t] = Wy0[f];
         __syncthreads();  // (1) row r primitives complete
+        if (stalled(q)) return;
         release(q);
 
         // ---- x slope and x face values of the own cell ----
@@ -415,7 +427,6 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
     }
     qb += nrows;
     }  // work items
-    if (timed_out && t == 0) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
     if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);
 }
 

@@ -84,6 +84,23 @@ __device__ __forceinline__ void tiled_hllc(const double WL[5], const double WR[5
     for (int k = 0; k < 5; ++k) F[k] = r.v[k];
 }
 
+// A stage load's bounded wait gave up (a block-uniform decision, taken after
+// the barrier that follows the wait): the block issues no further load and
+// skips the rest of its work.  Thread 0 waits, each wait bounded again, for
+// the item's stage loads that may still be in flight -- stage planes q .. q +
+// NS - 1 below nplanes, pipeline position qb -- so that no copy lands in the
+// block's shared memory after it has exited, and flags the box; every thread
+// waits for its own cp.async copies.  The caller then returns from the kernel.
+template <int NS>
+__device__ __noinline__ void stage_abandon(uint64_t *bars, int qb, int q, int nplanes, Ctrl *ctrl)
+{
+    cp_async_wait_all();
+    if (threadIdx.x != 0) return;
+    for (int j = q; j < q + NS && j < nplanes; ++j)
+        mbar_wait(&bars[(qb + j) % NS], ((qb + j) / NS) & 1, WAIT_LIMIT_NS);
+    atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
+}
+
 __device__ __forceinline__ int lo_class(int64_t c, int64_t n, bool periodic)
 {
     if (c > 0) return LO_BEFORE;

@@ -65,6 +65,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
     t3d::Smem<NS> &S = *reinterpret_cast<t3d::Smem<NS> *>(smem_raw);
     __shared__ double red[32];
     __shared__ int item_sh;
+    __shared__ int stall_sh;  // a stage load's bounded wait gave up
 
     const int t = threadIdx.x;
     const int tx = t & (TX - 1), ty = t >> 4;
@@ -83,10 +84,10 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
     if (t == 0) {
         for (int s = 0; s < NS; ++s) mbar_init(&S.bar[s], 1);
         fence_mbar_init();
+        stall_sh = 0;
     }
     __syncthreads();
 
-    bool timed_out = false;
     int qb = 0;
     for (;;) {
     if (t == 0) item_sh = (int)atomicAdd(&work[STAGE - 1], 1u);
@@ -162,7 +163,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
     // the halo strips; 2: as 1 without the halo strips (halo_c2p follows).
     auto consume = [&](int q, double Wn[5], int keep) {
         const int b = (qb + q) % NS;
-        if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) timed_out = true;
+        if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) stall_sh = 1;
         const double *u = S.u[b];
         {
             double uu[5];
@@ -202,19 +203,29 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
             issue(q + NS);
         }
     };
+    // after the barrier that follows consume(q): uniform across the block
+    auto stalled = [&](int q) -> bool {
+        if (!stall_sh) return false;
+        stage_abandon<NS>(S.bar, qb, q, nplanes, ctrl);
+        return true;
+    };
 
     double Wa[5], Wb[5], Wc[5], Wd[5];
     consume(0, Wa, 0);
     __syncthreads();
+    if (stalled(0)) return;
     release(0);
     consume(1, Wb, 0);
     __syncthreads();
+    if (stalled(1)) return;
     release(1);
     consume(2, Wc, 1);
     __syncthreads();
+    if (stalled(2)) return;
     release(2);
     consume(3, Wd, 1);
     __syncthreads();
+    if (stalled(3)) return;
     release(3);
 
     // z state entering plane k0: hi face value of k0 and the flux through k0-1/2
@@ -336,6 +347,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
                 if (k > k0) invdt = cf;
         }
         __syncthreads();  // (1) plane k+2 converted
+        if (stalled(q)) return;
         release(q);
         // ---- phase 2: the own lo x / lo y faces; the z face (warps 0..3) or
         //      a hi-edge face (warps 6, 7) ----
@@ -417,7 +429,6 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
     }
     if constexpr (STAGE == 2) invdt = cfl_term_exact<GRAV>(unp, g, invdt);  // the item's last plane
     qb += nplanes;
-    if (timed_out && t == 0) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
     if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);  // this box's CFL max
     }  // work items
 }

@@ -187,6 +187,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     t3m::Smem<NS> &S = *reinterpret_cast<t3m::Smem<NS> *>(smem_raw);
     __shared__ double red[32];
     __shared__ int item_sh;
+    __shared__ int stall_sh;  // a stage load's bounded wait gave up
 
     const int t = threadIdx.x;
     const int tx = t & (TX - 1), ty = t >> 4;
@@ -210,10 +211,10 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     if (t == 0) {
         for (int s = 0; s < NS; ++s) mbar_init(&S.bar[s], 1);
         fence_mbar_init();
+        stall_sh = 0;
     }
     __syncthreads();
 
-    bool timed_out = false;
     int qb = 0;
     for (;;) {
     if (t == 0) item_sh = (int)atomicAdd(&work[STAGE - 1], 1u);
@@ -295,7 +296,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     // the halo strips; 2: as 1 without the halo strips (halo_c2p follows).
     auto consume = [&](int q, float Wn[5], int keep) {
         const int b = (qb + q) % NS;
-        if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) timed_out = true;
+        if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) stall_sh = 1;
         const double *u = S.u[b];
         {
             double uu[5];
@@ -335,19 +336,29 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
             issue(q + NS);
         }
     };
+    // after the barrier that follows consume(q): uniform across the block
+    auto stalled = [&](int q) -> bool {
+        if (!stall_sh) return false;
+        stage_abandon<NS>(S.bar, qb, q, nplanes, ctrl);
+        return true;
+    };
 
     float Wa[5], Wb[5], Wc[5], Wd[5];
     consume(0, Wa, 0);
     __syncthreads();
+    if (stalled(0)) return;
     release(0);
     consume(1, Wb, 0);
     __syncthreads();
+    if (stalled(1)) return;
     release(1);
     consume(2, Wc, 1);
     __syncthreads();
+    if (stalled(2)) return;
     release(2);
     consume(3, Wd, 1);
     __syncthreads();
+    if (stalled(3)) return;
     release(3);
 
     // z state entering plane k0: hi face value of k0 and the flux through k0-1/2
@@ -465,6 +476,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
                 if (k > k0) invdtf = cf;
         }
         __syncthreads();  // (1) plane k+2 converted
+        if (stalled(q)) return;
         release(q);
         // ---- phase 2: the own lo x / lo y face pair; the z face (warps 0..3)
         //      or the tile's hi-edge faces (warp 7) ----
@@ -549,7 +561,6 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     if constexpr (STAGE == 2)  // the item's last plane
         invdt = (double)cfl_mixed<GRAV>(unp, g, gf, iw0, iw1, iw2, invdtf);
     qb += nplanes;
-    if (timed_out && t == 0) atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
     if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);  // this box's CFL max
     }  // work items
 }

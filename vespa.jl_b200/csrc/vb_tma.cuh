@@ -59,7 +59,8 @@ __device__ __forceinline__ uint64_t globaltimer_ns()
 }
 
 // Bounded wait: returns false once `limit_ns` of wall time has passed (the
-// caller records an error flag and carries on, so a block never hangs).
+// caller then abandons its work item, see stage_abandon, so a block never
+// hangs and never computes from a stage buffer that did not fill).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
 {
     if (mbar_try_wait(bar, parity)) return true;

@@ -18,7 +18,7 @@ STATUS_NAMES = {0: "VB_OK", 1: "VB_EINVAL", 2: "VB_ECUDA", 3: "VB_ENOMEM", 4: "V
                 5: "VB_ETIMEOUT", 6: "VB_ENOTSUP"}
 BC_OUTFLOW, BC_PERIODIC, BC_REFLECTING = 0, 1, 2
 FP64, MIXED = 0, 1
-OPT_KERNEL, OPT_TILE_KZ = 1, 2
+OPT_KERNEL, OPT_TILE_KZ, OPT_TILE_TAPER = 1, 2, 3
 KERNELS = {"auto": 0, "cell": 1, "tiled": 2}
 
 
@@ -102,6 +102,7 @@ SIGNATURES = {
     "vb_grid_get_time": [_VP, _DP, _I64P],
     "vb_compute_dt": [_VP, _DP],
     "vb_step": [_VP, C.c_double],
+    "vb_grid_selftest_wait": [_VP, C.c_int64],
     "vb_evolve": [_VP, C.c_double, C.c_int64, _DP, _I64P],
     "vb_run_steps_async": [_VP, C.c_int64],
     "vb_conserved_totals": [_VP, _DP],

@@ -222,11 +222,23 @@ class Simulation:
         _lib.call("vb_grid_set_time", self.handle, float(t), int(step))
 
     # -- kernel selection / tuning (results do not depend on these) --
-    def set_kernel(self, kind: str = "auto", kz: Optional[int] = None) -> None:
-        """kind: "auto", "cell" (cell-centric kernel) or "tiled" (tiled 3D kernel)."""
+    def set_kernel(self, kind: str = "auto", kz: Optional[int] = None,
+                   taper: Optional[bool] = None) -> None:
+        """kind: "auto", "cell" (cell-centric kernel) or "tiled" (tiled 3D kernel).
+        kz: z planes per tiled work item.  taper: tapered (True) or uniform
+        (False) z chunks in the 3D work queue; None restores the default
+        (tapered for VB_MIXED grids)."""
         _lib.call("vb_grid_set_option", self.handle, _lib.OPT_KERNEL, _lib.KERNELS[kind])
         if kz is not None:
             _lib.call("vb_grid_set_option", self.handle, _lib.OPT_TILE_KZ, int(kz))
+        _lib.call("vb_grid_set_option", self.handle, _lib.OPT_TILE_TAPER,
+                  -1 if taper is None else int(bool(taper)))
+
+    @property
+    def taper(self) -> bool:
+        v = C.c_int64()
+        _lib.call("vb_grid_get_option", self.handle, _lib.OPT_TILE_TAPER, C.byref(v))
+        return bool(v.value)
 
     def autotune(self, nsteps: int = 3) -> tuple:
         """Pick the fastest z-chunk for the tiled kernel on this grid (state and
