@@ -61,6 +61,8 @@ def parse():
                     help="skip the KH 512^2 adjoint timing and finite-difference check")
     ap.add_argument("--no-gravity", action="store_true",
                     help="skip the 256^3 self-gravity run")
+    ap.add_argument("--no-bflux", action="store_true",
+                    help="skip the 256^3 boundary-flux recording run")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the 64-box batch run")
     ap.add_argument("--no-muscl", action="store_true",
@@ -401,6 +403,7 @@ def run_ours(args, ranks: Ranks):
     amr = None if args.no_amr else amr_section(ctx, ranks)
     adjoint = None if args.no_adjoint else adjoint_section(ctx, ranks)
     plane = None if args.no_plane else plane_section(ctx, ranks, K, W)
+    bflux = None if args.no_bflux else bflux_section(ctx, ranks, min(K, 20), W)
     gravity = None if args.no_gravity else gravity_section(ctx, ranks, min(K, 20), W)
     muscl = None if args.no_muscl else muscl_section(ctx, ranks, min(K, 20), W)
 
@@ -446,6 +449,8 @@ def run_ours(args, ranks: Ranks):
         line["amr"] = amr
     if plane:
         line["plane2d"] = plane
+    if bflux:
+        line["bflux"] = bflux
     if gravity is not None:
         line["gravity"] = gravity
     if muscl is not None:
@@ -557,6 +562,39 @@ def plane_section(ctx, ranks: Ranks, K: int, W: int, n=4096):
                      "ms_per_step": round(ms / K, 4), "kernel": sim.kernel, "row_chunk": ky,
                      "stage2_hbm_frac": round(s2 / hbm, 4)}
         sim.close()
+    return out
+
+
+def bflux_section(ctx, ranks: Ranks, K: int, W: int, n=256):
+    """The cube's generator on an outflow 256^3 box, both precisions, with and
+    without the boundary-flux register recording the domain faces
+    (BoundaryFluxRegister, src/reflux.jl:113-132): the tiled kernels record
+    them in place, so the step keeps its speed."""
+    import vespa_b200 as vb
+    prob = vb.smooth_random_problem((n, n, n), seed=vb.problem.DEFAULT_SEED + ranks.rank)
+    prob.bcs = vb.problem.Outflow
+    U0 = vb.initial_state(prob)
+    mesh = vb.B200Mesh(prob.dims, prob.domain)
+    out = {"config": f"3D {n}^3, outflow on all six sides, gamma 5/3, CFL 0.4; the register "
+                     "records (0.5 dt F) area at every domain face in both RK2 stages"}
+    for prec in ("fp64", "mixed"):
+        res = {}
+        for on in (False, True):
+            sim = vb.Simulation(mesh, prob, precision=prec, ctx=ctx, initial=U0)
+            sim.bflux_enable(on)
+            vb.run_steps_async(sim, W)
+            ctx.synchronize()
+            ranks.barrier()
+            ctx.mark(8)
+            vb.run_steps_async(sim, K)
+            ctx.mark(9)
+            ms = ranks.max(ctx.elapsed_ms(8, 9))
+            res["on" if on else "off"] = {
+                "value": round(n ** 3 * ranks.world * K / (ms / 1e3) / 1e6, 1), "unit": UNIT,
+                "ms_per_step": round(ms / K, 4), "kernel": sim.kernel, "kz": sim.kz}
+            sim.close()
+        res["on_over_off_time"] = round(res["on"]["ms_per_step"] / res["off"]["ms_per_step"], 4)
+        out[prec] = res
     return out
 
 

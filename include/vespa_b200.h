@@ -200,15 +200,38 @@ int vb_batch_run_steps_async(vb_batch *batch, int64_t nsteps);
 int vb_batch_get_time(vb_batch *batch, int box, double *t, int64_t *step);
 int vb_batch_conserved_totals(vb_batch *batch, int box, double out[5]);
 
-/* Boundary-flux register (BoundaryFluxRegister, src/reflux.jl:113-132): while
- * enabled, every domain-boundary face accumulates (0.5*dt*F)*area per RK2
- * stage.  Planes are stored per axis d (1..ndim) and side (lo, hi), five
- * components each, the flux axis collapsed and the other axes column-major
- * with the lowest axis fastest (the bflux_plane raster, src/reflux.jl:148-191). */
+/* Boundary-flux register (BoundaryFluxRegister, src/reflux.jl:113-146).
+ * vb_bflux_enable(grid, VB_BFLUX_OUTER): while enabled, every domain-boundary
+ * face accumulates (0.5*dt*F)*area per RK2 stage (_bflux_capture!,
+ * src/reflux.jl:125-132) -- recorded by whichever stage kernel runs, the
+ * tiled ones included.  VB_BFLUX_INTERIOR also records every interior face
+ * (record_interior, _bflux_capture_interior!, src/reflux.jl:138-146; the
+ * cell-centric kernel then runs).  VB_BFLUX_OFF stops recording and keeps the
+ * values.  Changing between OUTER and INTERIOR reallocates a zeroed register.
+ * Layout (vb_bflux_read): the outer planes per axis d (1..ndim) and side (lo,
+ * hi), five components each, the flux axis collapsed and the other axes
+ * column-major with the lowest axis fastest; then, with INTERIOR, per axis the
+ * five components of every cell's hi face keyed by that (lo) cell, ncell
+ * values each, zero where the hi side is a domain boundary. */
+enum { VB_BFLUX_OFF = 0, VB_BFLUX_OUTER = 1, VB_BFLUX_INTERIOR = 2 };
 int vb_bflux_enable(vb_grid *grid, int enable);
 int vb_bflux_size(const vb_grid *grid, int64_t *n);
 int vb_bflux_read(vb_grid *grid, double *out, int64_t n);
 int vb_bflux_clear(vb_grid *grid);
+/* bflux_plane(Val(R), dim, start, stop, g0, flux_off, comp, Vcell, lookup)
+ * (src/reflux.jl:171-191) on the device: rasterises one face plane of the
+ * register into out (n = prod(stop - start + 1) doubles, column-major, axis 0
+ * fastest), each value the recorded flux component comp (1-based; comp <= 0
+ * gives zeros) divided by vcell.  dim is the 0-based flux axis; start, stop
+ * and g0 hold R = ndim global indices; along dim the active index is flux_off,
+ * across it g - g0 + 1.  source replaces the reference's lookup closure:
+ * VB_BFLUX_PLANE_LO / _HI read the outer register of that side (cells other
+ * than the boundary cell read 0), VB_BFLUX_PLANE_INTERIOR the interior
+ * register.  Cells outside the grid read 0. */
+enum { VB_BFLUX_PLANE_LO = 0, VB_BFLUX_PLANE_HI = 1, VB_BFLUX_PLANE_INTERIOR = 2 };
+int vb_bflux_plane(vb_grid *grid, int dim, int source, const int64_t *start, const int64_t *stop,
+                   const int64_t *g0, int64_t flux_off, int comp, double vcell, double *out,
+                   int64_t n);
 
 /* Self-gravity on a uniform grid (src/gravity.jl): enable_gravity!,
  * solve_poisson!, apply_laplacian!, and the source g = -grad phi that

@@ -72,6 +72,13 @@ const VB_GRAV_PRECOND_MG = Int32(1)
 const VB_MUSCL_BC_NONE = Int32(0)
 const VB_MUSCL_BC_PERIODIC = Int32(1)
 const VB_NOALLOC_MAX_FACES = 65536
+# boundary-flux register modes and bflux_plane sources
+const VB_BFLUX_OFF = Cint(0)
+const VB_BFLUX_OUTER = Cint(1)
+const VB_BFLUX_INTERIOR = Cint(2)
+const VB_BFLUX_PLANE_LO = Cint(0)
+const VB_BFLUX_PLANE_HI = Cint(1)
+const VB_BFLUX_PLANE_INTERIOR = Cint(2)
 
 # ------------------------------------------------------------------ structs
 # Field for field the C structs of the header (same order, same widths).
@@ -198,6 +205,8 @@ vb_bflux_size(grid, n) =
     ccall((:vb_bflux_size, libvespa_b200), Cint, (Ptr{Cvoid}, Ptr{Int64}), grid, n)
 vb_bflux_read(grid, out, n) =
     ccall((:vb_bflux_read, libvespa_b200), Cint, (Ptr{Cvoid}, Ptr{Float64}, Int64), grid, out, n)
+vb_bflux_plane(grid, dim, source, start, stop, g0, flux_off, comp, vcell, out, n) =
+    ccall((:vb_bflux_plane, libvespa_b200), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Int64, Cint, Float64, Ptr{Float64}, Int64), grid, dim, source, start, stop, g0, flux_off, comp, vcell, out, n)
 vb_bflux_clear(grid) =
     ccall((:vb_bflux_clear, libvespa_b200), Cint, (Ptr{Cvoid},), grid)
 vb_gravity_enable(grid, desc) =

@@ -83,6 +83,11 @@ def lib():
         L.vo_conserved_totals.argtypes = [gp, dp, dp]
         L.vo_bflux_size.argtypes = [gp]
         L.vo_bflux_size.restype = C.c_int64
+        u8p = C.POINTER(C.c_uint8)
+        i64p = C.POINTER(C.c_int64)
+        L.vo_step_breg.argtypes = [gp, dp, dp, dp, C.c_double, dp, u8p, dp, u8p]
+        L.vo_bflux_plane.argtypes = [gp, dp, u8p, dp, u8p, C.c_int, C.c_int, i64p, i64p, i64p,
+                                     C.c_int64, C.c_int, C.c_double, dp]
         L.vo_exact_riemann_star.argtypes = [dp, dp, C.c_double, dp]
         L.vo_exact_riemann_sample.argtypes = [dp, dp, C.c_double, C.c_double, dp]
         vp = C.c_void_p
@@ -241,6 +246,65 @@ def conserved_totals(g: VoGrid, U):
 
 def bflux_size(g: VoGrid) -> int:
     return int(lib().vo_bflux_size(C.byref(g)))
+
+
+class BoundaryFluxRegister:
+    """BoundaryFluxRegister (src/reflux.jl:113-118) in dense form: the outer
+    values in the vb_bflux_read plane layout plus a mask of the keys the Dict
+    would hold; with record_interior, the interior values [axis][5][ncell] and
+    their mask."""
+
+    def __init__(self, g: VoGrid, record_interior: bool = False):
+        self.g = g
+        n = bflux_size(g)
+        nc = ncell(g)
+        self.vals = np.zeros(n)
+        self.seen = np.zeros(n, dtype=np.uint8)
+        self.ivals = np.zeros(g.ndim * 5 * nc) if record_interior else None
+        self.iseen = np.zeros(g.ndim * nc, dtype=np.uint8) if record_interior else None
+
+    def empty(self):
+        self.vals[:] = 0.0
+        self.seen[:] = 0
+        if self.ivals is not None:
+            self.ivals[:] = 0.0
+            self.iseen[:] = 0
+
+    def dense(self) -> np.ndarray:
+        """The register in vb_bflux_read's layout (outer planes, then interior)."""
+        return self.vals if self.ivals is None else np.concatenate([self.vals, self.ivals])
+
+
+def _u8p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint8)) if a is not None else None
+
+
+def step_breg(g: VoGrid, U, dt, reg: BoundaryFluxRegister):
+    """step!(sim, dt; bflux = reg), serial face enumeration, in place on U."""
+    assert U.dtype == np.float64 and U.flags.c_contiguous
+    u0 = np.empty_like(U)
+    acc = np.empty_like(U)
+    lib().vo_step_breg(C.byref(g), _dp(U), _dp(u0), _dp(acc), float(dt), _dp(reg.vals),
+                       _u8p(reg.seen), _dp(reg.ivals) if reg.ivals is not None else None,
+                       _u8p(reg.iseen))
+    return U
+
+
+def bflux_plane(g: VoGrid, reg: BoundaryFluxRegister, dim, source, start, stop, g0, flux_off,
+                comp, vcell):
+    """bflux_plane (src/reflux.jl:171-191); source 0 / 1 / 2 = the outer lo /
+    hi keys or the interior keys stand for the caller's lookup."""
+    st = np.ascontiguousarray(start, dtype=np.int64)
+    sp = np.ascontiguousarray(stop, dtype=np.int64)
+    g0a = np.ascontiguousarray(g0, dtype=np.int64)
+    out = np.empty(int(np.prod(sp - st + 1)))
+    i64p = C.POINTER(C.c_int64)
+    lib().vo_bflux_plane(C.byref(g), _dp(reg.vals), _u8p(reg.seen),
+                         _dp(reg.ivals) if reg.ivals is not None else None, _u8p(reg.iseen),
+                         int(dim), int(source), st.ctypes.data_as(i64p), sp.ctypes.data_as(i64p),
+                         g0a.ctypes.data_as(i64p), int(flux_off), int(comp), float(vcell),
+                         _dp(out))
+    return out
 
 
 def exact_riemann_star(WL, WR, gamma):

@@ -317,11 +317,50 @@ static void bflux_capture(const geom_t *G, double *bflux, double scale, int d, i
     for (int k = 0; k < 5; ++k) bflux[base + k * P] += scale * F[k] * area;
 }
 
+/* The boundary-flux register as a dense restatement of its Dicts
+ * (src/reflux.jl:113-118): `vals` holds the values, `seen` marks the keys the
+ * Dict would contain (captured at least once).  Outer keys (axis, side, cell)
+ * map to the plane layout above; interior keys (axis, lo cell) to
+ * [axis][5][ncell]. */
+typedef struct {
+    double *vals, *ivals;
+    unsigned char *seen, *iseen;
+} breg_t;
+
+/* _bflux_capture!, keyed (axis d, side, cell lin) */
+static void breg_outer(const geom_t *G, const breg_t *r, double scale, int d, int side,
+                       int64_t lin, const double *F, double area)
+{
+    if (!r || !r->vals) return;
+    bflux_capture(G, r->vals, scale, d, side, lin, F, area);
+    if (r->seen) r->seen[bflux_base(G, d, side) + bflux_plane_index(G, lin, d)] = 1;
+}
+
+/* _bflux_capture_interior!, src/reflux.jl:138-146: keyed (axis d, lo cell lin),
+ * reg += (scale * f) * area, only when the register records interior faces */
+static void breg_interior(const geom_t *G, const breg_t *r, double scale, int d, int64_t lin,
+                          const double *F, double area)
+{
+    if (!r || !r->ivals) return;
+    for (int k = 0; k < 5; ++k) r->ivals[((int64_t)d * 5 + k) * G->ncell + lin] += scale * F[k] * area;
+    if (r->iseen) r->iseen[(int64_t)d * G->ncell + lin] = 1;
+}
+
+static void accumulate_flux_reg(const vo_grid *g, const double *U, double *acc, const breg_t *reg,
+                                double bscale);
+
 /* accumulate_flux! + for_each_face (src/driver.jl:209-281,
  * lib/RefMesh/src/RefMesh.jl:187-197): cells column-major; per cell and axis,
  * the hi face, then the lo face only when it is a domain boundary. */
 void vo_accumulate_flux(const vo_grid *g, const double *U, double *acc, double *bflux,
                         double bscale)
+{
+    breg_t r = {bflux, NULL, NULL, NULL};
+    accumulate_flux_reg(g, U, acc, bflux ? &r : NULL, bscale);
+}
+
+static void accumulate_flux_reg(const vo_grid *g, const double *U, double *acc, const breg_t *reg,
+                                double bscale)
 {
     geom_t G;
     make_geom(g, &G);
@@ -338,13 +377,14 @@ void vo_accumulate_flux(const vo_grid *g, const double *U, double *acc, double *
                 vo_hllc_flux(WL, WR, g->gamma, d + 1, F);
                 acc_add(&G, acc, lin, F, a);
                 acc_add(&G, acc, nhi, F, -a);
+                breg_interior(&G, reg, bscale, d, lin, F, a);  /* +axis lo cell = lin */
             } else {
                 /* hi-side domain boundary, driver.jl:256-267 */
                 face_value(g, &G, U, lin, d, 1, WL);
                 ghost_state(WL, g->bc_hi[d], d, Wg);
                 vo_hllc_flux(WL, Wg, g->gamma, d + 1, F);
                 acc_add(&G, acc, lin, F, a);
-                bflux_capture(&G, bflux, bscale, d, 1, lin, F, a);
+                breg_outer(&G, reg, bscale, d, 1, lin, F, a);
             }
             int64_t nlo = neighbor(g, &G, lin, d, 0);
             if (nlo < 0) {
@@ -352,7 +392,7 @@ void vo_accumulate_flux(const vo_grid *g, const double *U, double *acc, double *
                 face_value(g, &G, U, lin, d, 0, WR);
                 ghost_state(WR, g->bc_lo[d], d, Wg);
                 vo_hllc_flux(Wg, WR, g->gamma, d + 1, F);
-                bflux_capture(&G, bflux, bscale, d, 0, lin, F, a);
+                breg_outer(&G, reg, bscale, d, 0, lin, F, a);
                 acc_add(&G, acc, lin, F, -a);
             }
         }
@@ -491,6 +531,85 @@ void vo_step(const vo_grid *g, double *U, double *u0, double *acc, double dt, do
 #pragma omp parallel for schedule(static) num_threads(nthreads > 0 ? nthreads : omp_get_max_threads()) if (mode == 1)
 #endif
     for (int64_t i = 0; i < n5; ++i) U[i] = 0.5 * u0[i] + 0.5 * (U[i] - invV * acc[i]);
+}
+
+/* step!(sim, dt; bflux = reg) with a register that may record interior
+ * faces (src/driver.jl:333-359, src/reflux.jl:113-146): serial face
+ * enumeration, the register's scale set to 0.5*dt for both stages.  ivals and
+ * the masks may be NULL. */
+void vo_step_breg(const vo_grid *g, double *U, double *u0, double *acc, double dt, double *vals,
+                  unsigned char *seen, double *ivals, unsigned char *iseen)
+{
+    geom_t G;
+    make_geom(g, &G);
+    int64_t n5 = 5 * G.ncell;
+    breg_t r = {vals, ivals, seen, iseen};
+    double bscale = 0.5 * dt;
+    memcpy(u0, U, sizeof(double) * n5);
+    accumulate_flux_reg(g, U, acc, &r, bscale);
+    double invV = dt / (g->aexp * G.vol);
+    for (int64_t i = 0; i < n5; ++i) U[i] = u0[i] - invV * acc[i];
+    accumulate_flux_reg(g, U, acc, &r, bscale);
+    for (int64_t i = 0; i < n5; ++i) U[i] = 0.5 * u0[i] + 0.5 * (U[i] - invV * acc[i]);
+}
+
+/* bflux_plane, src/reflux.jl:171-191.  The lookup closure of the reference's
+ * callers (lib/EnzoLib/test/reflux_common.jl:104-133) becomes `source`: 0 / 1
+ * the outer register's (dim+1, :lo / :hi, I) keys, 2 the interior register's
+ * (dim+1, I) keys; a key the register never captured reads as `nothing`.  R =
+ * ndim; dim is 0-based; start, stop, g0 hold R global indices; out gets
+ * prod(stop - start + 1) values. */
+void vo_bflux_plane(const vo_grid *g, const double *vals, const unsigned char *seen,
+                    const double *ivals, const unsigned char *iseen, int dim, int source,
+                    const int64_t *start, const int64_t *stop, const int64_t *g0, int64_t flux_off,
+                    int comp, double vcell, double *out)
+{
+    geom_t G;
+    make_geom(g, &G);
+    const int R = G.nd;
+    int64_t Dim[3] = {1, 1, 1}, n = 1;
+    for (int d = 0; d < R; ++d) {
+        Dim[d] = stop[d] - start[d] + 1;
+        n *= Dim[d];
+    }
+    for (int64_t lin = 0; lin < n; ++lin) {
+        /* decode column-major (dim-0 fastest) plane offset -> active index */
+        int64_t rem = lin, act[3] = {1, 1, 1};
+        for (int d = 0; d < R; ++d) {
+            int64_t od = rem % Dim[d];
+            rem /= Dim[d];
+            int64_t gi = start[d] + od;
+            act[d] = d == dim ? flux_off : (gi - g0[d] + 1);
+        }
+        /* lookup(I): a captured key of a cell of this grid, else nothing */
+        const double *F = NULL;
+        double Fv[5];
+        int inside = 1;
+        for (int d = 0; d < R; ++d) inside = inside && act[d] >= 1 && act[d] <= G.n[d];
+        if (inside) {
+            int64_t cell = 0, mul = 1;
+            for (int d = 0; d < R; ++d) {
+                cell += (act[d] - 1) * mul;
+                mul *= G.n[d];
+            }
+            if (source == 2) {
+                if (iseen[(int64_t)dim * G.ncell + cell]) {
+                    for (int k = 0; k < 5; ++k) Fv[k] = ivals[((int64_t)dim * 5 + k) * G.ncell + cell];
+                    F = Fv;
+                }
+            } else {
+                int64_t base = bflux_base(&G, dim, source) + bflux_plane_index(&G, cell, dim);
+                /* the key holds the cell itself: only its own side's face */
+                int on_side = act[dim] == (source ? G.n[dim] : 1);
+                if (on_side && seen[base]) {
+                    int64_t P = G.ncell / G.n[dim];
+                    for (int k = 0; k < 5; ++k) Fv[k] = vals[base + k * P];
+                    F = Fv;
+                }
+            }
+        }
+        out[lin] = (F != NULL && comp > 0) ? F[comp - 1] / vcell : 0.0;
+    }
 }
 
 /* evolve!, src/driver.jl:483-508 (single-rate path, no regrid/callback) */

@@ -60,6 +60,12 @@ void vo_accumulate_flux(const vo_grid *g, const double *U, double *acc,
 void vo_accumulate_flux_gather(const vo_grid *g, const double *U, double *acc, int nthreads);
 void vo_step(const vo_grid *g, double *U, double *u0, double *acc, double dt,
              double *bflux, int mode, int nthreads);
+void vo_step_breg(const vo_grid *g, double *U, double *u0, double *acc, double dt, double *vals,
+                  unsigned char *seen, double *ivals, unsigned char *iseen);
+void vo_bflux_plane(const vo_grid *g, const double *vals, const unsigned char *seen,
+                    const double *ivals, const unsigned char *iseen, int dim, int source,
+                    const int64_t *start, const int64_t *stop, const int64_t *g0, int64_t flux_off,
+                    int comp, double vcell, double *out);
 int64_t vo_evolve(const vo_grid *g, double *U, double *u0, double *acc, double tfinal,
                   int64_t max_steps, double *t, int mode, int nthreads);
 void vo_conserved_totals(const vo_grid *g, const double *U, double *out);

@@ -161,3 +161,102 @@ def test_golden_steps_reproduced(oracle, name):
         assert dt == dt_ref
         oracle.step(g, U, dt)
     assert np.array_equal(U, d["U"])
+
+
+def test_interior_register_accounts_for_every_cell(oracle):
+    """With record_interior the register holds every face's time-integrated
+    flux (src/reflux.jl:138-146), so on a periodic box each cell's change
+    over a step is minus the net integrated flux through its faces over its
+    volume (the per-cell form of the conservation identity of
+    test/test_boundary_flux.jl)."""
+    dims = (6, 5, 4)
+    g = oracle.make_grid(dims, [0] * 3, [1] * 3, [1] * 3, [1] * 3, 1.4, 0.4)
+    U = P.initial_state(P.smooth_random_problem(dims, seed=4))
+    U0 = U.copy()
+    reg = oracle.BoundaryFluxRegister(g, record_interior=True)
+    oracle.step_breg(g, U, oracle.compute_dt(g, U), reg)
+    assert reg.iseen.all() and not reg.seen.any()   # periodic: no outer faces
+    nc = U.size // 5
+    R = reg.ivals.reshape(3, 5, *dims[::-1])        # [axis][comp][z][y][x]
+    net = np.zeros((5,) + dims[::-1])
+    for d in range(3):
+        ax = 2 - d                                   # array axis of grid axis d
+        net += R[d] - np.roll(R[d], 1, axis=1 + ax)  # out through hi face, in through lo face
+    V = 1.0 / nc
+    dU = (U - U0).reshape((5,) + dims[::-1])
+    scale = np.abs(U0).reshape((5,) + dims[::-1]).max(axis=(1, 2, 3), keepdims=True)
+    assert np.max(np.abs(dU + net / V) / scale) < 1e-12
+
+
+def _plane_restated(reg, g, dims, dim, source, start, stop, g0, flux_off, comp, vcell):
+    """bflux_plane (src/reflux.jl:171-191) transcribed over Dict registers built
+    from the dense one, with the lookups of lib/EnzoLib/test/reflux_common.jl."""
+    R = len(dims)
+    nc = int(np.prod(dims))
+    flux, interior = {}, {}
+    P_ = lambda d: nc // dims[d]
+    base = 0
+    for d in range(R):
+        for side in (0, 1):
+            for idx in range(P_(d)):
+                if reg.seen[base + idx]:
+                    rest, mul, cell = idx, 1, [0] * R
+                    for e in range(R):
+                        if e == d:
+                            continue
+                        cell[e] = rest % dims[e]
+                        rest //= dims[e]
+                    cell[d] = 0 if side == 0 else dims[d] - 1
+                    key = (d + 1, "lo" if side == 0 else "hi", tuple(c + 1 for c in cell))
+                    flux[key] = [reg.vals[base + k * P_(d) + idx] for k in range(5)]
+            base += 5 * P_(d)
+    if reg.ivals is not None:
+        for d in range(R):
+            for lin in range(nc):
+                if reg.iseen[d * nc + lin]:
+                    cell, rest = [], lin
+                    for e in range(R):
+                        cell.append(rest % dims[e] + 1)
+                        rest //= dims[e]
+                    interior[(d + 1, tuple(cell))] = [reg.ivals[(d * 5 + k) * nc + lin] for k in range(5)]
+    ax = dim + 1
+    if source == 2:
+        lookup = lambda I: interior.get((ax, I))
+    else:
+        lookup = lambda I: flux.get((ax, "lo" if source == 0 else "hi", I))
+    D = [stop[d] - start[d] + 1 for d in range(R)]
+    out = []
+    for lin in range(int(np.prod(D))):
+        rem, act = lin, []
+        for d in range(R):
+            od = rem % D[d]
+            rem //= D[d]
+            act.append(flux_off if d == dim else start[d] + od - g0[d] + 1)
+        F = lookup(tuple(act))
+        out.append(F[comp - 1] / vcell if (F is not None and comp > 0) else 0.0)
+    return np.array(out)
+
+
+def test_bflux_plane_matches_a_dict_restatement(oracle):
+    dims = (6, 5, 4)
+    g = oracle.make_grid(dims, [0] * 3, [1] * 3, [0, 2, 1], [2, 0, 1], 1.4, 0.4)
+    U = P.initial_state(P.smooth_random_problem(dims, seed=21))
+    reg = oracle.BoundaryFluxRegister(g, record_interior=True)
+    for _ in range(2):
+        oracle.step_breg(g, U, oracle.compute_dt(g, U), reg)
+    g0 = (11, 21, 31)  # the grid's first active cell in global indices
+    cases = [
+        (0, 0, (11, 21, 31), (11, 25, 34), 1, 1), (0, 1, (16, 21, 31), (16, 25, 34), 6, 2),
+        (1, 0, (11, 21, 31), (16, 21, 34), 1, 5), (1, 1, (11, 25, 31), (16, 25, 34), 5, 3),
+        (2, 0, (11, 21, 31), (16, 25, 31), 1, 1),                  # periodic axis: nothing recorded
+        (0, 0, (11, 19, 30), (11, 26, 35), 1, 4),                  # plane wider than the grid
+        (0, 1, (16, 21, 31), (16, 25, 34), 3, 2),                  # flux_off off the boundary cell
+        (0, 2, (13, 21, 31), (13, 25, 34), 2, 1), (2, 2, (11, 21, 34), (16, 25, 34), 4, 5),
+        (1, 2, (11, 25, 31), (16, 25, 34), 5, 2),                  # hi y is a wall: no interior key
+        (0, 0, (11, 21, 31), (11, 25, 34), 1, 0),                  # comp 0: zeros
+    ]
+    for dim, src, st, sp, off, comp in cases:
+        got = oracle.bflux_plane(g, reg, dim, src, st, sp, g0, off, comp, 0.125)
+        ref = _plane_restated(reg, g, dims, dim, src, st, sp, g0, off, comp, 0.125)
+        assert np.array_equal(got, ref), (dim, src, st, sp, off, comp)
+    assert np.any(oracle.bflux_plane(g, reg, 0, 0, (11, 21, 31), (11, 25, 34), g0, 1, 1, 0.125))

@@ -39,6 +39,21 @@ int use(vb_ctx *ctx)
     return VB_OK;
 }
 
+int ctx_scratch(vb_ctx *ctx, size_t bytes, void **out)
+{
+    if (bytes > ctx->scratch_bytes) {
+        // the previous buffer may still be read by queued work
+        VB_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (ctx->scratch) cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+        VB_CUDA(cudaMalloc(&ctx->scratch, bytes));
+        ctx->scratch_bytes = bytes;
+    }
+    *out = ctx->scratch;
+    return VB_OK;
+}
+
 }  // namespace detail
 }  // namespace vb
 
@@ -276,31 +291,37 @@ int sync_box(vb_grid *gr)
 int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout)
 {
     double *bf = gr->bflux_on ? gr->bflux : nullptr;
+    double *bfi = bf && gr->bflux_interior ? gr->bflux + gr->bflux_outer_n : nullptr;
     const bool grav = gr->grav != nullptr;  // self-gravity: 3D tiled kernels carry the source
-    if (gr->tiled && !bf && (!grav || gr->g.nd == 3)) {
+    // the tiled kernels record outer boundary fluxes themselves; interior
+    // faces, and boundary fluxes together with gravity, take the cell kernel
+    if (gr->tiled && !bfi && !(bf && grav) && (!grav || gr->g.nd == 3)) {
         int rc = sync_box(gr);
         if (rc) return rc;
+        gr->box.bflux = bf;
         const int64_t items = box_items(gr->g, gr->kz, grid_taper(gr));
         if (items > 0x7fffffff) return fail(VB_ENOTSUP, "too many tiled work items");
         unsigned int *work = gr->ctrl->work;  // device address of the cursors
         if (gr->g.nd == 2) {
             int n2 = gr->precision == VB_MIXED
-                         ? vb::launch_stage_tiled2d_mixed(&gr->box, (int)items, work, st, gr->ctx->stream)
-                         : vb::launch_stage_tiled2d_fp64(&gr->box, (int)items, work, st, gr->ctx->stream);
+                         ? vb::launch_stage_tiled2d_mixed(&gr->box, (int)items, work, st,
+                                                          gr->ctx->stream, bf != nullptr)
+                         : vb::launch_stage_tiled2d_fp64(&gr->box, (int)items, work, st,
+                                                         gr->ctx->stream, bf != nullptr);
             VB_CHECK_LAUNCH(gr->ctx, n2);
             return VB_OK;
         }
         int n = gr->precision == VB_MIXED
                     ? vb::launch_stage_tiled3d_mixed(&gr->box, nullptr, nullptr, (int)items, work,
-                                                     st, gr->ctx->stream, grav)
+                                                     st, gr->ctx->stream, grav, bf != nullptr)
                     : vb::launch_stage_tiled3d_fp64(&gr->box, nullptr, nullptr, (int)items, work,
-                                                    st, gr->ctx->stream, grav);
+                                                    st, gr->ctx->stream, grav, bf != nullptr);
         VB_CHECK_LAUNCH(gr->ctx, n);
         return VB_OK;
     }
     int n = gr->precision == VB_MIXED
-                ? vb::launch_stage_mixed(gr->g, st, Uin, U0, Uout, gr->ctrl, bf, gr->ctx->stream)
-                : vb::launch_stage_fp64(gr->g, st, Uin, U0, Uout, gr->ctrl, bf, gr->ctx->stream);
+                ? vb::launch_stage_mixed(gr->g, st, Uin, U0, Uout, gr->ctrl, bf, gr->ctx->stream, bfi)
+                : vb::launch_stage_fp64(gr->g, st, Uin, U0, Uout, gr->ctrl, bf, gr->ctx->stream, bfi);
     VB_CHECK_LAUNCH(gr->ctx, n);
     return VB_OK;
 }
@@ -359,7 +380,7 @@ constexpr int64_t GRAPH_STEPS = 8;
 uint64_t graph_key(const vb_grid *gr)
 {
     return (gr->tiled ? 1u : 0u) | (gr->bflux_on ? 2u : 0u) | (grid_taper(gr) ? 4u : 0u) |
-           ((uint64_t)gr->kz << 3);
+           (gr->bflux_interior ? 8u : 0u) | ((uint64_t)gr->kz << 4);
 }
 
 // Capture GRAPH_STEPS steps into the grid's graph for its current configuration.
@@ -557,14 +578,10 @@ int vb_hllc_faces(vb_ctx *ctx, int64_t nf, const double *WL, const double *WR,
     const size_t bw = sizeof(double) * 5 * (size_t)nf;
     const size_t ba = sizeof(int32_t) * (size_t)nf;
     const size_t need = 3 * bw + ((ba + 255) & ~(size_t)255);
-    if (need > ctx->scratch_bytes) {
-        if (ctx->scratch) cudaFree(ctx->scratch);
-        ctx->scratch = nullptr;
-        ctx->scratch_bytes = 0;
-        VB_CUDA(cudaMalloc(&ctx->scratch, need));
-        ctx->scratch_bytes = need;
-    }
-    char *base = (char *)ctx->scratch;
+    void *scratch = nullptr;
+    rc = vb::detail::ctx_scratch(ctx, need, &scratch);
+    if (rc) return rc;
+    char *base = (char *)scratch;
     double *dWL = (double *)base;
     double *dWR = (double *)(base + bw);
     double *dF = (double *)(base + 2 * bw);
@@ -996,29 +1013,91 @@ int vb_grid_profile_step(vb_grid *gr, int nsteps, double *ms_fin, double *ms_s1,
     return VB_OK;
 }
 
+namespace {
+int64_t bflux_outer_size(const vb::Geom &g)
+{
+    int64_t s = 0;
+    for (int a = 0; a < g.nd; ++a) s += 2 * 5 * (g.ncell / g.n[a]);
+    return s;
+}
+}  // namespace
+
 int vb_bflux_size(const vb_grid *gr, int64_t *n)
 {
     if (!gr || !n) return fail(VB_EINVAL, "null argument");
-    int64_t s = 0;
-    for (int a = 0; a < gr->g.nd; ++a) s += 2 * 5 * (gr->g.ncell / gr->g.n[a]);
-    *n = s;
+    *n = gr->bflux ? gr->bflux_n : bflux_outer_size(gr->g);
     return VB_OK;
 }
 
 int vb_bflux_enable(vb_grid *gr, int enable)
 {
     if (!gr) return fail(VB_EINVAL, "null grid");
+    if (enable < VB_BFLUX_OFF || enable > VB_BFLUX_INTERIOR)
+        return fail(VB_EINVAL, "enable must be VB_BFLUX_OFF, VB_BFLUX_OUTER or VB_BFLUX_INTERIOR");
     int rc = use(gr->ctx);
     if (rc) return rc;
-    if (enable && !gr->bflux) {
-        int64_t n = 0;
-        vb_bflux_size(gr, &n);
-        VB_CUDA(cudaMalloc(&gr->bflux, sizeof(double) * (size_t)n));
+    const bool interior = enable == VB_BFLUX_INTERIOR;
+    if (enable != VB_BFLUX_OFF && (!gr->bflux || interior != gr->bflux_interior)) {
+        // (re)allocate the register for this layout, zeroed
+        const int64_t outer = bflux_outer_size(gr->g);
+        const int64_t n = outer + (interior ? (int64_t)gr->g.nd * 5 * gr->g.ncell : 0);
+        double *p = nullptr;
+        VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
+        VB_CUDA(cudaMalloc(&p, sizeof(double) * (size_t)n));
+        cudaFree(gr->bflux);
+        gr->bflux = p;
         gr->bflux_n = n;
+        gr->bflux_outer_n = outer;
+        gr->bflux_interior = interior;
         VB_CUDA(cudaMemsetAsync(gr->bflux, 0, sizeof(double) * (size_t)n, gr->ctx->stream));
         VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
     }
-    gr->bflux_on = enable != 0;
+    gr->bflux_on = enable != VB_BFLUX_OFF;
+    return VB_OK;
+}
+
+int vb_bflux_plane(vb_grid *gr, int dim, int source, const int64_t *start, const int64_t *stop,
+                   const int64_t *g0, int64_t flux_off, int comp, double vcell, double *out,
+                   int64_t n)
+{
+    if (!gr || !start || !stop || !g0 || (!out && n > 0)) return fail(VB_EINVAL, "null argument");
+    if (!gr->bflux) return fail(VB_EINVAL, "boundary-flux register not enabled");
+    const int R = gr->g.nd;
+    if (dim < 0 || dim >= R) return fail(VB_EINVAL, "dim must be in 0..ndim-1");
+    if (source < VB_BFLUX_PLANE_LO || source > VB_BFLUX_PLANE_INTERIOR)
+        return fail(VB_EINVAL, "unknown plane source");
+    if (source == VB_BFLUX_PLANE_INTERIOR && !gr->bflux_interior)
+        return fail(VB_EINVAL, "the register does not record interior faces (VB_BFLUX_INTERIOR)");
+    if (comp > 5) return fail(VB_EINVAL, "comp must be at most 5 (comp <= 0 gives zeros)");
+    int64_t cnt = 1;
+    for (int d = 0; d < R; ++d) {
+        if (stop[d] < start[d]) return fail(VB_EINVAL, "stop must not be below start");
+        cnt *= stop[d] - start[d] + 1;
+    }
+    if (n != cnt) return fail(VB_EINVAL, "n must equal the plane's cell count");
+    if (n == 0) return VB_OK;
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    double *d_out = nullptr;
+    rc = vb::detail::ctx_scratch(gr->ctx, sizeof(double) * (size_t)n, (void **)&d_out);
+    if (rc) return rc;
+    vb::PlaneSpec ps{};
+    ps.R = R;
+    ps.dim = dim;
+    ps.source = source;
+    for (int d = 0; d < R; ++d) {
+        ps.start[d] = start[d];
+        ps.dims[d] = stop[d] - start[d] + 1;
+        ps.g0[d] = g0[d];
+    }
+    ps.flux_off = flux_off;
+    ps.comp = comp;
+    ps.vcell = vcell;
+    VB_CHECK_LAUNCH(gr->ctx, vb::launch_bflux_plane(gr->g, gr->bflux, gr->bflux_outer_n, ps, d_out, n,
+                                                    gr->ctx->stream));
+    VB_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost,
+                            gr->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(gr->ctx->stream));
     return VB_OK;
 }
 

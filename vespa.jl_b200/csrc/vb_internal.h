@@ -29,9 +29,11 @@ struct vb_grid {
     double *partials = nullptr;
     double *totals = nullptr;
     double *htot = nullptr;     // pinned
-    double *bflux = nullptr;
-    int64_t bflux_n = 0;
+    double *bflux = nullptr;            // outer planes, then (interior) the [axis][5][ncell] block
+    int64_t bflux_n = 0;                // doubles allocated
+    int64_t bflux_outer_n = 0;          // doubles of the outer planes
     bool bflux_on = false;
+    bool bflux_interior = false;        // the register also records interior faces
     bool invdt_valid = false;   // ctrl->invdt_bits holds the CFL max of the current state
     bool tiled = false;         // the tiled 3D kernels apply to this grid
     int kz = 64;                // z planes per tiled work item
@@ -68,6 +70,10 @@ int default_kz(const Geom &g);
 // automatic kernel choice and default chunk of a single grid
 bool tiled_auto(const Geom &g);
 int grid_default_kz(const Geom &g);
+
+// Context-owned device staging buffer of at least `bytes` (grown with
+// cudaMalloc; reused across calls on the context's stream).
+int ctx_scratch(vb_ctx *ctx, size_t bytes, void **out);
 
 // Grid stepping helpers shared with the adjoint (vb_api.cu).
 int grid_ensure_cfl(vb_grid *gr);   // CFL max of the current state, if stale

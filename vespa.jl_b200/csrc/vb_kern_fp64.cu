@@ -18,12 +18,13 @@ namespace {
 
 template <int ND, int STAGE>
 int launch_generic(const Geom &g, const double *Uin, const double *U0, double *Uout, Ctrl *ctrl,
-                   double *bflux, cudaStream_t s)
+                   double *bflux, double *bflux_int, cudaStream_t s)
 {
     const int bs = 256;
     const int64_t nb = (g.ncell + bs - 1) / bs;
     if (nb <= 0 || nb > 0x7fffffffLL) return -1;
-    k_stage_generic<double, ND, STAGE><<<(unsigned)nb, bs, 0, s>>>(g, Uin, U0, Uout, ctrl, bflux);
+    k_stage_generic<double, ND, STAGE><<<(unsigned)nb, bs, 0, s>>>(g, Uin, U0, Uout, ctrl, bflux,
+                                                                   bflux_int);
     return 1;
 }
 
@@ -148,29 +149,30 @@ __global__ void __launch_bounds__(256) k_hllc_faces(int64_t nf, const double *__
 }  // namespace
 
 int launch_stage_fp64(const Geom &g, int stage, const double *Uin, const double *U0,
-                      double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s)
+                      double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s, double *bflux_int)
 {
     switch (g.nd * 10 + stage) {
-    case 11: return launch_generic<1, 1>(g, Uin, U0, Uout, ctrl, bflux, s);
-    case 12: return launch_generic<1, 2>(g, Uin, U0, Uout, ctrl, bflux, s);
-    case 21: return launch_generic<2, 1>(g, Uin, U0, Uout, ctrl, bflux, s);
-    case 22: return launch_generic<2, 2>(g, Uin, U0, Uout, ctrl, bflux, s);
-    case 31: return launch_generic<3, 1>(g, Uin, U0, Uout, ctrl, bflux, s);
-    case 32: return launch_generic<3, 2>(g, Uin, U0, Uout, ctrl, bflux, s);
+    case 11: return launch_generic<1, 1>(g, Uin, U0, Uout, ctrl, bflux, bflux_int, s);
+    case 12: return launch_generic<1, 2>(g, Uin, U0, Uout, ctrl, bflux, bflux_int, s);
+    case 21: return launch_generic<2, 1>(g, Uin, U0, Uout, ctrl, bflux, bflux_int, s);
+    case 22: return launch_generic<2, 2>(g, Uin, U0, Uout, ctrl, bflux, bflux_int, s);
+    case 31: return launch_generic<3, 1>(g, Uin, U0, Uout, ctrl, bflux, bflux_int, s);
+    case 32: return launch_generic<3, 2>(g, Uin, U0, Uout, ctrl, bflux, bflux_int, s);
     default: return -1;
     }
 }
 
 int launch_stage_tiled2d_fp64(const BoxDesc *hbox, int nitems, unsigned int *work, int stage,
-                              cudaStream_t s)
+                              cudaStream_t s, bool bf)
 {
-    return launch_tiled2d<false, 2>(hbox, nitems, work, stage, s);
+    return launch_tiled2d<false, 2>(hbox, nitems, work, stage, s, bf);
 }
 
 int launch_stage_tiled3d_fp64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
-                              int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav)
+                              int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav,
+                              bool bf)
 {
-    return launch_tiled3d_f64<2>(hbox, boxes, item_box, nitems, work, stage, s, grav);
+    return launch_tiled3d_f64<2>(hbox, boxes, item_box, nitems, work, stage, s, grav, bf);
 }
 
 namespace {

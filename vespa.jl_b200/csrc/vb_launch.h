@@ -26,6 +26,7 @@ struct alignas(64) BoxDesc {
     Geom g;
     double *U, *U1;
     Ctrl *ctrl;
+    double *bflux;  // boundary-flux planes being recorded, or null
     int kz;       // z planes per work item (3D: of the leading chunks, see chunk_span)
     int nchu;     // 3D: chunks of kz planes
     int nch;      // 3D: z chunks in all
@@ -92,8 +93,11 @@ inline bool tiled_supported(const Geom &g) { return tiled3d_supported(g) || tile
 inline int64_t march_extent(const Geom &g) { return g.nd == 3 ? g.n[2] : g.n[1]; }
 
 // vb_kern_fp64.cu (compiled with -fmad=false)
+// bflux: the outer boundary-flux planes being recorded (or null); bflux_int:
+// the interior face register [axis][5][ncell] (or null).
 int launch_stage_fp64(const Geom &g, int stage, const double *Uin, const double *U0,
-                      double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s);
+                      double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s,
+                      double *bflux_int = nullptr);
 int launch_cfl(const Geom &g, const double *U, Ctrl *ctrl, cudaStream_t s);
 int launch_finalize_cfl(const Geom &g, Ctrl *ctrl, cudaStream_t s);
 int launch_set_dt(const Geom &g, Ctrl *ctrl, double dt, cudaStream_t s);
@@ -108,14 +112,17 @@ int launch_hllc_faces(int64_t nf, const double *WL, const double *WR, const int3
 // device box table `boxes` with `item_box` mapping each global work item to
 // its box.  `work` holds the two stage cursors (reset by the dt kernels).
 // grav: the self-gravity source and free-fall dt term (single boxes only).
+// bf: also record the domain-boundary face fluxes into hbox->bflux (single
+// boxes without gravity).
 int launch_stage_tiled3d_fp64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
                               int nitems, unsigned int *work, int stage, cudaStream_t s,
-                              bool grav = false);
-// Tiled 2D stage (single box by value).
+                              bool grav = false, bool bf = false);
+// Tiled 2D stage (single box by value); bf: also record the domain-boundary
+// face fluxes into hbox->bflux.
 int launch_stage_tiled2d_fp64(const BoxDesc *hbox, int nitems, unsigned int *work, int stage,
-                              cudaStream_t s);
+                              cudaStream_t s, bool bf = false);
 int launch_stage_tiled2d_mixed(const BoxDesc *hbox, int nitems, unsigned int *work, int stage,
-                               cudaStream_t s);
+                               cudaStream_t s, bool bf = false);
 // Per-box dt finalisation (evolve!'s loop head) and clock advance for a table.
 int launch_finalize_boxes(const BoxDesc *boxes, int nbox, unsigned int *work, cudaStream_t s);
 int launch_advance_boxes(const BoxDesc *boxes, int nbox, cudaStream_t s);
@@ -128,9 +135,10 @@ int launch_wait_selftest(Ctrl *ctrl, uint64_t limit_ns, cudaStream_t s);
 // vb_kern_mixed.cu
 int launch_stage_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
                                int nitems, unsigned int *work, int stage, cudaStream_t s,
-                               bool grav = false);
+                               bool grav = false, bool bf = false);
 int launch_stage_mixed(const Geom &g, int stage, const double *Uin, const double *U0,
-                       double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s);
+                       double *Uout, Ctrl *ctrl, double *bflux, cudaStream_t s,
+                       double *bflux_int = nullptr);
 
 // vb_adjoint_kern.cu (periodic meshes, float64): one adjoint RK2 stage,
 //   out = 0.5*lam + (M ? M : 0) - invV * (dD/dU)^T mu,  mu = M ? M : 0.5*lam,
@@ -140,6 +148,21 @@ int launch_adj_stage(const Geom &g, const double *U, const double *lam, const do
                      cudaStream_t s);
 // dts[ctrl->step - step0] = ctrl->dt while the step in flight is active
 int launch_record_dt(const Ctrl *ctrl, double *dts, int64_t step0, int64_t cap, cudaStream_t s);
+
+// bflux_plane raster request (src/reflux.jl:171-191): the plane [start,
+// start + dims) in global indices, the grid's first active cell g0, the
+// active index used along the flux axis, the 1-based component and the cell
+// volume; source picks the lo or hi outer planes or the interior register.
+struct PlaneSpec {
+    int R, dim, source, comp;
+    int64_t start[3], dims[3], g0[3];
+    int64_t flux_off;
+    double vcell;
+};
+// vb_bflux.cu: rasterise one plane from the register (outer planes of
+// `outer_n` doubles, then the interior block) into n doubles at d_out.
+int launch_bflux_plane(const Geom &g, const double *bflux, int64_t outer_n, const PlaneSpec &ps,
+                       double *d_out, int64_t n, cudaStream_t s);
 
 constexpr int TOTALS_PARTS = 1024;  // fixed partial count: deterministic sum order
 

@@ -141,7 +141,7 @@ __device__ __forceinline__ int64_t bflux_offset(const Geom &g, int ax, int side,
 template <typename T, int ND, int STAGE>
 __global__ void __launch_bounds__(256)
 k_stage_generic(Geom g, const double *__restrict__ Uin, const double *U0, double *Uout,
-                Ctrl *ctrl, double *bflux)
+                Ctrl *ctrl, double *bflux, double *bflux_int)
 {
     __shared__ double red[32];
     if (!ctrl->active) return;
@@ -195,6 +195,19 @@ k_stage_generic(Geom g, const double *__restrict__ Uin, const double *U0, double
                 un[k] = 0.5 * U0[i] + 0.5 * (Uin[i] - invV * acc[k]);
             }
             Uout[i] = un[k];
+        }
+
+        // interior faces (src/reflux.jl:138-146, _flux_face! src/driver.jl:251):
+        // the cell's hi face on each axis when the hi neighbour is a cell
+        // (periodic wrap included), keyed by this lo cell: [axis][5][ncell]
+        if (bflux_int) {
+            const double scale = 0.5 * ctrl->dt;
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                if (af[d].hi_bnd) continue;
+                double *o = bflux_int + (int64_t)d * 5 * g.ncell + lin;
+                for (int k = 0; k < 5; ++k) o[k * g.ncell] += scale * double(af[d].hi[k]) * g.area[d];
+            }
         }
 
         // boundary-flux register capture, src/reflux.jl:125-132

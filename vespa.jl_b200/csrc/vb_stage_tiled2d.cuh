@@ -56,7 +56,7 @@ struct Smem {
 
 }  // namespace t2
 
-template <bool MIXED, int NS, int STAGE>
+template <bool MIXED, int NS, int STAGE, bool BF = false>
 __global__ void __launch_bounds__(256, 2)
 k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *work)
 {
@@ -90,6 +90,12 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
     const float gf = (float)gamma, ig1 = 1.0f / ((float)gamma - 1.0f);
     const double ax = g.area[0], ay = g.area[1];
     const T half = T(0.5), mhalf = T(-0.5);
+    const double bscale = BF ? 0.5 * ctrl->dt : 0.0;  // boundary-flux stage weight
+    // boundary-flux capture of a solved domain face (axis d, side, plane entry)
+    auto capture = [&](int d, int side, int64_t idx, const T F[5]) {
+        const double Fd[5] = {(double)F[0], (double)F[1], (double)F[2], (double)F[3], (double)F[4]};
+        bflux_add(g, B.bflux, d, side, idx, bscale, g.area[d], Fd);
+    };
 
     // float32 slopes use the clamp form of minmod (t3m::mm), float64 the reference's
     auto slope = [](T l, T c, T r) -> T {
@@ -232,6 +238,9 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
         } else {
             hllc_flux<double, 2>(yl, loy, gamma, Fylo);
         }
+        if constexpr (BF) {
+            if (gl) capture(1, 0, x0 + t, Fylo);  // y-lo domain face of cell (x, 0)
+        }
     }
 
     const int gxc = x0 + t;
@@ -340,6 +349,10 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
             hllc_flux<double, 1>(Lx, Rx, gamma, Fx);
             hllc_flux<double, 2>(hy, yr, gamma, Fyhi);
         }
+        if constexpr (BF) {
+            if (t == 0 && xlo_bnd) capture(0, 0, r, Fx);                // x-lo face of (0, r)
+            if (!pery && r + 1 >= ny) capture(1, 1, x0 + t, Fyhi);     // y-hi face of (x, ny-1)
+        }
 #pragma unroll
         for (int f = 0; f < 5; ++f) S.gx[f][t] = ax * (double)Fx[f];
         if (t == TX - 1) {  // the segment's right edge face
@@ -368,6 +381,9 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
             }
 #pragma unroll
             for (int f = 0; f < 5; ++f) S.gx[f][TX] = ax * (double)F2[f];
+            if constexpr (BF) {
+                if (xhi_bnd) capture(0, 1, r, F2);  // x-hi face of (nx-1, r)
+            }
         }
         __syncthreads();  // (3) x fluxes ready
 
@@ -431,15 +447,24 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
 }
 
 template <bool MIXED, int NS>
-int launch_tiled2d(const BoxDesc *hbox, int nitems, unsigned int *work, int stage, cudaStream_t s)
+int launch_tiled2d(const BoxDesc *hbox, int nitems, unsigned int *work, int stage, cudaStream_t s,
+                   bool bf)
 {
     using T = typename std::conditional<MIXED, float, double>::type;
     const size_t smem = sizeof(t2::Smem<T, NS>);
-    static int res = 0;
+    static int res = 0, resf = 0;
     if (!res) res = persistent_blocks(k_stage_tiled2d<MIXED, NS, 1>, k_stage_tiled2d<MIXED, NS, 2>, smem);
-    if (res <= 0 || nitems <= 0 || !hbox) return -1;
-    const unsigned grid = (unsigned)(nitems < res ? nitems : res);
-    if (stage == 1)
+    if (!resf) resf = persistent_blocks(k_stage_tiled2d<MIXED, NS, 1, true>,
+                                        k_stage_tiled2d<MIXED, NS, 2, true>, smem);
+    if (!hbox || (bf && !hbox->bflux)) return -1;
+    const int resident = bf ? resf : res;
+    if (resident <= 0 || nitems <= 0) return -1;
+    const unsigned grid = (unsigned)(nitems < resident ? nitems : resident);
+    if (bf && stage == 1)
+        k_stage_tiled2d<MIXED, NS, 1, true><<<grid, t2::NT, smem, s>>>(*hbox, nitems, work);
+    else if (bf)
+        k_stage_tiled2d<MIXED, NS, 2, true><<<grid, t2::NT, smem, s>>>(*hbox, nitems, work);
+    else if (stage == 1)
         k_stage_tiled2d<MIXED, NS, 1><<<grid, t2::NT, smem, s>>>(*hbox, nitems, work);
     else
         k_stage_tiled2d<MIXED, NS, 2><<<grid, t2::NT, smem, s>>>(*hbox, nitems, work);

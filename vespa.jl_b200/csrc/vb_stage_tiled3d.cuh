@@ -101,6 +101,21 @@ __device__ __noinline__ void stage_abandon(uint64_t *bars, int qb, int q, int np
     atomicOr(&ctrl->flags, CTRL_F_TIMEOUT);
 }
 
+// _bflux_capture!, src/reflux.jl:125-132, for the tiled kernels: the thread
+// that solved domain-boundary face (axis d, side) adds (scale * F) * area to
+// entry `idx` of that plane (the other axes column-major, lowest fastest).
+// Each entry belongs to one face, hence to one thread of the launch.
+static __device__ __noinline__ void bflux_add(const Geom &g, double *bf, int d, int side, int64_t idx,
+                                       double scale, double area, const double F[5])
+{
+    int64_t off = 0;
+    for (int e = 0; e < d; ++e) off += 2 * 5 * (g.ncell / g.n[e]);
+    const int64_t P = g.ncell / g.n[d];
+    off += (int64_t)side * 5 * P + idx;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) bf[off + k * P] += scale * F[k] * area;
+}
+
 __device__ __forceinline__ int lo_class(int64_t c, int64_t n, bool periodic)
 {
     if (c > 0) return LO_BEFORE;

@@ -54,7 +54,7 @@ __device__ __forceinline__ void face_states(const double *wk, const int o[4], do
 
 }  // namespace t3d
 
-template <int NS, int STAGE, bool BATCH, bool GRAV = false>
+template <int NS, int STAGE, bool BATCH, bool GRAV = false, bool BF = false>
 __global__ void __launch_bounds__(256, 2)
 k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restrict__ boxes,
                     const int *__restrict__ item_box, int nitems, unsigned int *work)
@@ -111,6 +111,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
     const bool perz = g.bc_lo[2] == BC_PERIODIC;
     const double gamma = g.gamma;
     const double invV = ctrl->invV;
+    const double bscale = BF ? 0.5 * ctrl->dt : 0.0;  // boundary-flux stage weight
     const double ax = g.area[0], ay = g.area[1], az = g.area[2];
     const int bx_lo = g.bc_lo[0], bx_hi = g.bc_hi[0], by_lo = g.bc_lo[1], by_hi = g.bc_hi[1];
     const int bz_lo = g.bc_lo[2], bz_hi = g.bc_hi[2];
@@ -246,6 +247,8 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
             double gst[5];
             ghost_state<double>(loz, bz_lo, 2, gst);
             tiled_hllc<3>(gst, loz, gamma, Fzlo);
+            if constexpr (BF)  // z-lo domain face of cell (x, y, 0)
+                bflux_add(g, B.bflux, 2, 0, (int64_t)(x0 + tx) + (int64_t)nx * (y0 + ty), bscale, az, Fzlo);
         } else {
             const bool gll = !perz && k0 - 2 < 0;
             double hzm[5];
@@ -278,23 +281,35 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
             for (int f = 0; f < 5; ++f) hz1[f] = hz[f];
         }
         tiled_hllc<3>(hz, zr, gamma, Fzhi);
+        if constexpr (BF) {
+            if (!perz && k + 1 >= nz)  // z-hi domain face of cell (x, y, nz-1)
+                bflux_add(g, B.bflux, 2, 1, (int64_t)(x0 + tx) + (int64_t)nx * (y0 + ty), bscale, az, Fzhi);
+        }
 #pragma unroll
         for (int f = 0; f < 5; ++f) hz[f] = hz1[f];
     };
     // the own lo x face and lo y face of plane k (ring slot w0)
-    auto xy_faces = [&](const double *w0) {
+    auto xy_faces = [&](const double *w0, int k) {
         double L[5], R[5], F[5];
         face_states(w0, ox, L, R);
         tiled_hllc<1>(L, R, gamma, F);
 #pragma unroll
         for (int f = 0; f < 5; ++f) S.gx[f][ty * (TX + 1) + tx] = ax * F[f];
+        if constexpr (BF) {
+            if (xlo_bnd && tx == 0)  // x-lo domain face of cell (0, y, k)
+                bflux_add(g, B.bflux, 0, 0, (int64_t)(y0 + ty) + (int64_t)ny * k, bscale, ax, F);
+        }
         face_states(w0, oy, L, R);
         tiled_hllc<2>(L, R, gamma, F);
 #pragma unroll
         for (int f = 0; f < 5; ++f) S.gy[f][ty * TX + tx] = ay * F[f];
+        if constexpr (BF) {
+            if (ylo_bnd && ty == 0)  // y-lo domain face of cell (x, 0, k)
+                bflux_add(g, B.bflux, 1, 0, (int64_t)(x0 + tx) + (int64_t)nx * k, bscale, ay, F);
+        }
     };
     // the hi-edge faces: x at fx = TX (warp 7) or y at fy = TY (warp 6), lanes < 16
-    auto edge_face = [&](const double *w0) {
+    auto edge_face = [&](const double *w0, int k) {
         const int j = lane;
         double L[5], R[5], F[5];
         if (warp == 7) {
@@ -303,12 +318,20 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
             tiled_hllc<1>(L, R, gamma, F);
 #pragma unroll
             for (int f = 0; f < 5; ++f) S.gx[f][j * (TX + 1) + TX] = ax * F[f];
+            if constexpr (BF) {
+                if (xhi_bnd)  // x-hi domain face of cell (nx-1, y0+j, k)
+                    bflux_add(g, B.bflux, 0, 1, (int64_t)(y0 + j) + (int64_t)ny * k, bscale, ax, F);
+            }
         } else {
             const int ey[4] = {wrow(j, TY - 2), wrow(j, TY - 1), wrow(j, TY), wrow(j, TY + 1)};
             face_states(w0, ey, L, R);
             tiled_hllc<2>(L, R, gamma, F);
 #pragma unroll
             for (int f = 0; f < 5; ++f) S.gy[f][TY * TX + j] = ay * F[f];
+            if constexpr (BF) {
+                if (yhi_bnd)  // y-hi domain face of cell (x0+j, ny-1, k)
+                    bflux_add(g, B.bflux, 1, 1, (int64_t)(x0 + j) + (int64_t)nx * k, bscale, ay, F);
+            }
         }
     };
 
@@ -352,14 +375,14 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
         // ---- phase 2: the own lo x / lo y faces; the z face (warps 0..3) or
         //      a hi-edge face (warps 6, 7) ----
         if (z_early) {
-            xy_faces(w0);
-            if (warp >= 6 && lane < 16) edge_face(w0);
+            xy_faces(w0, k);
+            if (warp >= 6 && lane < 16) edge_face(w0, k);
         } else {
             double W2[5];
 #pragma unroll
             for (int f = 0; f < 5; ++f) W2[f] = w2[o_c + f * PC];
             zsolve(k, w0 + o_c, w1 + o_c, W2, Fzhi);
-            xy_faces(w0);
+            xy_faces(w0, k);
         }
         __syncthreads();  // (2) fluxes ready
 
@@ -435,18 +458,23 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
 
 template <int NS>
 int launch_tiled3d_f64(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
-                       int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav)
+                       int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav,
+                       bool bf)
 {
     const size_t smem = sizeof(t3d::Smem<NS>);
-    static int res1 = 0, resb = 0, resg = 0;
+    static int res1 = 0, resb = 0, resg = 0, resf = 0;
     if (!res1) res1 = persistent_blocks(k_stage_tiled3d_f64<NS, 1, false>,
                                         k_stage_tiled3d_f64<NS, 2, false>, smem);
     if (!resb) resb = persistent_blocks(k_stage_tiled3d_f64<NS, 1, true>,
                                         k_stage_tiled3d_f64<NS, 2, true>, smem);
     if (!resg) resg = persistent_blocks(k_stage_tiled3d_f64<NS, 1, false, true>,
                                         k_stage_tiled3d_f64<NS, 2, false, true>, smem);
-    if (grav && !hbox) return -1;  // gravity: single boxes only
-    const int resident = grav ? resg : hbox ? res1 : resb;
+    if (!resf) resf = persistent_blocks(k_stage_tiled3d_f64<NS, 1, false, false, true>,
+                                        k_stage_tiled3d_f64<NS, 2, false, false, true>, smem);
+    if ((grav || bf) && !hbox) return -1;  // gravity, boundary fluxes: single boxes only
+    if (grav && bf) return -1;
+    if (bf && !hbox->bflux) return -1;
+    const int resident = grav ? resg : bf ? resf : hbox ? res1 : resb;
     if (resident <= 0 || nitems <= 0) return -1;
     const unsigned grid = (unsigned)(nitems < resident ? nitems : resident);
     BoxDesc box0;
@@ -456,6 +484,10 @@ int launch_tiled3d_f64(const BoxDesc *hbox, const BoxDesc *boxes, const int *ite
         k_stage_tiled3d_f64<NS, 1, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
     else if (grav)
         k_stage_tiled3d_f64<NS, 2, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (bf && stage == 1)
+        k_stage_tiled3d_f64<NS, 1, false, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (bf)
+        k_stage_tiled3d_f64<NS, 2, false, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
     else if (hbox && stage == 1)
         k_stage_tiled3d_f64<NS, 1, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
     else if (hbox)

@@ -176,7 +176,7 @@ __device__ __forceinline__ void store_pair(double (*gx)[TY * (TX + 1)], double (
 
 }  // namespace t3m
 
-template <int NS, int STAGE, bool BATCH, bool GRAV = false>
+template <int NS, int STAGE, bool BATCH, bool GRAV = false, bool BF = false>
 __global__ void __launch_bounds__(256, 2)
 k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__restrict__ boxes,
                       const int *__restrict__ item_box, int nitems, unsigned int *work)
@@ -239,6 +239,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     const double gamma = g.gamma;
     const float gf = (float)gamma, ig1 = 1.0f / ((float)gamma - 1.0f);
     const double invV = ctrl->invV;
+    const double bscale = BF ? 0.5 * ctrl->dt : 0.0;  // boundary-flux stage weight
     const double ax = g.area[0], ay = g.area[1], az = g.area[2];
     const int bx_lo = g.bc_lo[0], bx_hi = g.bc_hi[0], by_lo = g.bc_lo[1], by_hi = g.bc_hi[1];
     const int bz_lo = g.bc_lo[2], bz_hi = g.bc_hi[2];
@@ -380,6 +381,10 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
             float gst[5];
             ghost_state<float>(loz, bz_lo, 2, gst);
             hllc_flux_fast_bf<3>(gst, loz, gf, ig1, Fzlo);
+            if constexpr (BF) {  // z-lo domain face of cell (x, y, 0)
+                const double Fd[5] = {Fzlo[0], Fzlo[1], Fzlo[2], Fzlo[3], Fzlo[4]};
+                bflux_add(g, B.bflux, 2, 0, (int64_t)(x0 + tx) + (int64_t)nx * (y0 + ty), bscale, az, Fd);
+            }
         } else {
             const bool gll = !perz && k0 - 2 < 0;
             float hzm[5];
@@ -414,19 +419,35 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
             for (int f = 0; f < 5; ++f) hz1[f] = hz[f];
         }
         hllc_flux_fast_bf<3>(hz, zr, gf, ig1, Fzhi);
+        if constexpr (BF) {
+            if (!perz && k + 1 >= nz) {  // z-hi domain face of cell (x, y, nz-1)
+                const double Fd[5] = {Fzhi[0], Fzhi[1], Fzhi[2], Fzhi[3], Fzhi[4]};
+                bflux_add(g, B.bflux, 2, 1, (int64_t)(x0 + tx) + (int64_t)nx * (y0 + ty), bscale, az, Fd);
+            }
+        }
 #pragma unroll
         for (int f = 0; f < 5; ++f) hz[f] = hz1[f];
     };
     // the own lo x face and lo y face of plane k (ring slot w0), one packed solve
-    auto xy_faces = [&](const float *w0) {
+    auto xy_faces = [&](const float *w0, int k) {
         Face2 L, R;
         face_pair(w0, ox, oy, L, R);
         f2 F[5];
         hllc_x2(L, R, gf, ig1, F);
         store_pair(S.gx, S.gy, ty * (TX + 1) + tx, ty * TX + tx, ax, ay, F);
+        if constexpr (BF) {
+            if (xlo_bnd && tx == 0) {  // x-lo domain face of cell (0, y, k)
+                const double Fd[5] = {F[0].v.x, F[1].v.x, F[2].v.x, F[3].v.x, F[4].v.x};
+                bflux_add(g, B.bflux, 0, 0, (int64_t)(y0 + ty) + (int64_t)ny * k, bscale, ax, Fd);
+            }
+            if (ylo_bnd && ty == 0) {  // y-lo domain face of cell (x, 0, k), un-rotated
+                const double Fd[5] = {F[0].v.y, F[2].v.y, F[1].v.y, F[3].v.y, F[4].v.y};
+                bflux_add(g, B.bflux, 1, 0, (int64_t)(x0 + tx) + (int64_t)nx * k, bscale, ay, Fd);
+            }
+        }
     };
     // the hi-edge faces (x at fx = TX, y at fy = TY), one pair per lane < 16
-    auto edge_faces = [&](const float *w0) {
+    auto edge_faces = [&](const float *w0, int k) {
         const int j = lane;
         const int ex[4] = {wrow(TX - 2, j), wrow(TX - 1, j), wxs(TX, j), wxs(TX + 1, j)};
         const int ey[4] = {wrow(j, TY - 2), wrow(j, TY - 1), wrow(j, TY), wrow(j, TY + 1)};
@@ -435,6 +456,16 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         f2 F[5];
         hllc_x2(L, R, gf, ig1, F);
         store_pair(S.gx, S.gy, j * (TX + 1) + TX, TY * TX + j, ax, ay, F);
+        if constexpr (BF) {
+            if (xhi_bnd) {  // x-hi domain face of cell (nx-1, y0+j, k)
+                const double Fd[5] = {F[0].v.x, F[1].v.x, F[2].v.x, F[3].v.x, F[4].v.x};
+                bflux_add(g, B.bflux, 0, 1, (int64_t)(y0 + j) + (int64_t)ny * k, bscale, ax, Fd);
+            }
+            if (yhi_bnd) {  // y-hi domain face of cell (x0+j, ny-1, k)
+                const double Fd[5] = {F[0].v.y, F[2].v.y, F[1].v.y, F[3].v.y, F[4].v.y};
+                bflux_add(g, B.bflux, 1, 1, (int64_t)(x0 + j) + (int64_t)nx * k, bscale, ay, Fd);
+            }
+        }
     };
 
     const int gx = x0 + tx, gy = y0 + ty;
@@ -481,14 +512,14 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         // ---- phase 2: the own lo x / lo y face pair; the z face (warps 0..3)
         //      or the tile's hi-edge faces (warp 7) ----
         if (z_early) {
-            xy_faces(w0);
-            if (warp == 7 && lane < 16) edge_faces(w0);
+            xy_faces(w0, k);
+            if (warp == 7 && lane < 16) edge_faces(w0, k);
         } else {
             float W2[5];
 #pragma unroll
             for (int f = 0; f < 5; ++f) W2[f] = w2[o_c + f * PC];
             zsolve(k, w0 + o_c, w1 + o_c, W2, Fzhi);
-            xy_faces(w0);
+            xy_faces(w0, k);
         }
         __syncthreads();  // (2) fluxes ready
 
@@ -567,18 +598,23 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
 
 template <int NS>
 int launch_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const int *item_box,
-                         int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav)
+                         int nitems, unsigned int *work, int stage, cudaStream_t s, bool grav,
+                         bool bf)
 {
     const size_t smem = sizeof(t3m::Smem<NS>);
-    static int res1 = 0, resb = 0, resg = 0;
+    static int res1 = 0, resb = 0, resg = 0, resf = 0;
     if (!res1) res1 = persistent_blocks(k_stage_tiled3d_mixed<NS, 1, false>,
                                         k_stage_tiled3d_mixed<NS, 2, false>, smem);
     if (!resb) resb = persistent_blocks(k_stage_tiled3d_mixed<NS, 1, true>,
                                         k_stage_tiled3d_mixed<NS, 2, true>, smem);
     if (!resg) resg = persistent_blocks(k_stage_tiled3d_mixed<NS, 1, false, true>,
                                         k_stage_tiled3d_mixed<NS, 2, false, true>, smem);
-    if (grav && !hbox) return -1;  // gravity: single boxes only
-    const int resident = grav ? resg : hbox ? res1 : resb;
+    if (!resf) resf = persistent_blocks(k_stage_tiled3d_mixed<NS, 1, false, false, true>,
+                                        k_stage_tiled3d_mixed<NS, 2, false, false, true>, smem);
+    if ((grav || bf) && !hbox) return -1;  // gravity, boundary fluxes: single boxes only
+    if (grav && bf) return -1;
+    if (bf && !hbox->bflux) return -1;
+    const int resident = grav ? resg : bf ? resf : hbox ? res1 : resb;
     if (resident <= 0 || nitems <= 0) return -1;
     const unsigned grid = (unsigned)(nitems < resident ? nitems : resident);
     BoxDesc box0;
@@ -588,6 +624,10 @@ int launch_tiled3d_mixed(const BoxDesc *hbox, const BoxDesc *boxes, const int *i
         k_stage_tiled3d_mixed<NS, 1, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
     else if (grav)
         k_stage_tiled3d_mixed<NS, 2, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (bf && stage == 1)
+        k_stage_tiled3d_mixed<NS, 1, false, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
+    else if (bf)
+        k_stage_tiled3d_mixed<NS, 2, false, false, true><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
     else if (hbox && stage == 1)
         k_stage_tiled3d_mixed<NS, 1, false><<<grid, t3::NT, smem, s>>>(box0, nullptr, nullptr, nitems, work);
     else if (hbox)

@@ -20,6 +20,8 @@ BC_OUTFLOW, BC_PERIODIC, BC_REFLECTING = 0, 1, 2
 FP64, MIXED = 0, 1
 OPT_KERNEL, OPT_TILE_KZ, OPT_TILE_TAPER = 1, 2, 3
 KERNELS = {"auto": 0, "cell": 1, "tiled": 2}
+BFLUX_OFF, BFLUX_OUTER, BFLUX_INTERIOR = 0, 1, 2
+BFLUX_PLANE_LO, BFLUX_PLANE_HI, BFLUX_PLANE_INTERIOR = 0, 1, 2
 
 
 class VespaB200Error(RuntimeError):
@@ -120,6 +122,8 @@ SIGNATURES = {
     "vb_bflux_size": [_VP, _I64P],
     "vb_bflux_read": [_VP, _DP, C.c_int64],
     "vb_bflux_clear": [_VP],
+    "vb_bflux_plane": [_VP, C.c_int, C.c_int, _I64P, _I64P, _I64P, C.c_int64, C.c_int, C.c_double,
+                       _DP, C.c_int64],
     "vb_gravity_enable": [_VP, C.POINTER(GravityDesc)],
     "vb_gravity_disable": [_VP],
     "vb_gravity_solve": [_VP, _I64P, _DP],
@@ -212,6 +216,12 @@ def i32ptr(a: np.ndarray):
     if a.dtype != np.int32 or not a.flags.c_contiguous:
         raise TypeError("expected a C-contiguous int32 array")
     return a.ctypes.data_as(_I32P)
+
+
+def i64ptr(a: np.ndarray):
+    if a.dtype != np.int64 or not a.flags.c_contiguous:
+        raise TypeError("expected a C-contiguous int64 array")
+    return a.ctypes.data_as(_I64P)
 
 
 class Context:

@@ -267,8 +267,27 @@ class Simulation:
         return {"ms_finalize": fin.value, "ms_stage1": s1.value, "ms_stage2": s2.value}
 
     # -- boundary-flux register --
-    def bflux_enable(self, on: bool = True) -> None:
-        _lib.call("vb_bflux_enable", self.handle, 1 if on else 0)
+    def bflux_enable(self, on=True) -> None:
+        """on: False / True (outer faces) or "interior" (outer and interior faces,
+        BoundaryFluxRegister(record_interior = true))."""
+        mode = _lib.BFLUX_INTERIOR if on == "interior" else (_lib.BFLUX_OUTER if on else _lib.BFLUX_OFF)
+        _lib.call("vb_bflux_enable", self.handle, mode)
+
+    def bflux_plane(self, dim: int, source: str, start, stop, g0, flux_off: int, comp: int,
+                    vcell: float) -> np.ndarray:
+        """bflux_plane (src/reflux.jl:171-191) on the device: `source` "lo", "hi"
+        or "interior" picks the register keys the reference's lookup reads."""
+        R = len(start)
+        st = np.ascontiguousarray(start, dtype=np.int64)
+        sp = np.ascontiguousarray(stop, dtype=np.int64)
+        g0a = np.ascontiguousarray(g0, dtype=np.int64)
+        n = int(np.prod(sp - st + 1)) if R else 0
+        out = np.empty(n)
+        src = {"lo": _lib.BFLUX_PLANE_LO, "hi": _lib.BFLUX_PLANE_HI,
+               "interior": _lib.BFLUX_PLANE_INTERIOR}[source]
+        _lib.call("vb_bflux_plane", self.handle, int(dim), src, _lib.i64ptr(st), _lib.i64ptr(sp),
+                  _lib.i64ptr(g0a), int(flux_off), int(comp), float(vcell), _lib.dptr(out), n)
+        return out
 
     def bflux_clear(self) -> None:
         _lib.call("vb_bflux_clear", self.handle)
