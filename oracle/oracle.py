@@ -77,6 +77,9 @@ def lib():
         L.vo_compute_dt.restype = C.c_double
         L.vo_accumulate_flux.argtypes = [gp, dp, dp, dp, C.c_double]
         L.vo_accumulate_flux_gather.argtypes = [gp, dp, dp, C.c_int]
+        L.vo_accumulate_flux_gather_range.argtypes = [gp, dp, dp, C.c_int64, C.c_int64, C.c_int]
+        L.vo_invdt_range.argtypes = [gp, dp, C.c_int64, C.c_int64]
+        L.vo_invdt_range.restype = C.c_double
         L.vo_step.argtypes = [gp, dp, dp, dp, C.c_double, dp, C.c_int, C.c_int]
         L.vo_evolve.argtypes = [gp, dp, dp, dp, C.c_double, C.c_int64, dp, C.c_int, C.c_int]
         L.vo_evolve.restype = C.c_int64
@@ -214,6 +217,20 @@ def accumulate_flux(g: VoGrid, U, gather=False, nthreads=0):
     else:
         lib().vo_accumulate_flux(C.byref(g), _dp(U), _dp(acc), None, 0.0)
     return acc
+
+
+def accumulate_flux_range(g: VoGrid, U, acc, lin0, lin1, nthreads=0):
+    """The per-cell gather for the cells lin0 <= lin < lin1 into acc (in place)."""
+    assert U.dtype == np.float64 and U.flags.c_contiguous and acc.flags.c_contiguous
+    lib().vo_accumulate_flux_gather_range(C.byref(g), _dp(U), _dp(acc), int(lin0), int(lin1),
+                                          int(nthreads))
+    return acc
+
+
+def invdt_range(g: VoGrid, U, lin0, lin1) -> float:
+    """compute_dt's CFL maximum over the cells lin0 <= lin < lin1."""
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    return float(lib().vo_invdt_range(C.byref(g), _dp(U), int(lin0), int(lin1)))
 
 
 def step(g: VoGrid, U, dt, mode=0, nthreads=0, bflux=None):

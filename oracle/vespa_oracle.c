@@ -483,6 +483,39 @@ void vo_accumulate_flux_gather(const vo_grid *g, const double *U, double *acc, i
     (void)nthreads;
 }
 
+/* The per-cell gather for the cells lin0 <= lin < lin1 only (a slab of whole
+ * planes of a domain split along its last axis).  The state must be valid on
+ * the cells the stencils reach: the slab and two planes on each side. */
+void vo_accumulate_flux_gather_range(const vo_grid *g, const double *U, double *acc, int64_t lin0,
+                                     int64_t lin1, int nthreads)
+{
+    geom_t G;
+    make_geom(g, &G);
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+#endif
+    for (int64_t lin = lin0; lin < lin1; ++lin) gather_cell(g, &G, U, lin, acc);
+    (void)nthreads;
+}
+
+/* compute_dt's maximum of (|v_d| + c) / w_d (src/driver.jl:176-187) over the
+ * cells lin0 <= lin < lin1: a slab's share of the global reduction (the
+ * maximum of the shares, then cfl / max, is compute_dt of the whole domain). */
+double vo_invdt_range(const vo_grid *g, const double *U, int64_t lin0, int64_t lin1)
+{
+    geom_t G;
+    make_geom(g, &G);
+    double invdt = 0.0;
+    double W[5];
+    for (int64_t lin = lin0; lin < lin1; ++lin) {
+        prim_at(g, &G, U, lin, W);
+        double c = sqrt(g->gamma * W[4] / W[0]);
+        for (int d = 0; d < G.nd; ++d) invdt = jl_max(invdt, (fabs(W[1 + d]) + c) / G.w[d]);
+    }
+    return jl_max(invdt, 0.0);
+}
+
 /* compute_dt, src/driver.jl:169-199 (no gravity, no cosmology) */
 double vo_compute_dt(const vo_grid *g, const double *U)
 {

@@ -58,6 +58,9 @@ double vo_compute_dt(const vo_grid *g, const double *U);
 void vo_accumulate_flux(const vo_grid *g, const double *U, double *acc,
                         double *bflux, double bscale);
 void vo_accumulate_flux_gather(const vo_grid *g, const double *U, double *acc, int nthreads);
+void vo_accumulate_flux_gather_range(const vo_grid *g, const double *U, double *acc, int64_t lin0,
+                                     int64_t lin1, int nthreads);
+double vo_invdt_range(const vo_grid *g, const double *U, int64_t lin0, int64_t lin1);
 void vo_step(const vo_grid *g, double *U, double *u0, double *acc, double dt,
              double *bflux, int mode, int nthreads);
 void vo_step_breg(const vo_grid *g, double *U, double *u0, double *acc, double dt, double *vals,

@@ -94,7 +94,7 @@ def test_mixed_tiled_register_conservation_identity(vb, oracle, dims, lo, hi):
         hi_b = bm[off + 5 * pl:off + 10 * pl].reshape(5, pl).sum(axis=1)
         net += lo_b - hi_b
         off += 10 * pl
-    assert np.any(np.abs(net) > 1e-4)
+    assert np.any(np.abs(net) > 1e-6)  # flux did cross the domain faces
     # the totals are sums of U * V; the register integrates F * area * dt
     assert np.allclose(t1 - t0, net, rtol=0, atol=1e-12 * np.abs(t0).max())
     np.testing.assert_allclose(bm, bf, rtol=0, atol=1e-5 * np.abs(bf).max())
