@@ -155,6 +155,31 @@ int vb_grid_get_time(vb_grid *grid, double *t, int64_t *step);
 /* compute_dt(sim), src/driver.jl:169-199: cfl / max over cells and axes of
  * (|v_d| + c) / w_d; +Inf when the gas is at rest. */
 int vb_compute_dt(vb_grid *grid, double *dt);
+/* Slab decomposition of one grid across GPUs (no counterpart in the
+ * reference, which runs on one host): a rank's grid holds its z slab plus
+ * ghost planes copied from its neighbours.  vb_grid_set_zwindow marks planes
+ * zw0 <= z < zw1 as the rank's own (the CFL maximum and the totals cover them
+ * only), gives plane zw0 the lo-face order class zcls0 it has in the whole
+ * domain (0 emitted by the plane below, 1 by itself: a wall, 2 by the
+ * periodic partner above; -1 keeps the slab's own) and sets the z cell width
+ * wz of the whole domain (areas and volume follow).  3D grids on the tiled
+ * kernel only, without gravity or boundary-flux recording. */
+int vb_grid_set_zwindow(vb_grid *grid, int64_t zw0, int64_t zw1, int zcls0, double wz);
+/* One step in phases, queued on the context's stream, so the ranks can
+ * all-reduce the CFL maximum (vb_grid_cfl_bits) and exchange ghost planes
+ * (vb_grid_planes) between them: CFL (fold the current state's maximum if
+ * stale), FINALIZE (dt from the maximum), STAGE1, STAGE2, ADVANCE (clock). */
+enum { VB_PHASE_CFL = 0, VB_PHASE_FINALIZE = 1, VB_PHASE_STAGE1 = 2, VB_PHASE_STAGE2 = 3,
+       VB_PHASE_ADVANCE = 4 };
+int vb_grid_step_phase(vb_grid *grid, int phase);
+/* Copy n whole z planes from plane z0 of the state (which = 0) or the
+ * stage-1 state (which = 1) to (put = 0) or from (put = 1) the device buffer
+ * dev, laid out [5 fields][n planes][ny][nx] float64. */
+int vb_grid_planes(vb_grid *grid, int which, int64_t z0, int64_t n, void *dev, int put);
+/* The running CFL maximum as one int64 device word at dev (put = 0 reads it
+ * out, put = 1 writes it back): non-negative doubles compare like their bit
+ * patterns, so an all-reduce max of the words is the max of the values. */
+int vb_grid_cfl_bits(vb_grid *grid, void *dev, int put);
 /* No counterpart in the reference: a self-test of the failure path.  Runs one
  * block that waits, bounded by limit_ns (1 us .. 10 s), on an mbarrier that
  * nothing completes, then takes the tiled stage kernels' abandon path, which

@@ -72,6 +72,12 @@ const VB_GRAV_PRECOND_MG = Int32(1)
 const VB_MUSCL_BC_NONE = Int32(0)
 const VB_MUSCL_BC_PERIODIC = Int32(1)
 const VB_NOALLOC_MAX_FACES = 65536
+# step phases (vb_grid_step_phase)
+const VB_PHASE_CFL = Cint(0)
+const VB_PHASE_FINALIZE = Cint(1)
+const VB_PHASE_STAGE1 = Cint(2)
+const VB_PHASE_STAGE2 = Cint(3)
+const VB_PHASE_ADVANCE = Cint(4)
 # boundary-flux register modes and bflux_plane sources
 const VB_BFLUX_OFF = Cint(0)
 const VB_BFLUX_OUTER = Cint(1)
@@ -171,6 +177,14 @@ vb_compute_dt(grid, dt) =
     ccall((:vb_compute_dt, libvespa_b200), Cint, (Ptr{Cvoid}, Ptr{Float64}), grid, dt)
 vb_grid_selftest_wait(grid, limit_ns) =
     ccall((:vb_grid_selftest_wait, libvespa_b200), Cint, (Ptr{Cvoid}, Int64), grid, limit_ns)
+vb_grid_set_zwindow(grid, zw0, zw1, zcls0, wz) =
+    ccall((:vb_grid_set_zwindow, libvespa_b200), Cint, (Ptr{Cvoid}, Int64, Int64, Cint, Float64), grid, zw0, zw1, zcls0, wz)
+vb_grid_step_phase(grid, phase) =
+    ccall((:vb_grid_step_phase, libvespa_b200), Cint, (Ptr{Cvoid}, Cint), grid, phase)
+vb_grid_planes(grid, which, z0, n, dev, put) =
+    ccall((:vb_grid_planes, libvespa_b200), Cint, (Ptr{Cvoid}, Cint, Int64, Int64, Ptr{Cvoid}, Cint), grid, which, z0, n, dev, put)
+vb_grid_cfl_bits(grid, dev, put) =
+    ccall((:vb_grid_cfl_bits, libvespa_b200), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cint), grid, dev, put)
 vb_step(grid, dt) =
     ccall((:vb_step, libvespa_b200), Cint, (Ptr{Cvoid}, Float64), grid, dt)
 vb_evolve(grid, tfinal, max_steps, t, nsteps) =

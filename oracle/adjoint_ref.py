@@ -29,6 +29,16 @@ minmod choices and hence the frozen-branch gradient.
 Layout: the state is a ``(5, ncell)`` float64 tensor, cells column-major with
 x fastest (``vespa_oracle.h``).  Internally it is viewed as
 ``(5, n_{nd-1}, ..., n_0)`` so axis d is tensor dimension ``nd - d``.
+
+Frozen map.  With a ``Tape`` every branch condition above is recorded in
+evaluation order during one run (``Tape(record=True)``) and replayed in a
+later run: that run then evaluates the step map with the recorded branch
+choices at any nearby input, a smooth map whose derivative is exactly what
+a frozen-branch adjoint computes.  Central differences of it check such an
+adjoint even where the unfrozen map has kinks (minmod ties in a uniform
+state).  Tensors may live on a GPU: there torch's float64 square root and
+division are correctly rounded, so the values stay bit-identical to the C
+oracle's.
 """
 from __future__ import annotations
 
@@ -55,7 +65,40 @@ class _Sqrt(torch.autograd.Function):
 
 
 def _sqrt(x):
+    if x.is_cuda:
+        return torch.sqrt(x)
     return _Sqrt.apply(x)
+
+
+class Tape:
+    """Branch conditions of one run, in evaluation order: recorded when
+    `record` is true, else replayed (the conditions computed from the current
+    values are ignored)."""
+
+    def __init__(self, record: bool = True):
+        self.record = record
+        self.masks = []
+        self.pos = 0
+
+    def replay(self):
+        self.record = False
+        self.pos = 0
+        return self
+
+    def __call__(self, cond):
+        if self.record:
+            self.masks.append(cond)
+            return cond
+        m = self.masks[self.pos]
+        self.pos += 1
+        return m
+
+
+_TAPE = None  # the active tape (set by evolve/rk2_step callers), or None
+
+
+def _br(cond):
+    return cond if _TAPE is None else _TAPE(cond)
 
 
 def cons2prim(U, g):
@@ -67,13 +110,13 @@ def cons2prim(U, g):
     ke = 0.5 * rho * (vx * vx + vy * vy + vz * vz)
     p = (g - 1.0) * (U[4] - ke)
     floor = 1e-12 * ke
-    p = torch.where(p >= floor, p, floor)
+    p = torch.where(_br(p >= floor), p, floor)
     return [rho, vx, vy, vz, p]
 
 
 def minmod(a, b):
     z = torch.zeros_like(a)
-    return torch.where(a * b <= 0, z, torch.where(a.abs() < b.abs(), a, b))
+    return torch.where(_br(a * b <= 0), z, torch.where(_br(a.abs() < b.abs()), a, b))
 
 
 def hllc(WL, WR, g, dim):
@@ -85,18 +128,18 @@ def hllc(WL, WR, g, dim):
     cL = _sqrt(g * pL / rhoL)
     cR = _sqrt(g * pR / rhoR)
     aL, aR = unL - cL, unR - cR
-    SL = torch.where(aL <= aR, aL, aR)
+    SL = torch.where(_br(aL <= aR), aL, aR)
     bL, bR = unL + cL, unR + cR
-    SR = torch.where(bL >= bR, bL, bR)
+    SR = torch.where(_br(bL >= bR), bL, bR)
     one = torch.ones_like(SL)
     zero = torch.zeros_like(SL)
-    supL = SL >= 0
-    supR = (~supL) & (SR <= 0)
+    supL = _br(SL >= 0)
+    supR = (~supL) & _br(SR <= 0)
     star = ~(supL | supR)
     N = pR - pL + rhoL * unL * (SL - unL) - rhoR * unR * (SR - unR)
     D = rhoL * (SL - unL) - rhoR * (SR - unR)
     Sstar = torch.where(star, N / torch.where(star, D, one), zero)
-    left = supL | (star & (Sstar >= 0))
+    left = supL | (star & _br(Sstar >= 0))
     SK = torch.where(left, SL, SR)
     rho = torch.where(left, rhoL, rhoR)
     v = [torch.where(left, WL[1 + j], WR[1 + j]) for j in range(3)]
@@ -163,7 +206,8 @@ def flux_divergence(grid: PeriodicGrid, U):
     coords = []
     for d in range(grid.nd):
         td = grid.nd - d - 1
-        idx = torch.arange(grid.dims[d]).reshape([-1 if e == td else 1 for e in range(grid.nd)])
+        idx = torch.arange(grid.dims[d], device=U.device)
+        idx = idx.reshape([-1 if e == td else 1 for e in range(grid.nd)])
         coords.append(idx.expand(shape))
     Fhi, Flo = [], []
     for d in range(grid.nd):
@@ -176,9 +220,10 @@ def flux_divergence(grid: PeriodicGrid, U):
         Flo.append([torch.roll(F[k], 1, td) for k in range(5)])
     acc = []
     for k in range(5):
-        a = torch.zeros(shape, dtype=W[0].dtype)
+        a = torch.zeros(shape, dtype=W[0].dtype, device=U.device)
         for d in reversed(range(grid.nd)):
-            before = (coords[d] > 0) if grid.dims[d] > 1 else torch.zeros(shape, dtype=torch.bool)
+            before = (coords[d] > 0) if grid.dims[d] > 1 else torch.zeros(shape, dtype=torch.bool,
+                                                                          device=U.device)
             a = torch.where(before, a + (-grid.area[d]) * Flo[d][k], a)
         for d in range(grid.nd):
             a = a + grid.area[d] * Fhi[d][k]
@@ -198,9 +243,16 @@ def rk2_step(grid: PeriodicGrid, U, dt):
     return 0.5 * U + 0.5 * (U1 - invV * flux_divergence(grid, U1))
 
 
-def evolve(grid: PeriodicGrid, U, dts):
-    for dt in dts:
-        U = rk2_step(grid, U, float(dt))
+def evolve(grid: PeriodicGrid, U, dts, tape: Tape = None):
+    """The run with the given dt sequence; with a tape, its branches are
+    recorded (tape.record) or replayed."""
+    global _TAPE
+    _TAPE = tape
+    try:
+        for dt in dts:
+            U = rk2_step(grid, U, float(dt))
+    finally:
+        _TAPE = None
     return U
 
 

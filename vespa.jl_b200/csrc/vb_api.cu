@@ -221,6 +221,11 @@ int make_geom(const vb_problem_desc *d, vb::Geom *out)
     g.gamma = d->gamma;
     g.cfl = d->cfl;
     g.aexp = d->aexp;
+    g.zw0 = 0;
+    g.zw1 = (int)g.n[2];
+    g.zcls0 = -1;
+    g.act0 = 0;
+    g.act1 = g.ncell;
     *out = g;
     return VB_OK;
 }
@@ -295,7 +300,10 @@ int stage(vb_grid *gr, int st, const double *Uin, const double *U0, double *Uout
     const bool grav = gr->grav != nullptr;  // self-gravity: 3D tiled kernels carry the source
     // the tiled kernels record outer boundary fluxes themselves; interior
     // faces, and boundary fluxes together with gravity, take the cell kernel
-    if (gr->tiled && !bfi && !(bf && grav) && (!grav || gr->g.nd == 3)) {
+    const bool use_tiled = gr->tiled && !bfi && !(bf && grav) && (!grav || gr->g.nd == 3);
+    if (gr->slab && !use_tiled)
+        return fail(VB_ENOTSUP, "a z-window (slab) grid steps with the tiled 3D kernels only");
+    if (use_tiled) {
         int rc = sync_box(gr);
         if (rc) return rc;
         gr->box.bflux = bf;
@@ -873,6 +881,94 @@ int vb_compute_dt(vb_grid *gr, double *dt)
         return fail(VB_ENONFINITE, "non-finite or negative density/pressure in the state");
     }
     *dt = invdt == 0.0 ? INFINITY : gr->g.cfl / invdt;
+    return VB_OK;
+}
+
+int vb_grid_set_zwindow(vb_grid *gr, int64_t zw0, int64_t zw1, int zcls0, double wz)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    vb::Geom &g = gr->g;
+    if (g.nd != 3 || !gr->tiled)
+        return fail(VB_ENOTSUP, "z windows need a 3D grid on the tiled kernel");
+    if (!(zw0 >= 0 && zw0 < zw1 && zw1 <= g.n[2])) return fail(VB_EINVAL, "need 0 <= zw0 < zw1 <= nz");
+    if (zcls0 < -1 || zcls0 > 2) return fail(VB_EINVAL, "zcls0 must be -1, 0, 1 or 2");
+    if (!(wz > 0.0) || !std::isfinite(wz)) return fail(VB_EINVAL, "wz must be positive");
+    if (gr->grav || gr->bflux_on)
+        return fail(VB_ENOTSUP, "z windows exclude self-gravity and boundary-flux recording");
+    // the z width of the whole domain, and the areas and volume derived from
+    // it as the grid's own geometry derives them (product in axis order)
+    g.w[2] = wz;
+    g.invw[2] = 1.0 / wz;
+    for (int a = 0; a < 3; ++a) {
+        double ar = 1.0;
+        for (int e = 0; e < 3; ++e)
+            if (e != a) ar *= g.w[e];
+        g.area[a] = ar;
+    }
+    g.vol = (g.w[0] * g.w[1]) * g.w[2];
+    g.zw0 = (int)zw0;
+    g.zw1 = (int)zw1;
+    g.zcls0 = zcls0;
+    g.act0 = zw0 * g.n[0] * g.n[1];
+    g.act1 = zw1 * g.n[0] * g.n[1];
+    gr->slab = true;
+    gr->box_kz = -1;        // the box descriptor carries the geometry
+    gr->invdt_valid = false;
+    if (gr->gexec) {        // captured launches hold the old geometry
+        cudaGraphExecDestroy(gr->gexec);
+        gr->gexec = nullptr;
+    }
+    return VB_OK;
+}
+
+int vb_grid_step_phase(vb_grid *gr, int phase)
+{
+    if (!gr) return fail(VB_EINVAL, "null grid");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    cudaStream_t s = gr->ctx->stream;
+    switch (phase) {
+    case VB_PHASE_CFL: return ensure_cfl(gr);
+    case VB_PHASE_FINALIZE:
+        VB_CHECK_LAUNCH(gr->ctx, vb::launch_finalize_cfl(gr->g, gr->ctrl, s));
+        return VB_OK;
+    case VB_PHASE_STAGE1: return stage(gr, 1, gr->U, gr->U, gr->U1);
+    case VB_PHASE_STAGE2: return stage(gr, 2, gr->U1, gr->U, gr->U);
+    case VB_PHASE_ADVANCE:
+        VB_CHECK_LAUNCH(gr->ctx, vb::launch_advance(gr->ctrl, s));
+        gr->invdt_valid = true;  // stage 2 folded the new state's CFL maximum
+        return VB_OK;
+    default: return fail(VB_EINVAL, "unknown phase");
+    }
+}
+
+int vb_grid_planes(vb_grid *gr, int which, int64_t z0, int64_t n, void *dev, int put)
+{
+    if (!gr || !dev) return fail(VB_EINVAL, "null argument");
+    if (which != 0 && which != 1) return fail(VB_EINVAL, "which must be 0 (state) or 1 (stage-1 state)");
+    const vb::Geom &g = gr->g;
+    if (g.nd != 3 || z0 < 0 || n < 1 || z0 + n > g.n[2]) return fail(VB_EINVAL, "planes out of range");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    double *buf = (which ? gr->U1 : gr->U) + z0 * g.n[0] * g.n[1];
+    const size_t width = sizeof(double) * (size_t)(n * g.n[0] * g.n[1]);
+    const size_t pitch = sizeof(double) * (size_t)g.ncell;
+    if (put)
+        VB_CUDA(cudaMemcpy2DAsync(buf, pitch, dev, width, width, 5, cudaMemcpyDeviceToDevice,
+                                  gr->ctx->stream));
+    else
+        VB_CUDA(cudaMemcpy2DAsync(dev, width, buf, pitch, width, 5, cudaMemcpyDeviceToDevice,
+                                  gr->ctx->stream));
+    return VB_OK;
+}
+
+int vb_grid_cfl_bits(vb_grid *gr, void *dev, int put)
+{
+    if (!gr || !dev) return fail(VB_EINVAL, "null argument");
+    int rc = use(gr->ctx);
+    if (rc) return rc;
+    VB_CHECK_LAUNCH(gr->ctx, vb::launch_cfl_bits(gr->ctrl, (unsigned long long *)dev, put ? 1 : 0,
+                                                 gr->ctx->stream));
     return VB_OK;
 }
 

@@ -32,6 +32,13 @@ struct Geom {
     // over a step; grav_G = the constant G of the free-fall dt limiter
     const double *grav_g;
     double grav_G;
+    // slab of a z-split domain (vb_grid_set_zwindow): planes zw0 <= z < zw1
+    // are this rank's own, the others ghost copies of its neighbours'.  The
+    // CFL maximum and the totals cover cells act0 <= lin < act1 only, and
+    // the tiled kernels give plane zw0 the lo-face order class zcls0 (its
+    // class in the whole domain; -1: the slab's own).  Defaults: all planes.
+    int zw0, zw1, zcls0;
+    int64_t act0, act1;
 };
 
 // 4 pi, as FOURPI in src/gravity.jl:21

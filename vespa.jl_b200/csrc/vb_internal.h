@@ -48,6 +48,7 @@ struct vb_grid {
     int64_t glaunches = 0;              // kernels per replay
     bool warmed = false;                // one direct step ran (launch setup done)
     vb_gravity *grav = nullptr;         // self-gravity (stages take the cell-centric kernel)
+    bool slab = false;                  // a z window is set (vb_grid_set_zwindow): tiled kernels only
 };
 
 namespace vb {

@@ -33,7 +33,7 @@ __global__ void __launch_bounds__(256) k_cfl(Geom g, const double *__restrict__ 
 {
     __shared__ double red[32];
     double m = 0.0;
-    for (int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.ncell;
+    for (int64_t lin = g.act0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.act1;
          lin += (int64_t)gridDim.x * blockDim.x) {
         double u[5], W[5];
 #pragma unroll
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(256) k_totals_part(Geom g, const double *__res
 {
     __shared__ double red[5][8];
     double s[5] = {0, 0, 0, 0, 0};
-    for (int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.ncell;
+    for (int64_t lin = g.act0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; lin < g.act1;
          lin += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) s[k] += __ldg(U + k * g.ncell + lin) * g.vol;
@@ -226,6 +226,20 @@ __global__ void k_advance(Ctrl *ctrl)
     }
 }
 
+// The running CFL maximum of a slab <-> a device word the ranks all-reduce
+// (max over int64: non-negative doubles order like their bit patterns; a NaN
+// with the sign bit set is stored as the positive quiet NaN, so that it still
+// wins the max).
+__global__ void k_cfl_bits(Ctrl *ctrl, unsigned long long *dev, int put)
+{
+    if (put) {
+        ctrl->invdt_bits = *dev;
+    } else {
+        const unsigned long long b = ctrl->invdt_bits;
+        *dev = (b >> 63) ? 0x7FF8000000000000ull : b;
+    }
+}
+
 // Failure-path self-test: the tiled kernels' bounded stage wait on an
 // mbarrier that nothing will ever complete (no copy is issued, so nothing is
 // in flight), then the same block-uniform decision and abandon path as a
@@ -246,6 +260,13 @@ __global__ void k_wait_selftest(Ctrl *ctrl, uint64_t limit_ns)
 }
 
 }  // namespace
+
+int launch_cfl_bits(Ctrl *ctrl, unsigned long long *dev, int put, cudaStream_t s)
+{
+    if (!ctrl || !dev) return -1;
+    k_cfl_bits<<<1, 1, 0, s>>>(ctrl, dev, put);
+    return 1;
+}
 
 int launch_wait_selftest(Ctrl *ctrl, uint64_t limit_ns, cudaStream_t s)
 {

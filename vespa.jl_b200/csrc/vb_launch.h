@@ -128,6 +128,9 @@ int launch_finalize_boxes(const BoxDesc *boxes, int nbox, unsigned int *work, cu
 int launch_advance_boxes(const BoxDesc *boxes, int nbox, cudaStream_t s);
 // Clock advance of a single control block (t += dt, step += 1 while active).
 int launch_advance(Ctrl *ctrl, cudaStream_t s);
+// Copy the running CFL maximum of ctrl out to (put = 0) or in from (put = 1)
+// the device word dev.
+int launch_cfl_bits(Ctrl *ctrl, unsigned long long *dev, int put, cudaStream_t s);
 // A bounded mbarrier wait that must run out after limit_ns, then the stage
 // kernels' abandon path (CTRL_F_TIMEOUT in ctrl).
 int launch_wait_selftest(Ctrl *ctrl, uint64_t limit_ns, cudaStream_t s);

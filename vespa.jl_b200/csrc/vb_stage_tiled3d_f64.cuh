@@ -367,7 +367,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
             if (z_early) zsolve(k, w0 + o_c, w1 + o_c, Wn, Fzhi);
             else halo_c2p(q);
             if constexpr (STAGE == 2)
-                if (k > k0) invdt = cf;
+                if (k > k0 && k > g.zw0 && k <= g.zw1) invdt = cf;  // plane k-1, if the slab's own
         }
         __syncthreads();  // (1) plane k+2 converted
         if (stalled(q)) return;
@@ -387,7 +387,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
         __syncthreads();  // (2) fluxes ready
 
         // ---- flux divergence in the reference's order, then the stage update ----
-        const int cz = lo_class(k, nz, perz);
+        const int cz = (k == g.zw0 && g.zcls0 >= 0) ? g.zcls0 : lo_class(k, nz, perz);
         const bool interior = cx == LO_BEFORE && cy == LO_BEFORE && cz == LO_BEFORE;
         double un[5];
         const double *pin = Uin + lin, *p0 = U0 + lin;
@@ -450,7 +450,8 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
             for (int f = 0; f < 5; ++f) unp[f] = un[f];
         }
     }
-    if constexpr (STAGE == 2) invdt = cfl_term_exact<GRAV>(unp, g, invdt);  // the item's last plane
+    if constexpr (STAGE == 2)  // the item's last plane, when it is one of the slab's own
+        if (k1 - 1 >= g.zw0 && k1 - 1 < g.zw1) invdt = cfl_term_exact<GRAV>(unp, g, invdt);
     qb += nplanes;
     if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);  // this box's CFL max
     }  // work items

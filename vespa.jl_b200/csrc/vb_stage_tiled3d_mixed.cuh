@@ -72,12 +72,15 @@ __device__ __forceinline__ float mm(float l, float c, float r)
 
 // cons2prim for VB_MIXED (src/eos.jl:8-25): velocities and the
 // total-energy-minus-kinetic pressure recovery in float64, results rounded
-// to float32.  1/rho comes from a float32 reciprocal refined by two float64
-// Newton steps (relative error ~1e-16) instead of a float64 division.
+// to float32.  1/rho comes from the float64 approximate-reciprocal
+// instruction refined by two Newton-Raphson steps x <- x (2 - rho x)
+// (quadratic convergence: the seed's relative error e becomes e^4, far below
+// float64 rounding) instead of a float64 division.
 __device__ __forceinline__ void cons2prim_mixed(const double U[5], double g, float W[5])
 {
     const double rho = U[0];
-    double inv = (double)rcp_approx((float)rho);
+    double inv;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(inv) : "d"(rho));
     inv = inv * (2.0 - rho * inv);
     inv = inv * (2.0 - rho * inv);
     const double vx = U[1] * inv, vy = U[2] * inv, vz = U[3] * inv;
@@ -279,10 +282,9 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     }
     // Halo strips of staged plane q into ring slot q % 3 (threads t < NH; a
     // strip outside a non-periodic boundary is left to the mirror ghosts).
-    auto halo_c2p = [&](int q) {
+    auto halo_c2p = [&](int q, float *ws) {
         if (t < NH && !h_ghost) {
             const double *u = S.u[(qb + q) % NS];
-            float *ws = S.w[q % 3];
             double uu[5];
             float w[5];
 #pragma unroll
@@ -295,7 +297,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     // Wait for staged plane q and convert the own cell into Wn.  keep = 0:
     // registers only; 1: also into ring slot q % 3 with the mirror ghosts and
     // the halo strips; 2: as 1 without the halo strips (halo_c2p follows).
-    auto consume = [&](int q, float Wn[5], int keep) {
+    auto consume = [&](int q, float Wn[5], int keep, float *ws) {
         const int b = (qb + q) % NS;
         if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) stall_sh = 1;
         const double *u = S.u[b];
@@ -306,7 +308,6 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
             cons2prim_mixed(uu, gamma, Wn);
         }
         if (!keep) return;
-        float *ws = S.w[q % 3];
 #pragma unroll
         for (int f = 0; f < 5; ++f) ws[f * PC + o_c] = Wn[f];
         if (xlo_bnd && tx < 2) {
@@ -329,7 +330,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
 #pragma unroll
             for (int f = 0; f < 5; ++f) d[f * PC] = (by_hi == BC_REFLECTING && f == 2) ? -Wn[f] : Wn[f];
         }
-        if (keep == 1) halo_c2p(q);
+        if (keep == 1) halo_c2p(q, ws);
     };
     auto release = [&](int q) {
         if (t == 0 && q + NS < nplanes) {
@@ -345,19 +346,19 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     };
 
     float Wa[5], Wb[5], Wc[5], Wd[5];
-    consume(0, Wa, 0);
+    consume(0, Wa, 0, nullptr);
     __syncthreads();
     if (stalled(0)) return;
     release(0);
-    consume(1, Wb, 0);
+    consume(1, Wb, 0, nullptr);
     __syncthreads();
     if (stalled(1)) return;
     release(1);
-    consume(2, Wc, 1);
+    consume(2, Wc, 1, S.w[2]);
     __syncthreads();
     if (stalled(2)) return;
     release(2);
-    consume(3, Wd, 1);
+    consume(3, Wd, 1, S.w[0]);
     __syncthreads();
     if (stalled(3)) return;
     release(3);
@@ -476,9 +477,10 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     const int64_t plane_cells = (int64_t)nx * ny;
     int64_t lin = (int64_t)gx + (int64_t)nx * ((int64_t)gy + (int64_t)ny * k0);
 
+    float *r0 = S.w[2], *r1 = S.w[0], *r2 = S.w[1];  // ring slots of planes k, k+1, k+2
     for (int k = k0; k < k1; ++k) {
         const int q = k - k0 + 4;
-        const float *w0 = S.w[(q - 2) % 3], *w1 = S.w[(q - 1) % 3], *w2 = S.w[q % 3];
+        const float *w0 = r0, *w1 = r1, *w2 = r2;
         {
             const double *pa = Uin + lin, *pb = U0 + lin;
 #pragma unroll
@@ -495,16 +497,16 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         float Fzhi[5];
         {
             float Wn[5];
-            consume(q, Wn, 2);
+            consume(q, Wn, 2, r2);
             float cf = 0.f;
             if constexpr (STAGE == 2) cf = cfl_mixed<GRAV>(unp, g, gf, iw0, iw1, iw2, invdtf);
             if (z_early) {
                 zsolve(k, w0 + o_c, w1 + o_c, Wn, Fzhi);
             } else {
-                halo_c2p(q);
+                halo_c2p(q, r2);
             }
             if constexpr (STAGE == 2)
-                if (k > k0) invdtf = cf;
+                if (k > k0 && k > g.zw0 && k <= g.zw1) invdtf = cf;  // plane k-1, if the slab's own
         }
         __syncthreads();  // (1) plane k+2 converted
         if (stalled(q)) return;
@@ -524,7 +526,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         __syncthreads();  // (2) fluxes ready
 
         // ---- flux divergence (float64, reference order) and the stage update ----
-        const int cz = lo_class(k, nz, perz);
+        const int cz = (k == g.zw0 && g.zcls0 >= 0) ? g.zcls0 : lo_class(k, nz, perz);
         const bool interior = cx == LO_BEFORE && cy == LO_BEFORE && cz == LO_BEFORE;
         double un[5];
         double *po = Uout + lin;
@@ -588,9 +590,15 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
 #pragma unroll
             for (int f = 0; f < 5; ++f) unp[f] = un[f];
         }
+        float *rt = r0;
+        r0 = r1;
+        r1 = r2;
+        r2 = rt;
     }
     if constexpr (STAGE == 2)  // the item's last plane
-        invdt = (double)cfl_mixed<GRAV>(unp, g, gf, iw0, iw1, iw2, invdtf);
+        invdt = (k1 - 1 >= g.zw0 && k1 - 1 < g.zw1)
+                    ? (double)cfl_mixed<GRAV>(unp, g, gf, iw0, iw1, iw2, invdtf)
+                    : (double)invdtf;
     qb += nplanes;
     if constexpr (STAGE == 2) block_max_to(&ctrl->invdt_bits, invdt, red);  // this box's CFL max
     }  // work items

@@ -21,6 +21,7 @@ FP64, MIXED = 0, 1
 OPT_KERNEL, OPT_TILE_KZ, OPT_TILE_TAPER = 1, 2, 3
 KERNELS = {"auto": 0, "cell": 1, "tiled": 2}
 BFLUX_OFF, BFLUX_OUTER, BFLUX_INTERIOR = 0, 1, 2
+PHASE_CFL, PHASE_FINALIZE, PHASE_STAGE1, PHASE_STAGE2, PHASE_ADVANCE = 0, 1, 2, 3, 4
 BFLUX_PLANE_LO, BFLUX_PLANE_HI, BFLUX_PLANE_INTERIOR = 0, 1, 2
 
 
@@ -105,6 +106,10 @@ SIGNATURES = {
     "vb_compute_dt": [_VP, _DP],
     "vb_step": [_VP, C.c_double],
     "vb_grid_selftest_wait": [_VP, C.c_int64],
+    "vb_grid_set_zwindow": [_VP, C.c_int64, C.c_int64, C.c_int, C.c_double],
+    "vb_grid_step_phase": [_VP, C.c_int],
+    "vb_grid_planes": [_VP, C.c_int, C.c_int64, C.c_int64, _VP, C.c_int],
+    "vb_grid_cfl_bits": [_VP, _VP, C.c_int],
     "vb_evolve": [_VP, C.c_double, C.c_int64, _DP, _I64P],
     "vb_run_steps_async": [_VP, C.c_int64],
     "vb_conserved_totals": [_VP, _DP],

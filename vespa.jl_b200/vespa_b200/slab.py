@@ -20,6 +20,7 @@ periodic z axis) copies locally.
 """
 from __future__ import annotations
 
+import math
 from typing import Callable, Optional
 
 GHOST = 2  # planes of the neighbouring slab a PLM face flux reaches
@@ -112,3 +113,175 @@ def allreduce_max_bits(t, group=None) -> None:
 def allreduce_sum(t, group=None) -> None:
     import torch.distributed as dist
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+
+
+# z-lo face order classes of the tiled kernels (the reference's emission order)
+_LO_AFTER = 2  # emitted by the periodic partner at the domain's far end
+
+
+class SlabSimulation:
+    """One rank's slab of a z-split uniform 3D grid, stepped on its GPU.
+
+    The rank's grid holds its planes plus the ghost planes of `Halo`; the
+    tiled kernels compute every local plane, the ghosts' results are
+    replaced by the exchange before anything reads them, and the window set
+    with vb_grid_set_zwindow keeps the CFL maximum and the totals to the
+    rank's own planes and gives the domain's first plane its global face
+    order.  Per step: CFL maximum all-reduced (max), dt, stage 1, stage-1
+    ghosts exchanged, stage 2, clock, state ghosts exchanged.  The results
+    equal one grid stepped alone, bit for bit.
+
+    `group`: the torch.distributed group of the ranks (None: the default
+    group, or a single rank when torch.distributed is not initialised).
+    `world`/`rank` override the group's size and rank: slabs of one process
+    then move their planes themselves (phase / get_planes / put_planes /
+    cfl_bits), which is how a single GPU runs several slabs.
+    """
+
+    def __init__(self, problem, *, precision: str = "fp64", group=None, ctx=None,
+                 initial=None, kz: Optional[int] = None, world: Optional[int] = None,
+                 rank: Optional[int] = None):
+        import numpy as np
+        import torch
+        import torch.distributed as dist
+        from . import problem as P
+        from .simulation import B200Mesh, Simulation
+        from ._lib import default_context
+        if problem.ndim != 3:
+            raise ValueError("slab decomposition splits 3D grids along z")
+        self.group = group
+        dist_on = dist.is_available() and dist.is_initialized()
+        self.world = world if world is not None else (dist.get_world_size(group) if dist_on else 1)
+        self.rank = rank if rank is not None else (dist.get_rank(group) if dist_on else 0)
+        nx, ny, nz = problem.dims
+        pairs = problem.bc_pairs()
+        periodic = pairs[2][0] == P.Periodic.code
+        self.halo = h = Halo(nz, self.world, self.rank, periodic)
+        self.global_dims = (nx, ny, nz)
+        code_bc = {P.Outflow.code: P.Outflow, P.Periodic.code: P.Periodic,
+                   P.Reflecting.code: P.Reflecting}
+        # a side with ghosts is an ordinary outflow side to the local grid:
+        # only ghost planes see it, and the exchange overwrites them
+        zlo = code_bc[pairs[2][0]] if h.g_lo == 0 else P.Outflow
+        zhi = code_bc[pairs[2][1]] if h.g_hi == 0 else P.Outflow
+        bcs = tuple((code_bc[a], code_bc[b]) for a, b in pairs[:2]) + ((zlo, zhi),)
+        (x0, x1), (y0, y1), (zd0, zd1) = problem.domain
+        wz = (zd1 - zd0) / nz
+        local = P.Problem(name=problem.name + f"[slab {self.rank}/{self.world}]",
+                          dims=(nx, ny, h.nloc), domain=((x0, x1), (y0, y1),
+                                                         (zd0 + (h.z0 - h.g_lo) * wz,
+                                                          zd0 + (h.z0 - h.g_lo + h.nloc) * wz)),
+                          gamma=problem.gamma, bcs=bcs, init=problem.init, tfinal=math.inf,
+                          cfl=problem.cfl)
+        self.ctx = ctx or default_context()
+        self.planes = h.global_planes(nz)
+        if initial is None:
+            initial = P.initial_state(problem)
+        Ug = np.asarray(initial).reshape(5, nz, ny, nx)
+        Ul = np.ascontiguousarray(Ug[:, self.planes].reshape(5, -1))
+        self.sim = Simulation(B200Mesh(local.dims, local.domain), local, precision=precision,
+                              ctx=self.ctx, initial=Ul)
+        self.sim.set_kernel("tiled", kz=kz)
+        zcls0 = _LO_AFTER if (periodic and h.holds_z0 and nz > 1) else -1
+        self._call("vb_grid_set_zwindow", h.act0, h.act0 + h.nact, zcls0, wz)
+        dev = torch.device("cuda", self.ctx.device)
+        self._bits = torch.zeros(1, dtype=torch.int64, device=dev)
+        n = 5 * GHOST * nx * ny
+        self._bufs = {k: torch.empty(n, dtype=torch.float64, device=dev) for k in ("lo", "hi")}
+        self._stream = torch.cuda.ExternalStream(self.ctx.stream, device=dev)
+        self.t = 0.0
+        self.step_count = 0
+
+    # -- library calls on the rank's grid --
+    def _call(self, name, *args):
+        from . import _lib
+        _lib.call(name, self.sim.handle, *args)
+
+    def phase(self, p: int) -> None:
+        """One phase of a step (_lib.PHASE_*), queued on the library's stream."""
+        self._call("vb_grid_step_phase", p)
+
+    def get_planes(self, which: int, first: int, count: int, out=None):
+        """Local planes [first, first + count) of the state (0) or stage-1 state
+        (1) as a (5, count, ny * nx) device tensor (queued on the library's stream)."""
+        import torch
+        nx, ny, _ = self.global_dims
+        if out is None:
+            out = torch.empty(5 * count * nx * ny, dtype=torch.float64, device=self._bits.device)
+        self._call("vb_grid_planes", which, first, count, out.data_ptr(), 0)
+        return out.view(5, count, nx * ny)
+
+    def put_planes(self, which: int, first: int, t) -> None:
+        t = t.contiguous()
+        self._call("vb_grid_planes", which, first, t.shape[1], t.data_ptr(), 1)
+
+    def cfl_bits(self, t=None, put: bool = False):
+        """The running CFL maximum as an int64 device word (read, or written back)."""
+        t = self._bits if t is None else t
+        self._call("vb_grid_cfl_bits", t.data_ptr(), 1 if put else 0)
+        return t
+
+    def _exchange(self, which):
+        import torch
+        h = self.halo
+
+        def get(first, count):
+            buf = self._bufs["lo" if first == h.act0 else "hi"]
+            return self.get_planes(which, first, count, out=buf)
+
+        def put(first, t):
+            self.put_planes(which, first, t)
+
+        # the collectives order themselves after the library's stream work
+        with torch.cuda.stream(self._stream):
+            h.exchange(get, put, torch.empty_like, self.group)
+
+    def _allreduce_cfl(self):
+        import torch
+        with torch.cuda.stream(self._stream):
+            self.cfl_bits()
+            if self.world > 1:
+                allreduce_max_bits(self._bits, self.group)
+            self.cfl_bits(put=True)
+
+    def step(self, nsteps: int = 1) -> None:
+        """nsteps CFL steps of the whole domain (every rank calls it)."""
+        from . import _lib
+        for _ in range(nsteps):
+            self.phase(_lib.PHASE_CFL)
+            self._allreduce_cfl()
+            self.phase(_lib.PHASE_FINALIZE)
+            self.phase(_lib.PHASE_STAGE1)
+            self._exchange(1)
+            self.phase(_lib.PHASE_STAGE2)
+            self.phase(_lib.PHASE_ADVANCE)
+            self._exchange(0)
+            self.step_count += 1
+
+    def time(self) -> tuple:
+        return self.sim.t, self.sim.step
+
+    def own_state(self):
+        """This rank's planes of the conserved state, (5, nact * ny * nx)."""
+        nx, ny, _ = self.global_dims
+        U = self.sim.state().reshape(5, self.halo.nloc, ny, nx)
+        a = self.halo.act0
+        return U[:, a:a + self.halo.nact].reshape(5, -1)
+
+    def conserved_totals(self):
+        """Totals of the whole domain (all-reduced sum; every rank calls it)."""
+        import numpy as np
+        import torch
+        tot = np.array(self.sim_totals())
+        if self.world > 1:
+            t = torch.tensor(tot, dtype=torch.float64, device=self._bits.device)
+            allreduce_sum(t, self.group)
+            tot = t.cpu().numpy()
+        return tot
+
+    def sim_totals(self):
+        from .simulation import conserved_totals
+        return conserved_totals(self.sim)
+
+    def close(self):
+        self.sim.close()
