@@ -145,7 +145,9 @@ def hllc(WL, WR, g, dim):
     v = [torch.where(left, WL[1 + j], WR[1 + j]) for j in range(3)]
     p = torch.where(left, pL, pR)
     un = v[dim - 1]
-    E = p / (g - 1.0) + 0.5 * rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+    # a tensor divisor: torch divides a CUDA tensor by a Python scalar as a
+    # multiplication by its reciprocal, which rounds differently
+    E = p / torch.full_like(p, g - 1.0) + 0.5 * rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
     Fk = [rho * un, (rho * v[0]) * un, (rho * v[1]) * un, (rho * v[2]) * un, (E + p) * un]
     Fk[dim] = Fk[dim] + p
     q = torch.where(star, rho * (SK - un), one)

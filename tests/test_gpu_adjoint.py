@@ -189,3 +189,65 @@ def test_evolve_function_backpropagates_through_the_device_run(vb):
     adj.close()
     sim.close()
     sim2.close()
+
+
+def _frozen_fd_errors(vb, prob, nsteps, every, ncells, h_rel, seed=3):
+    """The device adjoint's gradient of int rho^2 against central differences
+    of the step map with the branch choices of the unperturbed device run
+    frozen: the torch float64 restatement (oracle/adjoint_ref.py) runs on the
+    GPU, records its branch conditions while reproducing the device forward
+    bit for bit, and replays them for the perturbed runs."""
+    from oracle import adjoint_ref as R
+    sim = _sim(vb, prob)
+    U0 = sim.state()
+    adj = vb.Adjoint(sim, nsteps, every)
+    adj.forward(max_steps=nsteps)
+    UT = sim.state()
+    dts = adj.dts()
+    grad = adj.backward(vb.rho2_seed(sim, UT))
+    V = sim.backend.cell_volume()
+    adj.close()
+    sim.close()
+    grid = _grid(prob)
+    dev = torch.device("cuda")
+    tape = R.Tape(record=True)
+    with torch.no_grad():
+        UT_t = R.evolve(grid, torch.tensor(U0, device=dev), dts, tape=tape)
+        assert np.array_equal(UT_t.cpu().numpy(), UT)  # the device run's branches
+        del UT_t
+        errs = []
+        for cell in np.random.default_rng(seed).choice(U0.shape[1], size=ncells, replace=False):
+            h = h_rel * U0[0, cell]
+            Up = U0.copy(); Up[0, cell] += h
+            Um = U0.copy(); Um[0, cell] -= h
+            rp = R.evolve(grid, torch.tensor(Up, device=dev), dts, tape=tape.replay())[0]
+            rm = R.evolve(grid, torch.tensor(Um, device=dev), dts, tape=tape.replay())[0]
+            fd = float(((rp - rm) * (rp + rm)).sum().item()) * V / (2.0 * h)
+            errs.append(abs(fd - grad[0, cell]) / abs(grad[0, cell]))
+    del tape
+    torch.cuda.empty_cache()
+    return np.array(errs)
+
+
+def test_kh512_as_specified_matches_frozen_map_differences(vb):
+    """The KH 512^2 configuration exactly as specified (no texture), 200
+    steps with checkpoints every 20: at 32 random cells the adjoint agrees
+    with central differences of the frozen-branch map to 1e-6 relative,
+    every cell."""
+    prob = vb.kelvin_helmholtz_problem(n=512)
+    errs = _frozen_fd_errors(vb, prob, 200, 20, 32, 1e-6)
+    assert errs.max() <= 1e-6, errs
+
+
+@pytest.mark.xfail(reason="the KH state as specified starts on minmod kinks (a = b = 0 in "
+                          "every uniform band), where the step map has only one-sided "
+                          "derivatives: central differences of the plain map measured max "
+                          "1.1e-4 and 53 % of 32 cells within 1e-6 over 200 steps; the "
+                          "frozen-branch check above is the one that reaches 1e-6",
+                   strict=False)
+def test_kh512_as_specified_plain_differences_every_cell(vb):
+    """The strict form of the plain check on the configuration as specified:
+    every one of 32 cells within 1e-6 (expected to fail, see the marker)."""
+    prob = vb.kelvin_helmholtz_problem(n=512)
+    errs = _fd_errors(vb, prob, 200, 20, 32, 1e-6)
+    assert errs.max() <= 1e-6, errs

@@ -70,6 +70,15 @@ struct vb_amr {
     vb::AmrDev dev{};
     vb::AmrAreas areas{};
     double ms_regrid = 0.0;
+    // device-driven subcycling: per-level loop state, error bits, and the
+    // graph of one root step (nested WHILE nodes, one per level), valid for
+    // the table version and deepest level it was built for
+    vb::AmrSubLevel *sub = nullptr;
+    int *suberr = nullptr;
+    cudaGraphExec_t sg_exec = nullptr;
+    int64_t sg_version = -1;
+    int64_t table_version = 0;
+    int sg_launches = 0;
 };
 
 namespace {
@@ -78,6 +87,9 @@ double level_width(const vb_amr *a, int l, int d) { return a->w0[d] * std::ldexp
 
 void release(vb_amr *a)
 {
+    if (a->sg_exec) cudaGraphExecDestroy(a->sg_exec);
+    cudaFree(a->sub);
+    cudaFree(a->suberr);
     void *p[] = {a->U, a->U1, a->U2, a->lev2, a->cx2, a->reg, a->lev, a->cx, a->rep, a->faceid, a->kind, a->off,
                  a->fbase, a->cnt, a->fcnt, a->ecnt, a->bsum, a->tag, a->F, a->farea,
                  a->fL, a->fR, a->ent, a->fax, a->hkey, a->hval, a->word, a->ctrl,
@@ -224,6 +236,7 @@ int build_tables(vb_amr *a)
     m.off = a->off;
     m.ent = a->ent;
     m.reg = a->reg;
+    ++a->table_version;  // kernels capture the tables by value: graphs are stale
     return VB_OK;
 }
 
@@ -358,33 +371,150 @@ inline double jmin(double x, double y)
     return y < x ? y : x;
 }
 
-// evolve_level! (src/driver.jl:553-578)
-int evolve_level(vb_amr *a, int level, double dt_target, bool has_parent)
+// ---- device-driven subcycling: evolve_level! as nested CUDA-graph loops ----
+//
+// One root step is one graph.  Level l contributes, in the graph of its
+// parent's substep body (the root graph for level 0): its CFL maximum, a plan
+// node (substep count and dt from that maximum and the dt target: the
+// parent's substep dt), and a WHILE node whose body is one substep -- zero the
+// level's flux registers when a finer level exists, the two stages with the
+// substep dt read on the device, then (with a finer level) that level's own
+// CFL / plan / WHILE nodes and the reflux, and finally a node that counts the
+// substep and sets the loop condition.  Every loop is bounded
+// (AMR_MAX_SUBSTEPS) and stops on the first error bit, so the graph always
+// ends.  The kernels and their order are those of the host recursion below,
+// with the same dt values, so the results are the same bits.
+
+struct SubBody {
+    cudaGraph_t graph;
+    int level;
+    cudaGraphConditionalHandle handle;
+};
+
+// In the graph being captured on `s`: level l's CFL maximum, plan and WHILE
+// node; the node's (empty) body goes to `todo`.
+int emit_level_head(vb_amr *a, cudaStream_t s, int l, std::vector<SubBody> &todo)
 {
-    double dt_stable;
-    int rc = compute_dt_level(a, level, &dt_stable);
-    if (rc) return rc;
-    if (!std::isfinite(dt_stable)) return VB_OK;
-    const double q = std::ceil(dt_target / dt_stable * (1 - 1e-12));
-    const int64_t n = q < 1.0 ? 1 : (int64_t)q;
-    const double dt_sub = dt_target / (double)n;
-    const bool has_finer = level < max_level(a);
-    cudaStream_t st = a->ctx->stream;
-    for (int64_t k = 0; k < n; ++k) {
-        if (has_finer) VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_zero_reg(a->dev, level, st));
-        int rl[2] = {0, 0};
-        double rsc[2] = {0.0, 0.0};
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    VB_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps));
+    if (st != cudaStreamCaptureStatusActive || !g) return fail(VB_ECUDA, "subcycle graph: no capture");
+    cudaGraphConditionalHandle h;
+    VB_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_cfl_bits(a->dev, a->U, l, &a->sub[l].invdt_bits, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_sub_plan(a->sub, l, a->g.cfl,
+                                                    l > 0 ? &a->sub[l - 1].dt_sub : nullptr, h,
+                                                    a->suberr, s));
+    VB_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    VB_CUDA(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
+    VB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    todo.push_back({cp.conditional.phGraph_out[0], l, h});
+    return VB_OK;
+}
+
+// Capture one substep of level b.level into its WHILE body (b by value: the
+// nested head appends to `todo`).
+int fill_level_body(vb_amr *a, cudaStream_t s, SubBody b, std::vector<SubBody> &todo)
+{
+    const int l = b.level;
+    const bool has_finer = l < a->maxlev;
+    VB_CUDA(cudaStreamBeginCaptureToGraph(s, b.graph, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal));
+    int rc = VB_OK;
+    auto body = [&]() -> int {
+        if (has_finer) VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_zero_reg(a->dev, l, s));
+        vb::AmrStageArgs sa{};
+        sa.dt = 0.0;
+        sa.level = l;
+        sa.dt_dev = &a->sub[l].dt_sub;
         int nr = 0;
-        if (has_parent) { rl[nr] = level - 1; rsc[nr] = 1.0 * (0.5 * dt_sub); ++nr; }
-        if (has_finer) { rl[nr] = level; rsc[nr] = -1.0 * (0.5 * dt_sub); ++nr; }
-        rc = step_level(a, dt_sub, level, nr, rl, rsc);
-        if (rc) return rc;
+        if (l > 0) { sa.reg_level[nr] = l - 1; sa.reg_scale[nr] = 1.0; ++nr; }
+        if (has_finer) { sa.reg_level[nr] = l; sa.reg_scale[nr] = -1.0; ++nr; }
+        sa.nreg = nr;
+        sa.cfl_all = 0;
+        VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_stage(a->dev, 1, a->U, a->U, a->U1, a->F, sa, a->ctrl, s));
+        VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_stage(a->dev, 2, a->U1, a->U, a->U, a->F, sa, a->ctrl, s));
         if (has_finer) {
-            rc = evolve_level(a, level + 1, dt_sub, true);
-            if (rc) return rc;
-            VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_reflux(a->dev, a->U, level, st));
+            int r = emit_level_head(a, s, l + 1, todo);
+            if (r) return r;
+            VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_reflux(a->dev, a->U, l, s));
+        }
+        VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_sub_next(a->sub, l, b.handle, a->suberr, s));
+        return VB_OK;
+    };
+    rc = body();
+    cudaGraph_t out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &out);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(VB_ECUDA, std::string("subcycle body capture: ") + cudaGetErrorString(e));
+    return VB_OK;
+}
+
+// The graph of one root step for the current tables (rebuilt after a regrid).
+int build_subcycle_graph(vb_amr *a)
+{
+    if (a->sg_exec) {
+        cudaGraphExecDestroy(a->sg_exec);
+        a->sg_exec = nullptr;
+    }
+    if (!a->sub) {
+        VB_CUDA(cudaMalloc(&a->sub, sizeof(vb::AmrSubLevel) * (vb::AMR_MAX_LEVEL + 1)));
+        VB_CUDA(cudaMalloc(&a->suberr, sizeof(int)));
+    }
+    cudaStream_t s = a->ctx->stream;
+    const int64_t launches0 = a->ctx->launches;
+    cudaGraph_t root = nullptr;
+    VB_CUDA(cudaGraphCreate(&root, 0));
+    std::vector<SubBody> todo;
+    int rc = VB_OK;
+    cudaError_t e = cudaStreamBeginCaptureToGraph(s, root, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) rc = fail(VB_ECUDA, std::string("subcycle capture: ") + cudaGetErrorString(e));
+    if (!rc) {
+        rc = emit_level_head(a, s, 0, todo);
+        cudaGraph_t out = nullptr;
+        e = cudaStreamEndCapture(s, &out);
+        if (!rc && e != cudaSuccess)
+            rc = fail(VB_ECUDA, std::string("subcycle capture: ") + cudaGetErrorString(e));
+    }
+    for (size_t i = 0; i < todo.size() && !rc; ++i) rc = fill_level_body(a, s, todo[i], todo);
+    if (!rc) {
+        e = cudaGraphInstantiate(&a->sg_exec, root, 0);
+        if (e != cudaSuccess) {
+            a->sg_exec = nullptr;
+            rc = fail(VB_ECUDA, std::string("subcycle graph instantiate: ") + cudaGetErrorString(e));
         }
     }
+    cudaGraphDestroy(root);
+    a->sg_launches = (int)(a->ctx->launches - launches0);
+    a->ctx->launches = launches0;  // counted when the graph runs
+    if (rc) {
+        cudaGetLastError();
+        return rc;
+    }
+    a->sg_version = a->table_version;
+    return VB_OK;
+}
+
+// One subcycled root step of dt_root on the device (evolve_level!(sim, 0,
+// dt_root)); the host reads the error bits back with the next control-block
+// read.
+int root_step_graph(vb_amr *a, double dt_root)
+{
+    cudaStream_t s = a->ctx->stream;
+    VB_CUDA(cudaMemsetAsync(a->sub, 0, sizeof(vb::AmrSubLevel) * (vb::AMR_MAX_LEVEL + 1), s));
+    VB_CUDA(cudaMemsetAsync(a->suberr, 0, sizeof(int), s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_sub_target(a->sub, dt_root, s));
+    VB_CUDA(cudaGraphLaunch(a->sg_exec, s));
+    a->ctx->launches += a->sg_launches;  // nodes of one pass (loops repeat some)
     return VB_OK;
 }
 
@@ -688,20 +818,39 @@ int vb_amr_evolve(vb_amr *a, double tfinal, int64_t max_steps, double refine_abo
         return VB_OK;
     };
     if (subcycle) {
+        // each root step runs as one graph: the recursion over the levels,
+        // their substep counts and dts all on the device
+        int errbits = 0;
         while (a->t < tfinal * (1 - 1e-12)) {
             if (max_steps >= 0 && done >= max_steps) break;
             rc = do_regrid();
             if (rc) return rc;
             double dt0;
-            rc = compute_dt_level(a, 0, &dt0);
+            rc = compute_dt_level(a, 0, &dt0);  // also synchronises the previous root step
             if (rc) return rc;
+            if (a->sub) {
+                VB_CUDA(cudaMemcpy(&errbits, a->suberr, sizeof(int), cudaMemcpyDeviceToHost));
+                if (errbits) break;
+            }
             const double dt_root = jmin(dt0, tfinal - a->t);
-            rc = evolve_level(a, 0, dt_root, false);
+            if (a->sg_version != a->table_version) {
+                rc = build_subcycle_graph(a);
+                if (rc) return rc;
+            }
+            rc = root_step_graph(a, dt_root);
             if (rc) return rc;
             a->t += dt_root;
             a->step += 1;
             ++done;
         }
+        if (!errbits && a->sub) {
+            VB_CUDA(cudaStreamSynchronize(st));
+            VB_CUDA(cudaMemcpy(&errbits, a->suberr, sizeof(int), cudaMemcpyDeviceToHost));
+        }
+        if (errbits & vb::AMR_SUB_NONFINITE)
+            return fail(VB_ENONFINITE, "non-finite dt: NaN or negative density/pressure");
+        if (errbits & vb::AMR_SUB_TOO_MANY)
+            return fail(VB_ENONFINITE, "a level needed more than 2^20 substeps");
     } else {
         // single rate: dt, stages and clock on the device between regrids
         vb::Geom gq = a->g;  // finalize kernel reads cfl (its invV is unused here)

@@ -38,7 +38,28 @@ struct AmrStageArgs {
     int reg_level[2];
     double reg_scale[2];
     int cfl_all;
+    // set: dt is read from here (a subcycled level's substep dt, computed on
+    // the device) and reg_scale holds the register signs (+1 / -1), the scale
+    // being sign * (0.5 * dt) as evolve_level! forms it
+    const double *dt_dev;
 };
+
+// Device state of one level of a subcycled root step (evolve_level!,
+// src/driver.jl:553-578), for the graph that runs the recursion on the
+// device: the dt target handed down (the parent's substep dt; the root step's
+// dt at level 0), the substep dt and count, the level's CFL maximum.
+struct AmrSubLevel {
+    double dt_target;
+    double dt_sub;
+    unsigned long long invdt_bits;
+    long long left;   // substeps still to run
+    long long iters;  // substeps run so far
+};
+// A level runs at most this many substeps per parent substep; beyond it the
+// root step stops with VB_ENONFINITE-like error bits (a non-finite or
+// vanishing dt, never a sound run).
+constexpr long long AMR_MAX_SUBSTEPS = 1ll << 20;
+enum { AMR_SUB_NONFINITE = 1, AMR_SUB_TOO_MANY = 2 };
 
 // Topology view for the regrid kernels (vb_amr_regrid.cu).
 struct AmrTopo {
@@ -79,6 +100,19 @@ int launch_amr_csr_fill(const AmrTopo &t, const int8_t *kind, const int *rep, co
 int launch_amr_stage(const AmrDev &m, int stage, const double *Uin, const double *U0,
                      double *Uout, double *F, const AmrStageArgs &a, Ctrl *ctrl, cudaStream_t s);
 int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cudaStream_t s);
+// The same maximum into the word `bits` (not reset here).
+int launch_amr_cfl_bits(const AmrDev &m, const double *U, int level, unsigned long long *bits,
+                        cudaStream_t s);
+// Device-driven subcycling (graph nodes, one thread each).  plan: from the
+// level's CFL maximum and its dt target (the parent's substep dt when
+// `target_src` is set) the substep count and dt, and the WHILE condition
+// `h` of the level's substep loop; next: one substep done, condition for
+// the next.  Error bits go to *err.
+int launch_amr_sub_plan(AmrSubLevel *sub, int level, double cfl, const double *target_src,
+                        cudaGraphConditionalHandle h, int *err, cudaStream_t s);
+int launch_amr_sub_next(AmrSubLevel *sub, int level, cudaGraphConditionalHandle h, int *err,
+                        cudaStream_t s);
+int launch_amr_sub_target(AmrSubLevel *sub, double dt, cudaStream_t s);
 int launch_amr_tag(const AmrDev &m, const double *U, double above, int max_level, uint8_t *tag,
                    double *ind, int *ntag, cudaStream_t s);
 int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s);

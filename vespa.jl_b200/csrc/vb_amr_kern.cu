@@ -90,9 +90,12 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
             const double *__restrict__ F, AmrStageArgs a, Ctrl *ctrl)
 {
     __shared__ double red[32];
-    // a.dt < 0: dt from the control block, and nothing to do once inactive
+    // a.dt < 0: dt from the control block, and nothing to do once inactive;
+    // a.dt_dev: a subcycled level's substep dt
     double dt = a.dt;
-    if (dt < 0.0) {
+    if (a.dt_dev) {
+        dt = *a.dt_dev;
+    } else if (dt < 0.0) {
         if (!ctrl->active) return;
         dt = ctrl->dt;
     }
@@ -106,7 +109,9 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
             if (a.reg_level[r] == li) rslot = r;
         if (upd || rslot >= 0) {
             double acc[5] = {0, 0, 0, 0, 0}, rg[5];
-            const double rs = rslot >= 0 ? a.reg_scale[rslot] : 0.0;
+            const double rs = rslot < 0 ? 0.0
+                              : a.dt_dev ? a.reg_scale[rslot] * (0.5 * dt)
+                                         : a.reg_scale[rslot];
             if (rslot >= 0)
 #pragma unroll
                 for (int k = 0; k < 5; ++k) rg[k] = m.reg[(int64_t)k * m.cap + i];
@@ -181,6 +186,75 @@ __global__ void __launch_bounds__(256) k_amr_cfl(AmrDev m, const double *__restr
     }
     block_max_to(&ctrl->invdt_bits, invdt, red);
 }
+
+// the same maximum into a given word
+__global__ void __launch_bounds__(256) k_amr_cfl_bits(AmrDev m, const double *__restrict__ U,
+                                                      int level, unsigned long long *bits)
+{
+    __shared__ double red[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double invdt = 0.0;
+    if (i < m.nleaf && (level < 0 || m.lev[i] == level)) {
+        double W[5];
+        amr_prim(m, U, i, W);
+        const double c = sqrt(m.gamma * W[4] / W[0]);
+        for (int d = 0; d < m.nd; ++d)
+            invdt = nan_max(invdt, (fabs(W[1 + d]) + c) / m.w[m.lev[i]][d]);
+    }
+    block_max_to(bits, invdt, red);
+}
+
+// evolve_level!'s head (src/driver.jl:555-560) on the device: dt_stable from
+// the level's CFL maximum, n = max(1, ceil(target / dt_stable * (1 - 1e-12)))
+// substeps of target / n; no substeps when dt_stable is not finite (a level
+// at rest or without leaves).  The maximum word is reset for its next use.
+__global__ void k_amr_sub_plan(AmrSubLevel *sub, int level, double cfl, const double *target_src,
+                               cudaGraphConditionalHandle h, int *err)
+{
+    AmrSubLevel &L = sub[level];
+    const double target = target_src ? *target_src : L.dt_target;
+    L.dt_target = target;
+    const double invdt = __longlong_as_double((long long)L.invdt_bits);
+    L.invdt_bits = 0ull;
+    L.left = 0;
+    L.iters = 0;
+    if (invdt != invdt || *err) {
+        atomicOr(err, invdt != invdt ? AMR_SUB_NONFINITE : 0);
+        cudaGraphSetConditional(h, 0);
+        return;
+    }
+    const double dt_stable = invdt == 0.0 ? (double)INFINITY : cfl / invdt;
+    if (!(dt_stable < (double)INFINITY)) {
+        cudaGraphSetConditional(h, 0);
+        return;
+    }
+    const double q = ceil(target / dt_stable * (1 - 1e-12));
+    if (!(q <= (double)AMR_MAX_SUBSTEPS)) {
+        atomicOr(err, AMR_SUB_TOO_MANY);
+        cudaGraphSetConditional(h, 0);
+        return;
+    }
+    const long long n = q < 1.0 ? 1 : (long long)q;
+    L.dt_sub = target / (double)n;
+    L.left = n;
+    cudaGraphSetConditional(h, 1);
+}
+
+// end of one substep of the level's loop: the condition for another
+__global__ void k_amr_sub_next(AmrSubLevel *sub, int level, cudaGraphConditionalHandle h, int *err)
+{
+    AmrSubLevel &L = sub[level];
+    L.left -= 1;
+    L.iters += 1;
+    bool more = L.left > 0 && *err == 0;
+    if (L.iters >= AMR_MAX_SUBSTEPS) {
+        atomicOr(err, AMR_SUB_TOO_MANY);
+        more = false;
+    }
+    cudaGraphSetConditional(h, more ? 1 : 0);
+}
+
+__global__ void k_amr_sub_target(AmrSubLevel *sub, double dt) { sub[0].dt_target = dt; }
 
 // density_gradient_indicator (src/driver.jl:406-420) and the regrid! tag
 __global__ void __launch_bounds__(256) k_amr_tag(AmrDev m, const double *__restrict__ U,
@@ -261,7 +335,8 @@ int launch_amr_stage(const AmrDev &m, int stage, const double *Uin, const double
                      double *Uout, double *F, const AmrStageArgs &a, Ctrl *ctrl, cudaStream_t s)
 {
     if (m.nface > 0)
-        k_amr_faces<<<blocks(m.nface, 256), 256, 0, s>>>(m, Uin, F, a.dt < 0.0 ? ctrl : nullptr);
+        k_amr_faces<<<blocks(m.nface, 256), 256, 0, s>>>(m, Uin, F,
+                                                         (a.dt < 0.0 && !a.dt_dev) ? ctrl : nullptr);
     if (stage == 1)
         k_amr_cells<1><<<blocks(m.nleaf, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
     else
@@ -272,6 +347,33 @@ int launch_amr_stage(const AmrDev &m, int stage, const double *Uin, const double
 int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cudaStream_t s)
 {
     k_amr_cfl<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, level, ctrl);
+    return 1;
+}
+
+int launch_amr_cfl_bits(const AmrDev &m, const double *U, int level, unsigned long long *bits,
+                        cudaStream_t s)
+{
+    k_amr_cfl_bits<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, level, bits);
+    return 1;
+}
+
+int launch_amr_sub_plan(AmrSubLevel *sub, int level, double cfl, const double *target_src,
+                        cudaGraphConditionalHandle h, int *err, cudaStream_t s)
+{
+    k_amr_sub_plan<<<1, 1, 0, s>>>(sub, level, cfl, target_src, h, err);
+    return 1;
+}
+
+int launch_amr_sub_next(AmrSubLevel *sub, int level, cudaGraphConditionalHandle h, int *err,
+                        cudaStream_t s)
+{
+    k_amr_sub_next<<<1, 1, 0, s>>>(sub, level, h, err);
+    return 1;
+}
+
+int launch_amr_sub_target(AmrSubLevel *sub, double dt, cudaStream_t s)
+{
+    k_amr_sub_target<<<1, 1, 0, s>>>(sub, dt);
     return 1;
 }
 

@@ -105,7 +105,7 @@ __device__ __noinline__ void stage_abandon(uint64_t *bars, int qb, int q, int np
 // that solved domain-boundary face (axis d, side) adds (scale * F) * area to
 // entry `idx` of that plane (the other axes column-major, lowest fastest).
 // Each entry belongs to one face, hence to one thread of the launch.
-static __device__ __noinline__ void bflux_add(const Geom &g, double *bf, int d, int side, int64_t idx,
+static __device__ __forceinline__ void bflux_add(const Geom &g, double *bf, int d, int side, int64_t idx,
                                        double scale, double area, const double F[5])
 {
     int64_t off = 0;
