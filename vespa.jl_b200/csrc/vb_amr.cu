@@ -363,8 +363,6 @@ int step_level(vb_amr *a, double dt, int level, int nreg, const int *rl, const d
     return VB_OK;
 }
 
-int max_level(const vb_amr *a) { return a->maxlev; }
-
 inline double jmin(double x, double y)
 {
     if (x != x || y != y) return x + y;
