@@ -104,16 +104,21 @@ __device__ __noinline__ void stage_abandon(uint64_t *bars, int qb, int q, int np
 // _bflux_capture!, src/reflux.jl:125-132, for the tiled kernels: the thread
 // that solved domain-boundary face (axis d, side) adds (scale * F) * area to
 // entry `idx` of that plane (the other axes column-major, lowest fastest).
-// Each entry belongs to one face, hence to one thread of the launch.
-static __device__ __forceinline__ void bflux_add(const Geom &g, double *bf, int d, int side, int64_t idx,
-                                       double scale, double area, const double F[5])
+// Each entry belongs to one face, hence to one thread of the launch, and the
+// launches of a step are ordered, so the sum is the serial one; the add is a
+// fire-and-forget reduction (no value returned), so the solving warp does not
+// wait for the register's memory before the block's next barrier.
+static __device__ __forceinline__ void bflux_add(const Geom &g, double *bf, int d, int side,
+                                                 int64_t idx, double scale, double area,
+                                                 const double F[5])
 {
-    int64_t off = 0;
-    for (int e = 0; e < d; ++e) off += 2 * 5 * (g.ncell / g.n[e]);
-    const int64_t P = g.ncell / g.n[d];
+    // plane sizes as products of the other axes (ncell / n[e] without a division)
+    const int64_t P0 = g.n[1] * g.n[2], P1 = g.n[0] * g.n[2], P2 = g.n[0] * g.n[1];
+    const int64_t P = d == 0 ? P0 : (d == 1 ? P1 : P2);
+    int64_t off = d == 0 ? 0 : (d == 1 ? 10 * P0 : 10 * (P0 + P1));
     off += (int64_t)side * 5 * P + idx;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) bf[off + k * P] += scale * F[k] * area;
+    for (int k = 0; k < 5; ++k) atomicAdd(bf + off + k * P, scale * F[k] * area);
 }
 
 __device__ __forceinline__ int lo_class(int64_t c, int64_t n, bool periodic)

@@ -171,8 +171,9 @@ class SlabSimulation:
                           dims=(nx, ny, h.nloc), domain=((x0, x1), (y0, y1),
                                                          (zd0 + (h.z0 - h.g_lo) * wz,
                                                           zd0 + (h.z0 - h.g_lo + h.nloc) * wz)),
-                          gamma=problem.gamma, bcs=bcs, init=problem.init, tfinal=math.inf,
-                          cfl=problem.cfl)
+                          gamma=problem.gamma, bcs=bcs, tfinal=math.inf, cfl=problem.cfl,
+                          # the slab's state comes from the whole domain's (below)
+                          init=lambda x, y, z: (1.0, 0.0, 0.0, 0.0, 1.0))
         self.ctx = ctx or default_context()
         self.planes = h.global_planes(nz)
         if initial is None:
