@@ -357,7 +357,7 @@ def run_ours(args, ranks: Ranks):
         ms_max = ranks.max(ms)
         finals[prec] = sim.state()[0]  # density after W + K steps, for the L1 check
         out[prec] = {"ms": ms_max, "launches": launches, "kernel": sim.kernel, "kz": kz,
-                     **sim.profile_step(5)}
+                     "taper": sim.taper, **sim.profile_step(5)}
         sim.close()
     # accuracy statement: density L1 of the mixed path against float64
     l1_mixed = float(np.sum(np.abs(finals["mixed"] - finals["fp64"])) /
@@ -425,13 +425,16 @@ def run_ours(args, ranks: Ranks):
         "data": DATA,
         "config": {"workload": workload(n),
                    "cells_per_gpu": cells, "precision": "mixed", "kernel": mixed["kernel"],
-                   "tile": f"16x16 columns, z chunk {mixed['kz']} (autotuned)",
+                   "tile": f"16x16 columns, z chunk {mixed['kz']}, "
+                           f"{'tapered' if mixed['taper'] else 'uniform'} work queue (autotuned)",
                    "l2": "inputs larger than L2 (671 MB per state buffer)",
                    "parallelism": f"one independent instance per GPU x{ranks.world}"},
         "accuracy": {"l1_rho_mixed_vs_fp64_rel": l1_mixed, "after_steps": W + K,
                      "bound": 1e-6},
         "fp64": {"value": round(fp64_value, 1), "unit": UNIT,
                  "ms_per_step": round(out["fp64"]["ms"] / K, 4),
+                 "tile": f"16x16 columns, z chunk {out['fp64']['kz']}, "
+                         f"{'tapered' if out['fp64']['taper'] else 'uniform'} work queue (autotuned)",
                  "speedup_mixed_over_fp64": round(value / fp64_value, 3),
                  "roofline": roofline(out["fp64"], "stage2_fp64")},
         "roofline": roofline(mixed, "stage2_mixed"),

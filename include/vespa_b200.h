@@ -133,16 +133,18 @@ int vb_grid_device_state(vb_grid *grid, double **dU);
  * tiled 3D kernel when the grid allows it (nx, ny multiples of 16, nz >= 2),
  * VB_KERNEL_CELL forces the cell-centric kernel, VB_KERNEL_TILED requires the
  * tiled one.  VB_OPT_TILE_KZ: z planes per tiled work item.
- * VB_OPT_TILE_TAPER: -1 (default) tapers the 3D work queue's last z chunks
- * for VB_MIXED grids only, 0 keeps uniform chunks, 1 tapers in either
- * precision.  Results do not depend on any of these knobs. */
+ * VB_OPT_TILE_TAPER: -1 (default) lets the autotuner choose whether the 3D
+ * work queue's last z chunks taper (untuned: VB_MIXED grids taper), 0 keeps
+ * uniform chunks, 1 tapers in either precision.  Results do not depend on
+ * any of these knobs. */
 enum { VB_OPT_KERNEL = 1, VB_OPT_TILE_KZ = 2, VB_OPT_TILE_TAPER = 3 };
 enum { VB_KERNEL_AUTO = 0, VB_KERNEL_CELL = 1, VB_KERNEL_TILED = 2 };
 int vb_grid_set_option(vb_grid *grid, int option, int64_t value);
 int vb_grid_get_option(const vb_grid *grid, int option, int64_t *value);
 /* Autotuner (no counterpart in the reference): times the tiled kernel's
  * z-chunk candidates (16 .. 128 planes) on this grid for nsteps CFL steps
- * each, keeps the fastest, and restores the state and clock.  The choice is
+ * each -- on 3D grids with VB_OPT_TILE_TAPER at -1 both as uniform and as
+ * tapered work queues -- keeps the fastest, and restores the state and clock.  The choice is
  * cached for the process per (device, dims, boundaries, precision) and later
  * grids of the same kind start from it.  Allocates one state-sized scratch
  * buffer for the duration of the call.  No-op (returns the current kz) when

@@ -9,7 +9,8 @@ bit-identical to the serial face loop) on all host threads:
   the same run on the tapered work queue that the mixed-precision headline
   uses (chunks of 128, 64, 32, 16, 8, 8 planes): 2 steps, bit-identical;
 - 4096^2 periodic, VB_FP64 on the tiled 2D kernel: 2 steps, bit-identical;
-- 256^3 VB_MIXED: the tapered queue is bit-identical to uniform chunks, and
+- 256^3 VB_MIXED: the tapered queue (at the autotuned chunk) is
+  bit-identical to uniform chunks, and
   after the benchmark's 3 + 20 steps the density L1 error against VB_FP64 is
   at most 1e-6 relative, with the five totals conserved to 1e-12.
 
@@ -68,8 +69,8 @@ def test_cube256_fp64_autotuned_tiled_bit_identical(vb, cube, cube_oracle_2steps
     t_ref, U_ref = cube_oracle_2steps
     sim = make_sim(vb, prob, U0, "fp64")
     sim.set_kernel("tiled")
-    kz, _ = sim.autotune(3)  # the benchmark's setup; state and clock restored
-    assert sim.kz == kz and not sim.taper
+    kz, _ = sim.autotune(3)  # the benchmark's setup (chunk and queue shape); state restored
+    assert sim.kz == kz
     vb.evolve(sim, max_steps=2)
     assert sim.step == 2 and sim.t == t_ref
     assert_bit_identical(sim.state(), U_ref)
@@ -108,6 +109,7 @@ def test_cube256_mixed_taper_bits_and_l1_against_fp64(vb, cube):
     tap = make_sim(vb, prob, U0, "mixed")
     tap.set_kernel("tiled")
     kz, _ = tap.autotune(3)
+    tap.set_kernel("tiled", kz=kz, taper=True)
     assert tap.taper
     t0 = np.array(vb.conserved_totals(tap))
     vb.evolve(tap, max_steps=BENCH_STEPS)

@@ -97,7 +97,7 @@ int encode_state_map(CUtensorMap *m, const double *base, const vb::Geom &g, uint
 
 // Autotuned z-chunk per (device, dims, boundaries, precision), process-wide.
 std::mutex g_tune_mu;
-std::map<std::string, int> g_tune_kz;
+std::map<std::string, std::pair<int, int>> g_tune_kz;  // (kz, tapered queue: 0 / 1 / -1 untuned)
 
 std::string tune_key(int device, const vb::Geom &g, int precision)
 {
@@ -279,7 +279,9 @@ using vb::detail::make_box;
 // by default single VB_MIXED grids do).
 bool grid_taper(const vb_grid *gr)
 {
-    return gr->taper < 0 ? gr->precision == VB_MIXED : gr->taper != 0;
+    if (gr->taper >= 0) return gr->taper != 0;
+    if (gr->taper_tuned >= 0) return gr->taper_tuned != 0;
+    return gr->precision == VB_MIXED;
 }
 
 // Refresh the grid's box descriptor after kz, the taper (or the maps) changed.
@@ -655,7 +657,10 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
         gr->kz = vb::detail::grid_default_kz(g);
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_kz.find(tune_key(ctx->device, g, precision));
-        if (it != g_tune_kz.end()) gr->kz = it->second;
+        if (it != g_tune_kz.end()) {
+            gr->kz = it->second.first;
+            gr->taper_tuned = it->second.second;
+        }
     }
     *out = gr;
     return VB_OK;
@@ -678,16 +683,21 @@ int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
     rc = pull_ctrl(gr);
     vb::Ctrl ctrl0 = *gr->hctrl;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    int best = gr->kz;
+    int best = gr->kz, best_taper = gr->taper_tuned;
     float best_t = INFINITY;
     if (!rc && (cudaMemcpyAsync(save, gr->U, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
                 cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
         rc = fail(VB_ECUDA, "autotune setup failed");
+    // candidates: z chunk (3D planes / 2D rows) and, in 3D when the caller
+    // left VB_OPT_TILE_TAPER at its default, uniform or tapered work queues
     const int cand[] = {16, 24, 32, 40, 48, 64, 96, 128};
-    for (int kz : cand) {
+    const int ntaper = (gr->g.nd == 3 && gr->taper < 0) ? 2 : 1;
+    for (int ci = 0; ci < 8 * ntaper; ++ci) {
+        const int kz = cand[ci % 8];
         if (rc) break;
         if (kz > vb::march_extent(gr->g)) continue;
         gr->kz = kz;
+        if (ntaper == 2) gr->taper_tuned = ci / 8;
         rc = ensure_cfl(gr);
         if (!rc) rc = queue_steps(gr, 1);  // warm-up
         // capture this chunk's step graph before the timed region, so that
@@ -709,6 +719,7 @@ int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
         if (ms < best_t) {
             best_t = ms;
             best = kz;
+            best_taper = gr->taper_tuned;
         }
     }
     // restore the state and the clock whatever happened
@@ -720,11 +731,12 @@ int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
     if (e1) cudaEventDestroy(e1);
     gr->invdt_valid = false;
     gr->kz = best;
+    gr->taper_tuned = best_taper;
     if (rc) return rc;
     if (rc2) return rc2;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tune_kz[tune_key(gr->ctx->device, gr->g, gr->precision)] = best;
+        g_tune_kz[tune_key(gr->ctx->device, gr->g, gr->precision)] = {best, best_taper};
     }
     if (best_kz) *best_kz = best;
     if (best_ms) *best_ms = best_t / nsteps;

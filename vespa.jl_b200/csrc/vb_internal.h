@@ -40,7 +40,8 @@ struct vb_grid {
     vb::TiledMaps maps_U{}, maps_U1{};  // TMA descriptors of the two stage inputs
     vb::BoxDesc box{};                  // the tiled kernels' box descriptor (passed by value)
     int box_kz = 0;                     // kz the descriptor was written with
-    int taper = -1;                     // tapered z chunks: -1 auto (VB_MIXED 3D), 0 off, 1 on
+    int taper = -1;                     // tapered z chunks: -1 auto, 0 off, 1 on
+    int taper_tuned = -1;               // auto: the autotuner's choice (-1: none, VB_MIXED tapers)
     int box_taper = -1;                 // taper the descriptor was written with
     // CUDA graph of GRAPH_STEPS steps (finalize + RK2), replayed by the step loop
     cudaGraphExec_t gexec = nullptr;
