@@ -82,6 +82,13 @@ int vb_ctx_synchronize(vb_ctx *ctx);
 int vb_ctx_stream(vb_ctx *ctx, void **stream);
 /* Number of kernels this context has launched so far (graph nodes included). */
 int vb_ctx_launch_count(vb_ctx *ctx, int64_t *count);
+/* Device bounds checks of the check build (-DVB_CHECK: libvespa_b200_check.so,
+ * `make -C vespa.jl_b200/csrc check`).  Waits for the context's stream, then
+ * *line = 0 when no device bounds check failed since the last call, the
+ * source line of the first failed check otherwise (the guarded access was
+ * skipped), and -1 in the normal build, which has no checks.  Clears the
+ * record. */
+int vb_check_read(vb_ctx *ctx, int64_t *line);
 /* CUDA-event timing on the context's stream (the reference's Instrumented
  * span timing, lib/MeshInterface/src/instrument.jl:30-95, moved to device
  * time): vb_ctx_mark records event `slot` (0..15); vb_ctx_elapsed_ms waits
@@ -362,8 +369,10 @@ int vb_muscl_step_fields(vb_muscl *m, double *D, double *S1, double *S2, double 
  * and every step's dt.  vb_adjoint_backward maps dJ/dU at the end of that run
  * (host, the state layout) to dJ/dU at its start, recomputing each segment
  * from its checkpoint.  Device memory: (ceil(max_steps/checkpoint_every) +
- * 2*checkpoint_every + 2 + 2*ndim) states.  The grid must be VB_FP64 and
- * periodic on every side (VB_ENOTSUP otherwise). */
+ * 2*checkpoint_every + 2 + 2*ndim) states.  checkpoint_every = 1 keeps a
+ * tape instead: every step's state and stage-1 state (2*max_steps + 4 +
+ * 2*ndim states), and the reverse sweep recomputes nothing.  The grid must
+ * be VB_FP64 and periodic on every side (VB_ENOTSUP otherwise). */
 typedef struct vb_adjoint vb_adjoint;
 int vb_adjoint_create(vb_grid *grid, int64_t max_steps, int64_t checkpoint_every,
                       vb_adjoint **out);

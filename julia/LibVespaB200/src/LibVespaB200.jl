@@ -141,6 +141,8 @@ vb_ctx_stream(ctx, stream) =
     ccall((:vb_ctx_stream, libvespa_b200), Cint, (Ptr{Cvoid}, Ref{Ptr{Cvoid}}), ctx, stream)
 vb_ctx_launch_count(ctx, count) =
     ccall((:vb_ctx_launch_count, libvespa_b200), Cint, (Ptr{Cvoid}, Ptr{Int64}), ctx, count)
+vb_check_read(ctx, line) =
+    ccall((:vb_check_read, libvespa_b200), Cint, (Ptr{Cvoid}, Ptr{Int64}), ctx, line)
 vb_ctx_mark(ctx, slot) =
     ccall((:vb_ctx_mark, libvespa_b200), Cint, (Ptr{Cvoid}, Cint), ctx, slot)
 vb_ctx_elapsed_ms(ctx, slot_a, slot_b, ms) =

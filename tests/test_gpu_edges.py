@@ -113,3 +113,29 @@ def test_bounded_wait_gives_up_and_reports_a_timeout(vb, oracle):
     with pytest.raises(vb.VespaB200Error) as e:
         _lib.call("vb_grid_selftest_wait", sim.handle, 0)
     assert e.value.status == _lib.VB_EINVAL
+
+
+def test_autotune_cache_file(vb, tmp_path, monkeypatch):
+    """VB_AUTOTUNE_CACHE: a tuning is appended as "key kz taper" (key: GPU
+    model, precision, dims and boundaries), and a grid created later starts
+    from the file's entry for its key."""
+    path = tmp_path / "tune.txt"
+    monkeypatch.setenv("VB_AUTOTUNE_CACHE", str(path))
+    prob = P.smooth_random_problem((64, 64, 40), seed=3)
+    sim = make_sim(prob, P.initial_state(prob))
+    sim.set_kernel("tiled")
+    kz, _ = sim.autotune(1)
+    sim.close()
+    key, kz_file, taper_file = path.read_text().split()
+    assert int(kz_file) == kz and int(taper_file) in (0, 1)
+    parts = key.split(":")
+    assert len(parts) == 5 and parts[2:] == ["64/11", "64/11", "40/11"]
+    # an entry for a shape this process never tuned: the new grid takes it
+    parts[4] = "36/11"
+    with open(path, "a") as f:
+        f.write(f"{':'.join(parts)} 24 1\n")
+    prob2 = P.smooth_random_problem((64, 64, 36), seed=4)
+    sim2 = make_sim(prob2, P.initial_state(prob2))
+    sim2.set_kernel("tiled")
+    assert sim2.kz == 24 and sim2.taper
+    sim2.close()

@@ -32,6 +32,15 @@ def test_library_exports_every_declared_symbol():
     assert L.vb_abi_version() == 1
 
 
+def test_check_build_exports_every_declared_symbol():
+    # the device-bounds-check build of the same sources (make ... check)
+    path = os.path.join(ROOT, "vespa.jl_b200", "libvespa_b200_check.so")
+    assert os.path.exists(path), "build it with `make -C vespa.jl_b200/csrc check`"
+    L = C.CDLL(path)
+    for n in declared_symbols():
+        assert hasattr(L, n), n
+
+
 def test_library_is_self_contained():
     # no dependency on a CUDA runtime being on the loader path
     import subprocess

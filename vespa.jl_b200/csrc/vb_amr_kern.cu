@@ -23,9 +23,10 @@ namespace {
 __device__ __forceinline__ void amr_prim(const AmrDev &m, const double *__restrict__ U, int i,
                                          double W[5])
 {
-    double u[5];
+    double u[5] = {1.0, 0.0, 0.0, 0.0, 1.0};
+    if (VB_DCHECK(i >= 0 && i < m.nleaf))  // check build only
 #pragma unroll
-    for (int k = 0; k < 5; ++k) u[k] = U[(int64_t)k * m.cap + i];
+        for (int k = 0; k < 5; ++k) u[k] = U[(int64_t)k * m.cap + i];
     cons2prim(u, m.gamma, W);
 }
 
@@ -35,6 +36,7 @@ __device__ __forceinline__ void amr_face_value(const AmrDev &m, const double *__
 {
     double Wc[5], Wl[5], Wr[5];
     amr_prim(m, U, i, Wc);
+    if (!VB_DCHECK(i >= 0 && i < m.nleaf)) i = 0;  // check build only (amr_prim flagged it)
     const int jl = m.rep[(2 * ax) * m.cap + i];
     const int jr = m.rep[(2 * ax + 1) * m.cap + i];
     if (jl >= 0) amr_prim(m, U, jl, Wl); else ghost_state<double>(Wc, m.bc_lo[ax], ax, Wl);
@@ -49,6 +51,7 @@ __device__ __forceinline__ void amr_face(const AmrDev &m, const double *__restri
                                          double *__restrict__ F)
 {
     const int L = m.fL[f], R = m.fR[f];
+    if (!VB_DCHECK(L < m.nleaf && R < m.nleaf && (L >= 0 || R >= 0))) return;  // check build only
     constexpr int ax = DIM - 1;
     double WL[5], WR[5], out[5];
     if (L >= 0 && R >= 0) {
@@ -67,11 +70,14 @@ __device__ __forceinline__ void amr_face(const AmrDev &m, const double *__restri
 }
 
 __global__ void __launch_bounds__(256) k_amr_faces(AmrDev m, const double *__restrict__ U,
-                                                   double *__restrict__ F, const Ctrl *gate)
+                                                   double *__restrict__ F, const Ctrl *gate,
+                                                   const int *__restrict__ list, int nlist)
 {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= m.nface) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (list ? nlist : m.nface)) return;
     if (gate && !gate->active) return;
+    const int f = list ? list[t] : t;
+    if (!VB_DCHECK(f >= 0 && f < m.nface)) return;  // check build only
     switch (m.fax[f]) {
     case 0: amr_face<1>(m, U, f, F); break;
     case 1: amr_face<2>(m, U, f, F); break;
@@ -99,9 +105,10 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
         if (!ctrl->active) return;
         dt = ctrl->dt;
     }
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     double invdt = 0.0;
-    if (i < m.nleaf) {
+    const int i = t < (a.cells ? a.ncells : m.nleaf) ? (a.cells ? a.cells[t] : t) : -1;
+    if (i >= 0 && VB_DCHECK(i < m.nleaf)) {  // (the check: check build only)
         const int li = m.lev[i];
         const bool upd = a.level < 0 || li == a.level;
         int rslot = -1;
@@ -117,8 +124,10 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
                 for (int k = 0; k < 5; ++k) rg[k] = m.reg[(int64_t)k * m.cap + i];
             const int e0 = m.off[i], e1 = m.off[i + 1];
             for (int e = e0; e < e1; ++e) {
+                if (!VB_DCHECK(e >= 0 && e < m.nent)) break;  // check build only
                 const int code = m.ent[e];
                 const int f = code >> 1;
+                if (!VB_DCHECK(f >= 0 && f < m.nface)) continue;
                 const bool neg = code & 1;
                 const double ar = m.farea[f];
                 double Fk[5];
@@ -129,7 +138,7 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
                 for (int k = 0; k < 5; ++k) acc[k] = acc[k] + s * Fk[k];
                 if (rslot >= 0) {
                     const int other = neg ? m.fL[f] : m.fR[f];
-                    if (other >= 0 && m.lev[other] == li + 1) {
+                    if (other >= 0 && VB_DCHECK(other < m.nleaf) && m.lev[other] == li + 1) {
                         const double ss = neg ? -rs : rs;
 #pragma unroll
                         for (int k = 0; k < 5; ++k) rg[k] = rg[k] + ss * Fk[k] * ar;
@@ -150,6 +159,7 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
                     else
                         un[k] = 0.5 * U0[o] + 0.5 * (Uin[o] - invV * acc[k]);
                     Uout[o] = un[k];
+                    if (STAGE == 2 && a.mirror) a.mirror[o] = un[k];
                 }
                 if constexpr (STAGE == 2) {
                     double W[5];
@@ -161,7 +171,7 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
             }
         }
         if constexpr (STAGE == 1) {
-            if (!upd)
+            if (!upd && !a.cells)
 #pragma unroll
                 for (int k = 0; k < 5; ++k) Uout[(int64_t)k * m.cap + i] = Uin[(int64_t)k * m.cap + i];
         }
@@ -187,14 +197,16 @@ __global__ void __launch_bounds__(256) k_amr_cfl(AmrDev m, const double *__restr
     block_max_to(&ctrl->invdt_bits, invdt, red);
 }
 
-// the same maximum into a given word
+// the same maximum into a given word; with a list, over its leaves
 __global__ void __launch_bounds__(256) k_amr_cfl_bits(AmrDev m, const double *__restrict__ U,
-                                                      int level, unsigned long long *bits)
+                                                      int level, unsigned long long *bits,
+                                                      const int *__restrict__ list, int nlist)
 {
     __shared__ double red[32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t < (list ? nlist : m.nleaf) ? (list ? list[t] : t) : -1;
     double invdt = 0.0;
-    if (i < m.nleaf && (level < 0 || m.lev[i] == level)) {
+    if (i >= 0 && VB_DCHECK(i < m.nleaf) && (level < 0 || m.lev[i] == level)) {
         double W[5];
         amr_prim(m, U, i, W);
         const double c = sqrt(m.gamma * W[4] / W[0]);
@@ -280,26 +292,68 @@ __global__ void __launch_bounds__(256) k_amr_tag(AmrDev m, const double *__restr
     if (on && ntag) atomicAdd(ntag, 1);
 }
 
-// _reflux_apply! (src/reflux.jl:91-101) for the leaves of one level
-__global__ void k_amr_reflux(AmrDev m, double *U, int level)
+// _reflux_apply! (src/reflux.jl:91-101) for the leaves of one level (with a
+// list: its leaves, and the result mirrored)
+__global__ void k_amr_reflux(AmrDev m, double *U, int level, const int *__restrict__ list,
+                             int nlist, double *mirror)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.nleaf || m.lev[i] != level) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (list ? nlist : m.nleaf)) return;
+    const int i = list ? list[t] : t;
+    if (!VB_DCHECK(i >= 0 && i < m.nleaf) || m.lev[i] != level) return;
     const double invV = 1.0 / m.vol[level];
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
         const int64_t o = (int64_t)k * m.cap + i;
-        U[o] = U[o] - invV * m.reg[o];
+        const double u = U[o] - invV * m.reg[o];
+        U[o] = u;
+        if (mirror) mirror[o] = u;
         m.reg[o] = 0.0;
     }
 }
 
-__global__ void k_amr_zero_reg(AmrDev m, int level)
+__global__ void k_amr_zero_reg(AmrDev m, int level, const int *__restrict__ list, int nlist)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m.nleaf || m.lev[i] != level) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (list ? nlist : m.nleaf)) return;
+    const int i = list ? list[t] : t;
+    if (!VB_DCHECK(i >= 0 && i < m.nleaf) || m.lev[i] != level) return;
 #pragma unroll
     for (int k = 0; k < 5; ++k) m.reg[(int64_t)k * m.cap + i] = 0.0;
+}
+
+// The per-level work lists (vb_amr.h): one thread per leaf, then per face.
+__global__ void __launch_bounds__(256) k_amr_lists_leaf(AmrDev m, int *leaf, int *cell, int *cnt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nleaf) return;
+    const int li = m.lev[i];
+    if (!VB_DCHECK(li >= 0 && li < AMR_LIST_STRIDE - 1)) return;  // check build only
+    leaf[(int64_t)li * m.cap + atomicAdd(&cnt[li], 1)] = i;
+    cell[(int64_t)li * m.cap + atomicAdd(&cnt[AMR_LIST_STRIDE + li], 1)] = i;
+    bool finer = false;
+    for (int e = m.off[i]; e < m.off[i + 1] && !finer; ++e) {
+        if (!VB_DCHECK(e >= 0 && e < m.nent)) break;
+        const int code = m.ent[e];
+        const int f = code >> 1;
+        if (!VB_DCHECK(f >= 0 && f < m.nface)) break;
+        const int other = (code & 1) ? m.fL[f] : m.fR[f];
+        finer = other >= 0 && VB_DCHECK(other < m.nleaf) && m.lev[other] == li + 1;
+    }
+    if (finer)
+        cell[(int64_t)(li + 1) * m.cap + atomicAdd(&cnt[AMR_LIST_STRIDE + li + 1], 1)] = i;
+}
+
+__global__ void __launch_bounds__(256) k_amr_lists_face(AmrDev m, int *face, int *cnt)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nface) return;
+    const int L = m.fL[f], R = m.fR[f];
+    if (!VB_DCHECK(L < m.nleaf && R < m.nleaf)) return;  // check build only
+    const int a = L >= 0 ? m.lev[L] : -1, b = R >= 0 ? m.lev[R] : -1;
+    if (a >= 0) face[(int64_t)a * m.fcap + atomicAdd(&cnt[2 * AMR_LIST_STRIDE + a], 1)] = f;
+    if (b >= 0 && b != a)
+        face[(int64_t)b * m.fcap + atomicAdd(&cnt[2 * AMR_LIST_STRIDE + b], 1)] = f;
 }
 
 // conserved_totals: fixed partition (deterministic), then one folding block
@@ -334,14 +388,17 @@ static unsigned blocks(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs 
 int launch_amr_stage(const AmrDev &m, int stage, const double *Uin, const double *U0,
                      double *Uout, double *F, const AmrStageArgs &a, Ctrl *ctrl, cudaStream_t s)
 {
-    if (m.nface > 0)
-        k_amr_faces<<<blocks(m.nface, 256), 256, 0, s>>>(m, Uin, F,
-                                                         (a.dt < 0.0 && !a.dt_dev) ? ctrl : nullptr);
+    const int nf = a.faces ? a.nfaces : m.nface;
+    const int nc = a.cells ? a.ncells : m.nleaf;
+    if (nf > 0)
+        k_amr_faces<<<blocks(nf, 256), 256, 0, s>>>(m, Uin, F,
+                                                    (a.dt < 0.0 && !a.dt_dev) ? ctrl : nullptr,
+                                                    a.faces, a.nfaces);
     if (stage == 1)
-        k_amr_cells<1><<<blocks(m.nleaf, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
+        k_amr_cells<1><<<blocks(nc, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
     else
-        k_amr_cells<2><<<blocks(m.nleaf, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
-    return m.nface > 0 ? 2 : 1;
+        k_amr_cells<2><<<blocks(nc, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
+    return nf > 0 ? 2 : 1;
 }
 
 int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cudaStream_t s)
@@ -351,10 +408,19 @@ int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cuda
 }
 
 int launch_amr_cfl_bits(const AmrDev &m, const double *U, int level, unsigned long long *bits,
-                        cudaStream_t s)
+                        cudaStream_t s, const int *list, int n)
 {
-    k_amr_cfl_bits<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, level, bits);
+    k_amr_cfl_bits<<<blocks(list ? n : m.nleaf, 256), 256, 0, s>>>(m, U, level, bits, list, n);
     return 1;
+}
+
+int launch_amr_level_lists(const AmrDev &m, int *leaf, int *cell, int *face, int *cnt,
+                           cudaStream_t s)
+{
+    if (cudaMemsetAsync(cnt, 0, sizeof(int) * 3 * AMR_LIST_STRIDE, s) != cudaSuccess) return -1;
+    k_amr_lists_leaf<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, leaf, cell, cnt);
+    k_amr_lists_face<<<blocks(m.nface, 256), 256, 0, s>>>(m, face, cnt);
+    return 2;
 }
 
 int launch_amr_sub_plan(AmrSubLevel *sub, int level, double cfl, const double *target_src,
@@ -384,15 +450,16 @@ int launch_amr_tag(const AmrDev &m, const double *U, double above, int max_level
     return 1;
 }
 
-int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s)
+int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s, const int *list,
+                      int n, double *mirror)
 {
-    k_amr_reflux<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, level);
+    k_amr_reflux<<<blocks(list ? n : m.nleaf, 256), 256, 0, s>>>(m, U, level, list, n, mirror);
     return 1;
 }
 
-int launch_amr_zero_reg(const AmrDev &m, int level, cudaStream_t s)
+int launch_amr_zero_reg(const AmrDev &m, int level, cudaStream_t s, const int *list, int n)
 {
-    k_amr_zero_reg<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, level);
+    k_amr_zero_reg<<<blocks(list ? n : m.nleaf, 256), 256, 0, s>>>(m, level, list, n);
     return 1;
 }
 

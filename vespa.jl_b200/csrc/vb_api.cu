@@ -7,6 +7,8 @@
 
 #include <climits>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -18,6 +20,11 @@
 using vb::detail::fail;
 using vb::detail::use;
 
+#ifdef VB_CHECK
+namespace vb {
+__device__ unsigned int vb_check_word = 0;  // VB_DCHECK's record (vb_common.cuh)
+}
+#endif
 
 namespace {
 thread_local std::string g_err;
@@ -95,17 +102,56 @@ int encode_state_map(CUtensorMap *m, const double *base, const vb::Geom &g, uint
     return VB_OK;
 }
 
-// Autotuned z-chunk per (device, dims, boundaries, precision), process-wide.
+// Autotuned z-chunk per (GPU model, dims, boundaries, precision),
+// process-wide, and in the file named by VB_AUTOTUNE_CACHE when that is set:
+// one "key kz taper" line per tuning, appended by vb_grid_autotune and read
+// when a grid is created (the last line of a key wins).
 std::mutex g_tune_mu;
 std::map<std::string, std::pair<int, int>> g_tune_kz;  // (kz, tapered queue: 0 / 1 / -1 untuned)
 
 std::string tune_key(int device, const vb::Geom &g, int precision)
 {
-    std::string k = std::to_string(device) + ":" + std::to_string(precision);
+    cudaDeviceProp p{};
+    std::string k = cudaGetDeviceProperties(&p, device) == cudaSuccess
+                        ? std::string(p.name) + "/" + std::to_string(p.multiProcessorCount)
+                        : "device" + std::to_string(device);
+    for (char &c : k)
+        if (c == ' ') c = '_';
+    k += ":" + std::to_string(precision);
     for (int a = 0; a < 3; ++a)
         k += ":" + std::to_string(g.n[a]) + "/" + std::to_string(g.bc_lo[a]) +
              std::to_string(g.bc_hi[a]);
     return k;
+}
+
+// (call with g_tune_mu held) the cache file's entry for `key`, if any
+bool tune_file_lookup(const std::string &key, std::pair<int, int> *v)
+{
+    const char *path = std::getenv("VB_AUTOTUNE_CACHE");
+    if (!path || !*path) return false;
+    FILE *f = std::fopen(path, "r");
+    if (!f) return false;
+    char kbuf[512];
+    int kz = 0, taper = 0;
+    bool found = false;
+    while (std::fscanf(f, "%511s %d %d", kbuf, &kz, &taper) == 3)
+        if (key == kbuf && kz > 0 && taper >= -1 && taper <= 1) {
+            *v = {kz, taper};
+            found = true;
+        }
+    std::fclose(f);
+    return found;
+}
+
+// (call with g_tune_mu held) append a tuning to the cache file, if one is named
+void tune_file_append(const std::string &key, int kz, int taper)
+{
+    const char *path = std::getenv("VB_AUTOTUNE_CACHE");
+    if (!path || !*path) return;
+    FILE *f = std::fopen(path, "a");
+    if (!f) return;
+    std::fprintf(f, "%s %d %d\n", key.c_str(), kz, taper);
+    std::fclose(f);
 }
 
 }  // namespace
@@ -541,6 +587,24 @@ int vb_ctx_launch_count(vb_ctx *ctx, int64_t *count)
     return VB_OK;
 }
 
+int vb_check_read(vb_ctx *ctx, int64_t *line)
+{
+    if (!ctx || !line) return fail(VB_EINVAL, "null argument");
+#ifdef VB_CHECK
+    int rc = use(ctx);
+    if (rc) return rc;
+    VB_CUDA(cudaStreamSynchronize(ctx->stream));
+    unsigned int w = 0;
+    VB_CUDA(cudaMemcpyFromSymbol(&w, vb::vb_check_word, sizeof w));
+    const unsigned int zero = 0;
+    VB_CUDA(cudaMemcpyToSymbol(vb::vb_check_word, &zero, sizeof zero));
+    *line = (int64_t)w;
+#else
+    *line = -1;  // a build without device bounds checks
+#endif
+    return VB_OK;
+}
+
 int vb_ctx_mark(vb_ctx *ctx, int slot)
 {
     int rc = use(ctx);
@@ -578,6 +642,7 @@ int vb_hllc_faces_device_async(vb_ctx *ctx, int64_t nf, const double *dWL, const
 int vb_hllc_faces(vb_ctx *ctx, int64_t nf, const double *WL, const double *WR,
                   const int32_t *axis, double gamma, double *F)
 {
+    VB_RANGE("vb_hllc_faces");
     int rc = use(ctx);
     if (rc) return rc;
     if (nf < 0) return fail(VB_EINVAL, "nf < 0");
@@ -656,10 +721,16 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
         gr->tiled = vb::detail::tiled_auto(g);
         gr->kz = vb::detail::grid_default_kz(g);
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        auto it = g_tune_kz.find(tune_key(ctx->device, g, precision));
+        const std::string key = tune_key(ctx->device, g, precision);
+        auto it = g_tune_kz.find(key);
+        std::pair<int, int> v;
         if (it != g_tune_kz.end()) {
             gr->kz = it->second.first;
             gr->taper_tuned = it->second.second;
+        } else if (tune_file_lookup(key, &v) && v.first <= vb::march_extent(g)) {
+            gr->kz = v.first;
+            gr->taper_tuned = v.second;
+            g_tune_kz[key] = v;
         }
     }
     *out = gr;
@@ -668,6 +739,7 @@ int vb_grid_create(vb_ctx *ctx, const vb_problem_desc *d, int precision, vb_grid
 
 int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
 {
+    VB_RANGE("vb_grid_autotune");
     if (!gr || nsteps < 1) return fail(VB_EINVAL, "bad argument");
     int rc = use(gr->ctx);
     if (rc) return rc;
@@ -736,7 +808,9 @@ int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
     if (rc2) return rc2;
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
-        g_tune_kz[tune_key(gr->ctx->device, gr->g, gr->precision)] = {best, best_taper};
+        const std::string key = tune_key(gr->ctx->device, gr->g, gr->precision);
+        g_tune_kz[key] = {best, best_taper};
+        tune_file_append(key, best, best_taper);
     }
     if (best_kz) *best_kz = best;
     if (best_ms) *best_ms = best_t / nsteps;
@@ -823,6 +897,7 @@ int vb_grid_ncell(const vb_grid *gr, int64_t *n)
 
 int vb_grid_upload(vb_grid *gr, const double *U)
 {
+    VB_RANGE("vb_grid_upload");
     if (!gr || !U) return fail(VB_EINVAL, "null argument");
     int rc = use(gr->ctx);
     if (rc) return rc;
@@ -835,6 +910,7 @@ int vb_grid_upload(vb_grid *gr, const double *U)
 
 int vb_grid_download(vb_grid *gr, double *U)
 {
+    VB_RANGE("vb_grid_download");
     if (!gr || !U) return fail(VB_EINVAL, "null argument");
     int rc = use(gr->ctx);
     if (rc) return rc;
@@ -878,6 +954,7 @@ int vb_grid_get_time(vb_grid *gr, double *t, int64_t *step)
 
 int vb_compute_dt(vb_grid *gr, double *dt)
 {
+    VB_RANGE("vb_compute_dt");
     if (!gr || !dt) return fail(VB_EINVAL, "null argument");
     int rc = use(gr->ctx);
     if (rc) return rc;
@@ -935,6 +1012,7 @@ int vb_grid_set_zwindow(vb_grid *gr, int64_t zw0, int64_t zw1, int zcls0, double
 
 int vb_grid_step_phase(vb_grid *gr, int phase)
 {
+    VB_RANGE("vb_grid_step_phase");
     if (!gr) return fail(VB_EINVAL, "null grid");
     int rc = use(gr->ctx);
     if (rc) return rc;
@@ -956,6 +1034,7 @@ int vb_grid_step_phase(vb_grid *gr, int phase)
 
 int vb_grid_planes(vb_grid *gr, int which, int64_t z0, int64_t n, void *dev, int put)
 {
+    VB_RANGE("vb_grid_planes");
     if (!gr || !dev) return fail(VB_EINVAL, "null argument");
     if (which != 0 && which != 1) return fail(VB_EINVAL, "which must be 0 (state) or 1 (stage-1 state)");
     const vb::Geom &g = gr->g;
@@ -1004,6 +1083,7 @@ int vb_grid_selftest_wait(vb_grid *gr, int64_t limit_ns)
 
 int vb_step(vb_grid *gr, double dt)
 {
+    VB_RANGE("vb_step");
     if (!gr) return fail(VB_EINVAL, "null grid");
     int rc = use(gr->ctx);
     if (rc) return rc;
@@ -1020,6 +1100,7 @@ int vb_step(vb_grid *gr, double dt)
 
 int vb_run_steps_async(vb_grid *gr, int64_t nsteps)
 {
+    VB_RANGE("vb_run_steps_async");
     if (!gr) return fail(VB_EINVAL, "null grid");
     if (nsteps < 0) return fail(VB_EINVAL, "nsteps < 0");
     int rc = use(gr->ctx);
@@ -1031,6 +1112,7 @@ int vb_run_steps_async(vb_grid *gr, int64_t nsteps)
 
 int vb_evolve(vb_grid *gr, double tfinal, int64_t max_steps, double *t, int64_t *nsteps)
 {
+    VB_RANGE("vb_evolve");
     if (!gr) return fail(VB_EINVAL, "null grid");
     int rc = use(gr->ctx);
     if (rc) return rc;
@@ -1075,6 +1157,7 @@ int vb_evolve(vb_grid *gr, double tfinal, int64_t max_steps, double *t, int64_t 
 
 int vb_conserved_totals(vb_grid *gr, double out[5])
 {
+    VB_RANGE("vb_conserved_totals");
     if (!gr || !out) return fail(VB_EINVAL, "null argument");
     int rc = use(gr->ctx);
     if (rc) return rc;
@@ -1168,6 +1251,7 @@ int vb_bflux_plane(vb_grid *gr, int dim, int source, const int64_t *start, const
                    const int64_t *g0, int64_t flux_off, int comp, double vcell, double *out,
                    int64_t n)
 {
+    VB_RANGE("vb_bflux_plane");
     if (!gr || !start || !stop || !g0 || (!out && n > 0)) return fail(VB_EINVAL, "null argument");
     if (!gr->bflux) return fail(VB_EINVAL, "boundary-flux register not enabled");
     const int R = gr->g.nd;

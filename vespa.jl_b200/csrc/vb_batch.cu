@@ -271,6 +271,7 @@ int vb_batch_download(vb_batch *b, int box, double *U)
 
 int vb_batch_run_steps_async(vb_batch *b, int64_t nsteps)
 {
+    VB_RANGE("vb_batch_run_steps_async");
     if (!b) return fail(VB_EINVAL, "null batch");
     if (nsteps < 0) return fail(VB_EINVAL, "nsteps < 0");
     if (nsteps == 0) return VB_OK;
@@ -283,6 +284,7 @@ int vb_batch_run_steps_async(vb_batch *b, int64_t nsteps)
 
 int vb_batch_run_steps(vb_batch *b, int64_t nsteps)
 {
+    VB_RANGE("vb_batch_run_steps");
     int rc = vb_batch_run_steps_async(b, nsteps);
     if (rc) return rc;
     rc = pull(b);

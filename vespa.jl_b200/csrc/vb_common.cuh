@@ -8,6 +8,25 @@
 
 namespace vb {
 
+// Device bounds checks of the check build (`make -C vespa.jl_b200/csrc check`:
+// -DVB_CHECK with relocatable device code, libvespa_b200_check.so).
+// VB_DCHECK(cond) is true when cond holds; otherwise it records the source
+// line of the check in vb_check_word (the first failure wins; vb_check_read
+// returns and clears it) and the caller skips the access it guards, so a bad
+// index becomes a status instead of a fault.  In the normal build it is the
+// constant true and generates no code.
+#ifdef VB_CHECK
+extern __device__ unsigned int vb_check_word;
+__device__ __noinline__ inline bool vb_dcheck_fail(unsigned line)
+{
+    atomicCAS(&vb_check_word, 0u, line);
+    return false;
+}
+#define VB_DCHECK(cond) ((cond) ? true : ::vb::vb_dcheck_fail(__LINE__))
+#else
+#define VB_DCHECK(cond) true
+#endif
+
 enum { BC_OUTFLOW = 0, BC_PERIODIC = 1, BC_REFLECTING = 2 };
 enum { PREC_FP64 = 0, PREC_MIXED = 1 };
 

@@ -1140,6 +1140,7 @@ int vb_gravity_disable(vb_grid *gr)
 
 int vb_gravity_solve(vb_grid *gr, int64_t *iters, double *relres)
 {
+    VB_RANGE("vb_gravity_solve");
     int rc = check_grid(gr);
     if (rc) return rc;
     return vb::detail::gravity_solve(gr, iters, relres);
@@ -1182,6 +1183,7 @@ int vb_gravity_accel(vb_grid *gr, double *gout)
 
 int vb_gravity_laplacian(vb_grid *gr, const double *x, double *Ax)
 {
+    VB_RANGE("vb_gravity_laplacian");
     int rc = check_grid(gr);
     if (rc) return rc;
     if (!x || !Ax) return fail(VB_EINVAL, "null argument");

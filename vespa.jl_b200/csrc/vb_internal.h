@@ -4,6 +4,8 @@
 
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/vespa_b200.h"
 #include "vb_launch.h"
 
@@ -88,8 +90,20 @@ int grid_push_ctrl(vb_grid *gr);    // gr->hctrl -> device control block (synchr
 int gravity_solve(vb_grid *gr, int64_t *iters, double *relres);
 void gravity_free(vb_gravity *gv);
 
+// NVTX range over a host API call, named after it: Nsight Systems shows the
+// calls (and the launches they enqueue) on the host timeline; without an
+// attached tool a push/pop costs a few nanoseconds.
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
+
 }  // namespace detail
 }  // namespace vb
+
+#define VB_RANGE(name) vb::detail::Range vb_range_(name)
 
 #define VB_CUDA(call)                                                                      \
     do {                                                                                   \

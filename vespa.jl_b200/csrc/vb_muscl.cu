@@ -499,6 +499,7 @@ int vb_muscl_state(vb_muscl *mu, double **dU)
 
 int vb_muscl_step(vb_muscl *mu, const vb_muscl_params *p)
 {
+    VB_RANGE("vb_muscl_step");
     if (!mu) return fail(VB_EINVAL, "null handle");
     int rc = check_params(p, mu);
     if (!rc) rc = use(mu->ctx);
@@ -510,6 +511,7 @@ int vb_muscl_step(vb_muscl *mu, const vb_muscl_params *p)
 
 int vb_muscl_run_async(vb_muscl *mu, const vb_muscl_params *p, int64_t nsteps)
 {
+    VB_RANGE("vb_muscl_run_async");
     if (!mu) return fail(VB_EINVAL, "null handle");
     if (nsteps < 0) return fail(VB_EINVAL, "nsteps < 0");
     int rc = check_params(p, mu);
@@ -521,6 +523,7 @@ int vb_muscl_run_async(vb_muscl *mu, const vb_muscl_params *p, int64_t nsteps)
 int vb_muscl_step_fields(vb_muscl *mu, double *D, double *S1, double *S2, double *S3, double *Tau,
                          const vb_muscl_params *p)
 {
+    VB_RANGE("vb_muscl_step_fields");
     if (!mu || !D || !S1 || !S2 || !S3 || !Tau) return fail(VB_EINVAL, "null argument");
     int rc = check_params(p, mu);
     if (!rc) rc = use(mu->ctx);

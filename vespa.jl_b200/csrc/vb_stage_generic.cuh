@@ -45,9 +45,10 @@ template <typename T>
 __device__ __forceinline__ void load_prim(const Geom &g, const double *__restrict__ U, int64_t lin,
                                           T W[5])
 {
-    double u[5], w[5];
+    double u[5] = {1.0, 0.0, 0.0, 0.0, 1.0}, w[5];
+    if (VB_DCHECK(lin >= 0 && lin < g.ncell))
 #pragma unroll
-    for (int k = 0; k < 5; ++k) u[k] = __ldg(U + k * g.ncell + lin);
+        for (int k = 0; k < 5; ++k) u[k] = __ldg(U + k * g.ncell + lin);
     cons2prim(u, g.gamma, w);
 #pragma unroll
     for (int k = 0; k < 5; ++k) W[k] = T(w[k]);

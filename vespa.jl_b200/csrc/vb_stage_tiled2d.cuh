@@ -252,11 +252,13 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
         const int q = r - r0 + 4;
         const int slot = (q - 2) % 3;  // ring slot of row r's halo
         const int64_t lin = (int64_t)gxc + (int64_t)nx * r;
+        const bool inb = VB_DCHECK(lin >= 0 && lin < g.ncell);  // check build only
+        if (inb)
 #pragma unroll
-        for (int f = 0; f < 5; ++f) {
-            cp_async8(&S.ep[0][f][t], Uin + (int64_t)f * g.ncell + lin);
-            if constexpr (STAGE == 2) cp_async8(&S.ep[1][f][t], U0 + (int64_t)f * g.ncell + lin);
-        }
+            for (int f = 0; f < 5; ++f) {
+                cp_async8(&S.ep[0][f][t], Uin + (int64_t)f * g.ncell + lin);
+                if constexpr (STAGE == 2) cp_async8(&S.ep[1][f][t], U0 + (int64_t)f * g.ncell + lin);
+            }
         cp_async_commit();
         consume(q, Wy2, true);
         if constexpr (STAGE == 2) {
@@ -423,7 +425,7 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
                 else
                     un[f] = 0.5 * S.ep[1][f][t] + 0.5 * (S.ep[0][f][t] - invV * a);
             }
-            Uout[(int64_t)f * g.ncell + lin] = un[f];
+            if (inb) Uout[(int64_t)f * g.ncell + lin] = un[f];
         }
         if constexpr (STAGE == 2) {
 #pragma unroll

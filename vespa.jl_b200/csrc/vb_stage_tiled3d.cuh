@@ -117,6 +117,7 @@ static __device__ __forceinline__ void bflux_add(const Geom &g, double *bf, int 
     const int64_t P = d == 0 ? P0 : (d == 1 ? P1 : P2);
     int64_t off = d == 0 ? 0 : (d == 1 ? 10 * P0 : 10 * (P0 + P1));
     off += (int64_t)side * 5 * P + idx;
+    if (!VB_DCHECK(idx >= 0 && idx < P)) return;  // check build only
 #pragma unroll
     for (int k = 0; k < 5; ++k) atomicAdd(bf + off + k * P, scale * F[k] * area);
 }

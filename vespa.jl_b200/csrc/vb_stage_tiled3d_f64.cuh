@@ -390,6 +390,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
         const int cz = (k == g.zw0 && g.zcls0 >= 0) ? g.zcls0 : lo_class(k, nz, perz);
         const bool interior = cx == LO_BEFORE && cy == LO_BEFORE && cz == LO_BEFORE;
         double un[5];
+        const bool inb = VB_DCHECK(lin >= 0 && lin < g.ncell);  // check build only
         const double *pin = Uin + lin, *p0 = U0 + lin;
         double *po = Uout + lin;
         double acc[5];  // GRAV: the flux sums, completed by the gravity source
@@ -422,12 +423,13 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
                 acc[f] = a;
                 continue;
             }
+            const double uin = inb ? __ldg(pin) : 0.0;
             if constexpr (STAGE == 1) {
-                un[f] = __ldg(pin) - invV * a;
+                un[f] = uin - invV * a;
             } else {
-                un[f] = 0.5 * *p0 + 0.5 * (__ldg(pin) - invV * a);
+                un[f] = 0.5 * (inb ? *p0 : 0.0) + 0.5 * (uin - invV * a);
             }
-            *po = un[f];
+            if (inb) *po = un[f];
             pin += g.ncell;
             p0 += g.ncell;
             po += g.ncell;
@@ -435,13 +437,13 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
         if constexpr (GRAV) {  // the source from the stage state, after the fluxes
             double u[5];
 #pragma unroll
-            for (int f = 0; f < 5; ++f) u[f] = __ldg(pin + f * g.ncell);
-            gravity_source<3>(g, lin, u, acc);
+            for (int f = 0; f < 5; ++f) u[f] = inb ? __ldg(pin + f * g.ncell) : 0.0;
+            if (inb) gravity_source<3>(g, lin, u, acc);
 #pragma unroll
             for (int f = 0; f < 5; ++f) {
                 if constexpr (STAGE == 1) un[f] = u[f] - invV * acc[f];
-                else un[f] = 0.5 * p0[f * g.ncell] + 0.5 * (u[f] - invV * acc[f]);
-                po[f * g.ncell] = un[f];
+                else un[f] = 0.5 * (inb ? p0[f * g.ncell] : 0.0) + 0.5 * (u[f] - invV * acc[f]);
+                if (inb) po[f * g.ncell] = un[f];
             }
         }
         lin += plane_cells;

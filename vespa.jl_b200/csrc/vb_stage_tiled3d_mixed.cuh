@@ -481,7 +481,8 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     for (int k = k0; k < k1; ++k) {
         const int q = k - k0 + 4;
         const float *w0 = r0, *w1 = r1, *w2 = r2;
-        {
+        const bool inb = VB_DCHECK(lin >= 0 && lin < g.ncell);  // check build only
+        if (inb) {
             const double *pa = Uin + lin, *pb = U0 + lin;
 #pragma unroll
             for (int f = 0; f < 5; ++f) {
@@ -570,19 +571,19 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
                 un[f] = __fma_rn(0.5, S.ep[1][f][t],
                                  __dmul_rn(0.5, __fma_rn(-invV, a, S.ep[0][f][t])));
             }
-            *po = un[f];
+            if (inb) *po = un[f];
             po += g.ncell;
         }
         if constexpr (GRAV) {  // the source from the stage state, after the fluxes
             double u[5];
 #pragma unroll
             for (int f = 0; f < 5; ++f) u[f] = S.ep[0][f][t];
-            gravity_source<3>(g, lin, u, acc);
+            if (inb) gravity_source<3>(g, lin, u, acc);
 #pragma unroll
             for (int f = 0; f < 5; ++f) {
                 if constexpr (STAGE == 1) un[f] = __fma_rn(-invV, acc[f], u[f]);
                 else un[f] = __fma_rn(0.5, S.ep[1][f][t], __dmul_rn(0.5, __fma_rn(-invV, acc[f], u[f])));
-                po[f * g.ncell] = un[f];
+                if (inb) po[f * g.ncell] = un[f];
             }
         }
         lin += plane_cells;

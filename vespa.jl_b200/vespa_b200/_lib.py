@@ -87,6 +87,7 @@ SIGNATURES = {
     "vb_ctx_synchronize": [_VP],
     "vb_ctx_stream": [_VP, C.POINTER(_VP)],
     "vb_ctx_launch_count": [_VP, _I64P],
+    "vb_check_read": [_VP, _I64P],
     "vb_ctx_mark": [_VP, C.c_int],
     "vb_ctx_elapsed_ms": [_VP, C.c_int, C.c_int, C.POINTER(C.c_float)],
     "vb_hllc_faces": [_VP, C.c_int64, _DP, _DP, _I32P, C.c_double, _DP],
@@ -270,6 +271,14 @@ class Context:
     def launch_count(self) -> int:
         n = C.c_int64()
         call("vb_ctx_launch_count", self.handle, C.byref(n))
+        return n.value
+
+    def check_read(self) -> int:
+        """Device bounds-check record (vb_check_read): 0 = no check failed
+        since the last read, else the source line of the first failed check;
+        -1 in the normal build (no checks).  Waits for the stream; clears."""
+        n = C.c_int64()
+        call("vb_check_read", self.handle, C.byref(n))
         return n.value
 
 

@@ -28,7 +28,8 @@ from .simulation import Simulation
 class Adjoint:
     """Checkpointed adjoint of up to ``max_steps`` steps of ``sim``
     (vb_adjoint_create); a state copy is kept every ``checkpoint_every``
-    steps."""
+    steps.  ``checkpoint_every=1`` keeps a tape of both states of every step
+    in device memory instead, and the reverse sweep recomputes nothing."""
 
     def __init__(self, sim: Simulation, max_steps: int, checkpoint_every: int = 20):
         self.sim = sim
