@@ -933,8 +933,9 @@ int vb_amr_evolve(vb_amr *a, double tfinal, int64_t max_steps, double refine_abo
             a->hctrl->step_limit = a->step + chunk;
             a->hctrl->active = 1;
             a->hctrl->flags = 0;
-            rc = push_ctrl(a);
-            if (rc) return rc;
+            // queued, not awaited: the host writes hctrl again only after the
+            // pull below has synchronised the stream
+            VB_CUDA(cudaMemcpyAsync(a->ctrl, a->hctrl, sizeof(vb::Ctrl), cudaMemcpyHostToDevice, st));
             VB_CUDA(cudaMemsetAsync(&a->ctrl->invdt_bits, 0, sizeof(unsigned long long), st));
             VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_cfl(a->dev, a->U, -1, a->ctrl, st));
             vb::AmrStageArgs s{};
