@@ -24,17 +24,23 @@ namespace vb {
 
 namespace {
 
+// the cell `off` cells away along ax (periodic); the modulo only at the wrap
 __device__ __forceinline__ int64_t wrap_lin(const Geom &g, int ax, int64_t lin, int64_t c, int off)
 {
     const int64_t n = g.n[ax];
-    int64_t j = (c + off) % n;
-    if (j < 0) j += n;
+    int64_t j = c + off;
+    if (j < 0 || j >= n) {
+        j %= n;
+        if (j < 0) j += n;
+    }
     return lin + (j - c) * g.stride[ax];
 }
 
 __device__ __forceinline__ int64_t coord(const Geom &g, int ax, int64_t lin)
 {
-    return (lin / g.stride[ax]) % g.n[ax];
+    int64_t cc[3];
+    cell_coords(g, lin, cc);
+    return cc[ax];
 }
 
 template <int AX>

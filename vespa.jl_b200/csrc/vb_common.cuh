@@ -60,6 +60,24 @@ struct Geom {
     int64_t act0, act1;
 };
 
+// Coordinates of cell `lin` (x fastest, strides 1, n0, n0*n1): 32-bit
+// unsigned divisions while the grid has fewer than 2^31 cells, 64-bit ones
+// beyond (a 64-bit division is a long instruction sequence).
+__device__ __forceinline__ void cell_coords(const Geom &g, int64_t lin, int64_t cc[3])
+{
+    if (g.ncell <= 0x7fffffffLL) {
+        const unsigned l = (unsigned)lin, n0 = (unsigned)g.n[0], n1 = (unsigned)g.n[1];
+        const unsigned q = l / n0, r = q / n1;
+        cc[0] = (int64_t)(l - q * n0);
+        cc[1] = (int64_t)(q - r * n1);
+        cc[2] = (int64_t)r;
+    } else {
+        cc[0] = lin % g.n[0];
+        cc[1] = (lin / g.n[0]) % g.n[1];
+        cc[2] = lin / (g.n[0] * g.n[1]);
+    }
+}
+
 // 4 pi, as FOURPI in src/gravity.jl:21
 constexpr double VB_FOURPI = 4.0 * 3.14159265358979323846;
 

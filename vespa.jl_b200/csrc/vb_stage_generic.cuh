@@ -150,9 +150,7 @@ k_stage_generic(Geom g, const double *__restrict__ Uin, const double *U0, double
     double invdt = 0.0;
     if (lin < g.ncell) {
         int64_t cc[3];
-        cc[0] = lin % g.n[0];
-        cc[1] = (lin / g.n[0]) % g.n[1];
-        cc[2] = lin / (g.n[0] * g.n[1]);
+        cell_coords(g, lin, cc);
         T Wc[5];
         load_prim<T>(g, Uin, lin, Wc);
         AxisFlux<T> af[ND];
