@@ -840,6 +840,7 @@ def batch64_section(ctx, ranks: Ranks, K: int, W: int):
     probs = [P.riemann_box_problem(i, seed=P.DEFAULT_SEED + 1000 * ranks.rank) for i in range(64)]
     batch = vb.Batch(probs, precision="mixed", ctx=ctx)
     cells = batch.ncell()
+    cap, _ = batch.autotune(3)  # work-item depth; states and clocks restored
     batch.run_steps(W)
     batch.run_steps_async(K)  # capture the K-step graph once, outside the timing
     ctx.synchronize()
@@ -856,12 +857,15 @@ def batch64_section(ctx, ranks: Ranks, K: int, W: int):
     return {"value": round(total * K / (ms / 1e3) / 1e6, 1), "unit": UNIT,
             "ms_per_step": round(ms / K, 4), "steps": K, "warmup": W,
             "cells_per_gpu": cells, "boxes": 64,
+            "items": "16x16 column tiles, " + ("each box's default z chunk" if cap == 0 else
+                                                f"z chunks capped at {cap} planes") + " (autotuned)",
             "sides": sorted({p.dims[0] for p in probs}),
             "step_hbm_frac": round(200 * cells / (ms / K / 1e3) / 1e9 / hbm, 4),
             "hbm_peak_gbs": hbm, "hbm_peak_source": hbm_kind, "gpu_launches": launches,
             "precision": "mixed", "data": BATCH_DATA,
             "what": "per-box CFL dt; finalise, stage 1, stage 2 and advance per step for all "
-                    "boxes; the K timed steps replay one CUDA graph"}
+                    "boxes; the K timed steps replay one CUDA graph; work-item depth picked by "
+                    "vb_batch_autotune"}
 
 
 def run_batch64(args, ranks: Ranks):

@@ -231,6 +231,13 @@ int vb_batch_download(vb_batch *batch, int box, double *U);
 int vb_batch_run_steps(vb_batch *batch, int64_t nsteps);
 /* The same, queued on the context's stream without waiting. */
 int vb_batch_run_steps_async(vb_batch *batch, int64_t nsteps);
+/* Pick the depth of the batch's work items (16 x 16 x kz column tiles): the
+ * default chunks (*best_cap = 0) or a cap of 16..128 planes on every box's
+ * chunk, each timed over nsteps steps of the whole batch (CUDA-graph
+ * replays, after a warm-up step).  States and clocks are restored; needs
+ * device memory for a copy of every box's state.  Results do not depend on
+ * the layout (same bits). */
+int vb_batch_autotune(vb_batch *batch, int nsteps, int64_t *best_cap, double *best_ms);
 int vb_batch_get_time(vb_batch *batch, int box, double *t, int64_t *step);
 int vb_batch_conserved_totals(vb_batch *batch, int box, double out[5]);
 

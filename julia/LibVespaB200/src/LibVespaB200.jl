@@ -211,6 +211,8 @@ vb_batch_run_steps(batch, nsteps) =
     ccall((:vb_batch_run_steps, libvespa_b200), Cint, (Ptr{Cvoid}, Int64), batch, nsteps)
 vb_batch_run_steps_async(batch, nsteps) =
     ccall((:vb_batch_run_steps_async, libvespa_b200), Cint, (Ptr{Cvoid}, Int64), batch, nsteps)
+vb_batch_autotune(batch, nsteps, best_cap, best_ms) =
+    ccall((:vb_batch_autotune, libvespa_b200), Cint, (Ptr{Cvoid}, Cint, Ptr{Int64}, Ptr{Float64}), batch, nsteps, best_cap, best_ms)
 vb_batch_get_time(batch, box, t, step) =
     ccall((:vb_batch_get_time, libvespa_b200), Cint, (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Int64}), batch, box, t, step)
 vb_batch_conserved_totals(batch, box, out) =

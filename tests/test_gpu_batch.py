@@ -106,3 +106,28 @@ def test_seeded_64_box_batch_equals_single_runs_and_oracle(vb, oracle):
         checked += 1
     batch.close()
     assert checked >= 10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_autotune_restores_state_and_keeps_bits(vb, precision):
+    """vb_batch_autotune times every work-item depth on the batch itself,
+    then restores states and clocks; the chosen layout steps to the same
+    bits as the default one."""
+    probs = box_problems()
+    a = vb.Batch(probs, precision=precision)
+    b = vb.Batch(probs, precision=precision)
+    a.run_steps(1)
+    b.run_steps(1)
+    s0 = [a.state(i) for i in range(len(probs))]
+    cap, ms = a.autotune(2)
+    assert cap in (0, 16, 24, 32, 48, 64, 96, 128) and ms > 0
+    for i in range(len(probs)):
+        assert a.time(i) == b.time(i)
+        assert np.array_equal(a.state(i), s0[i])
+    a.run_steps(3)
+    b.run_steps(3)
+    for i in range(len(probs)):
+        assert a.time(i) == b.time(i)
+        assert np.array_equal(a.state(i), b.state(i)), (i, cap)
+    a.close()
+    b.close()

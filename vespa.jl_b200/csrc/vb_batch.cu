@@ -6,7 +6,9 @@
 // persistent tiled kernels pulling (box, column tile, z chunk) items from one
 // queue, and the per-box clock advance.  Items are numbered largest box first
 // so the tail of each stage is made of small items.  A run of nsteps steps is
-// captured once as a CUDA graph and replayed.
+// captured once as a CUDA graph and replayed.  vb_batch_autotune picks the
+// work items' depth: a cap on the z chunk of every box, timed over the whole
+// batch.
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -32,6 +34,9 @@ struct vb_batch {
     vb::BoxDesc *boxes = nullptr;
     int *item_box = nullptr;
     int nitems = 0;
+    int kz_cap = 0;                          // chunk cap of the item layout (0: default chunks)
+    std::vector<vb::TiledMaps> mU, mU1;      // per-box TMA descriptors
+    std::vector<int> order;                  // boxes, largest first
     unsigned int *work = nullptr;  // the two stage cursors
     double *partials = nullptr, *totals = nullptr, *htot = nullptr;
     bool invdt_valid = false;
@@ -80,6 +85,41 @@ int queue(vb_batch *b, int64_t nsteps)
                                                                         b->work, st, s));
         VB_CHECK_LAUNCH(b->ctx, vb::launch_advance_boxes(b->boxes, b->nbox, s));
     }
+    return VB_OK;
+}
+
+// Work items for chunk cap `cap` (0: each box's default chunk): box
+// descriptors and the item -> box table, uploaded on the stream.  Captured
+// graphs hold the old item count, so they are dropped.
+int set_layout(vb_batch *b, int cap)
+{
+    std::vector<vb::BoxDesc> hb(b->nbox);
+    std::vector<int> item_box;
+    for (int i : b->order) {
+        const vb::Geom &g = b->geom[i];
+        const int nz = (int)g.n[2];
+        const int kz = cap > 0 ? (cap < nz ? cap : nz) : vb::detail::default_kz(g);
+        const int64_t n = vb::detail::box_items(g, kz);
+        if ((int64_t)item_box.size() + n > INT_MAX) return fail(VB_ENOTSUP, "too many work items");
+        hb[i] = vb::detail::make_box(b->mU[i], b->mU1[i], g, b->U[i], b->U1[i], b->ctrl + i, kz,
+                                     (int)item_box.size());
+        item_box.insert(item_box.end(), (size_t)n, i);
+    }
+    VB_CUDA(cudaStreamSynchronize(b->ctx->stream));  // no step still reads the old tables
+    for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+    if ((int)item_box.size() > b->nitems || !b->item_box) {
+        cudaFree(b->item_box);
+        b->item_box = nullptr;
+        VB_CUDA(cudaMalloc(&b->item_box, sizeof(int) * item_box.size()));
+    }
+    b->nitems = (int)item_box.size();
+    VB_CUDA(cudaMemcpyAsync(b->boxes, hb.data(), sizeof(vb::BoxDesc) * b->nbox,
+                            cudaMemcpyHostToDevice, b->ctx->stream));
+    VB_CUDA(cudaMemcpyAsync(b->item_box, item_box.data(), sizeof(int) * item_box.size(),
+                            cudaMemcpyHostToDevice, b->ctx->stream));
+    VB_CUDA(cudaStreamSynchronize(b->ctx->stream));
+    b->kz_cap = cap;
     return VB_OK;
 }
 
@@ -177,33 +217,23 @@ int vb_batch_create(vb_ctx *ctx, int nbox, const vb_problem_desc *descs, int pre
     if (rc) return bail(rc, "batch control upload failed");
 
     // work items: largest boxes first, chunk-major within a box
-    std::vector<int> order(nbox);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(),
+    b->order.resize(nbox);
+    std::iota(b->order.begin(), b->order.end(), 0);
+    std::stable_sort(b->order.begin(), b->order.end(),
                      [&](int a, int c) { return geom[a].ncell > geom[c].ncell; });
-    std::vector<vb::BoxDesc> hb(nbox);
-    std::vector<int> item_box;
-    for (int i : order) {
-        vb::TiledMaps mU, mU1;
-        rc = vb::detail::encode_maps(&mU, b->U[i], geom[i]);
-        if (!rc) rc = vb::detail::encode_maps(&mU1, b->U1[i], geom[i]);
+    b->mU.resize(nbox);
+    b->mU1.resize(nbox);
+    for (int i = 0; i < nbox; ++i) {
+        rc = vb::detail::encode_maps(&b->mU[i], b->U[i], geom[i]);
+        if (!rc) rc = vb::detail::encode_maps(&b->mU1[i], b->U1[i], geom[i]);
         if (rc) return bail(rc, "batch tensor maps failed");
-        const int kz = vb::detail::default_kz(geom[i]);
-        const int64_t n = vb::detail::box_items(geom[i], kz);
-        if ((int64_t)item_box.size() + n > INT_MAX) return bail(VB_ENOTSUP, "too many work items");
-        hb[i] = vb::detail::make_box(mU, mU1, geom[i], b->U[i], b->U1[i], b->ctrl + i, kz,
-                                     (int)item_box.size());
-        item_box.insert(item_box.end(), (size_t)n, i);
     }
-    b->nitems = (int)item_box.size();
-    if ((e = cudaMalloc(&b->item_box, sizeof(int) * item_box.size())) != cudaSuccess)
-        return bail(VB_ENOMEM, std::string("item table: ") + cudaGetErrorString(e));
-    if ((e = cudaMemcpyAsync(b->boxes, hb.data(), sizeof(vb::BoxDesc) * nbox,
-                             cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(b->item_box, item_box.data(), sizeof(int) * item_box.size(),
-                             cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
-        return bail(VB_ECUDA, std::string("batch table upload: ") + cudaGetErrorString(e));
+    rc = set_layout(b, 0);
+    if (rc) {
+        char msg[256];
+        vb_last_error(msg, sizeof msg);
+        return bail(rc, std::string("batch work items: ") + msg);
+    }
     *out = b;
     return VB_OK;
 }
@@ -295,6 +325,80 @@ int vb_batch_run_steps(vb_batch *b, int64_t nsteps)
         if (b->hctrl[i].flags & vb::CTRL_F_TIMEOUT)
             return fail(VB_ETIMEOUT, "box " + std::to_string(i) + ": a bounded device wait gave up");
     }
+    return VB_OK;
+}
+
+int vb_batch_autotune(vb_batch *b, int nsteps, int64_t *best_cap, double *best_ms)
+{
+    VB_RANGE("vb_batch_autotune");
+    if (!b || nsteps < 1) return fail(VB_EINVAL, "bad argument");
+    int rc = use(b->ctx);
+    if (rc) return rc;
+    cudaStream_t s = b->ctx->stream;
+    // scratch copies of every box's state and of the control blocks: the
+    // candidates' steps are undone afterwards
+    std::vector<double *> save(b->nbox, nullptr);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&]() {
+        for (double *p : save) cudaFree(p);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    };
+    for (int i = 0; i < b->nbox && !rc; ++i) {
+        const size_t bytes = sizeof(double) * 5 * (size_t)b->geom[i].ncell;
+        if (cudaMalloc(&save[i], bytes) != cudaSuccess ||
+            cudaMemcpyAsync(save[i], b->U[i], bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            rc = fail(VB_ENOMEM, "autotune: no room for a copy of the batch state");
+    }
+    if (!rc) rc = pull(b);
+    if (rc) {
+        cleanup();
+        return rc;
+    }
+    const std::vector<vb::Ctrl> ctrl0(b->hctrl, b->hctrl + b->nbox);
+    const bool valid0 = b->invdt_valid;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cleanup();
+        return fail(VB_ECUDA, "autotune events");
+    }
+    // candidates: the default chunks (0) and caps on every box's chunk
+    const int cand[] = {0, 16, 24, 32, 48, 64, 96, 128};
+    int best = b->kz_cap;
+    float best_t = INFINITY;
+    for (int c : cand) {
+        rc = set_layout(b, c);
+        if (!rc) rc = cfl_all(b);
+        if (!rc) rc = queue(b, 1);               // warm-up
+        if (!rc) rc = run_graph(b, nsteps);      // capture outside the timed region
+        if (rc) break;
+        cudaEventRecord(e0, s);
+        rc = run_graph(b, nsteps);
+        cudaEventRecord(e1, s);
+        if (rc) break;
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            rc = fail(VB_ECUDA, "autotune timing failed");
+            break;
+        }
+        if (ms < best_t) {
+            best_t = ms;
+            best = c;
+        }
+    }
+    // restore states, clocks and the best layout, whatever happened
+    for (int i = 0; i < b->nbox; ++i)
+        cudaMemcpyAsync(b->U[i], save[i], sizeof(double) * 5 * (size_t)b->geom[i].ncell,
+                        cudaMemcpyDeviceToDevice, s);
+    std::copy(ctrl0.begin(), ctrl0.end(), b->hctrl);
+    int rc2 = push(b);
+    b->invdt_valid = valid0;  // the restored control blocks hold the saved states' CFL maxima
+    int rc3 = set_layout(b, best);
+    cleanup();
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (rc3) return rc3;
+    if (best_cap) *best_cap = best;
+    if (best_ms) *best_ms = best_t / nsteps;
     return VB_OK;
 }
 

@@ -122,6 +122,7 @@ SIGNATURES = {
     "vb_batch_download": [_VP, C.c_int, _DP],
     "vb_batch_run_steps": [_VP, C.c_int64],
     "vb_batch_run_steps_async": [_VP, C.c_int64],
+    "vb_batch_autotune": [_VP, C.c_int, _I64P, _DP],
     "vb_batch_get_time": [_VP, C.c_int, _DP, _I64P],
     "vb_batch_conserved_totals": [_VP, C.c_int, _DP],
     "vb_bflux_enable": [_VP, C.c_int],

@@ -130,6 +130,14 @@ class Batch:
     def run_steps_async(self, nsteps: int) -> None:
         _lib.call("vb_batch_run_steps_async", self.handle, int(nsteps))
 
+    def autotune(self, nsteps: int = 3) -> tuple:
+        """Pick the work items' depth (vb_batch_autotune): returns (cap, ms per
+        step); cap 0 = each box's default chunk, else the cap on every box's
+        z chunk.  States and clocks are restored."""
+        cap, ms = C.c_int64(), C.c_double()
+        _lib.call("vb_batch_autotune", self.handle, int(nsteps), C.byref(cap), C.byref(ms))
+        return cap.value, ms.value
+
     def time(self, box: int) -> tuple:
         t, n = C.c_double(), C.c_int64()
         _lib.call("vb_batch_get_time", self.handle, int(box), C.byref(t), C.byref(n))
