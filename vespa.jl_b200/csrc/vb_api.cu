@@ -109,14 +109,25 @@ int encode_state_map(CUtensorMap *m, const double *base, const vb::Geom &g, uint
 std::mutex g_tune_mu;
 std::map<std::string, std::pair<int, int>> g_tune_kz;  // (kz, tapered queue: 0 / 1 / -1 untuned)
 
-std::string tune_key(int device, const vb::Geom &g, int precision)
+// (call with g_tune_mu held) "model/SMs" of a device, looked up once
+const std::string &device_model(int device)
 {
+    static std::map<int, std::string> names;
+    auto it = names.find(device);
+    if (it != names.end()) return it->second;
     cudaDeviceProp p{};
     std::string k = cudaGetDeviceProperties(&p, device) == cudaSuccess
                         ? std::string(p.name) + "/" + std::to_string(p.multiProcessorCount)
                         : "device" + std::to_string(device);
     for (char &c : k)
         if (c == ' ') c = '_';
+    return names[device] = k;
+}
+
+// (call with g_tune_mu held)
+std::string tune_key(int device, const vb::Geom &g, int precision)
+{
+    std::string k = device_model(device);
     k += ":" + std::to_string(precision);
     for (int a = 0; a < 3; ++a)
         k += ":" + std::to_string(g.n[a]) + "/" + std::to_string(g.bc_lo[a]) +
