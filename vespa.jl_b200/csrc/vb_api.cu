@@ -14,6 +14,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "vb_internal.h"
 
@@ -22,8 +23,25 @@ using vb::detail::use;
 
 #ifdef VB_CHECK
 namespace vb {
-__device__ unsigned int vb_check_word = 0;  // VB_DCHECK's record (vb_common.cuh)
+namespace {
+std::vector<unsigned (*)()> &check_readers()
+{
+    static std::vector<unsigned (*)()> v;
+    return v;
 }
+std::mutex &check_mu()
+{
+    static std::mutex m;
+    return m;
+}
+}  // namespace
+// each translation unit's reader of its VB_DCHECK record (vb_common.cuh)
+void check_register(unsigned (*read_and_clear)())
+{
+    std::lock_guard<std::mutex> lk(check_mu());
+    check_readers().push_back(read_and_clear);
+}
+}  // namespace vb
 #endif
 
 namespace {
@@ -606,9 +624,11 @@ int vb_check_read(vb_ctx *ctx, int64_t *line)
     if (rc) return rc;
     VB_CUDA(cudaStreamSynchronize(ctx->stream));
     unsigned int w = 0;
-    VB_CUDA(cudaMemcpyFromSymbol(&w, vb::vb_check_word, sizeof w));
-    const unsigned int zero = 0;
-    VB_CUDA(cudaMemcpyToSymbol(vb::vb_check_word, &zero, sizeof zero));
+    std::lock_guard<std::mutex> lk(vb::check_mu());
+    for (auto fn : vb::check_readers()) {
+        const unsigned x = fn();
+        if (!w) w = x;
+    }
     *line = (int64_t)w;
 #else
     *line = -1;  // a build without device bounds checks

@@ -9,20 +9,35 @@
 namespace vb {
 
 // Device bounds checks of the check build (`make -C vespa.jl_b200/csrc check`:
-// -DVB_CHECK with relocatable device code, libvespa_b200_check.so).
-// VB_DCHECK(cond) is true when cond holds; otherwise it records the source
-// line of the check in vb_check_word (the first failure wins; vb_check_read
-// returns and clears it) and the caller skips the access it guards, so a bad
-// index becomes a status instead of a fault.  In the normal build it is the
-// constant true and generates no code.
+// -DVB_CHECK, libvespa_b200_check.so).  VB_DCHECK(cond) is true when cond
+// holds; otherwise it records the source line of the check in its
+// translation unit's word (the first failure wins) and the caller skips the
+// access it guards, so a bad index becomes a status instead of a fault.
+// vb_check_read collects and clears the words through readers that each
+// translation unit registers at load time.  In the normal build VB_DCHECK is
+// the constant true and generates no code.
 #ifdef VB_CHECK
-extern __device__ unsigned int vb_check_word;
-__device__ __noinline__ inline bool vb_dcheck_fail(unsigned line)
+void check_register(unsigned (*read_and_clear)());  // vb_api.cu
+namespace {
+__device__ unsigned int vb_check_word = 0;
+__device__ __noinline__ bool vb_dcheck_fail(unsigned line)
 {
     atomicCAS(&vb_check_word, 0u, line);
     return false;
 }
-#define VB_DCHECK(cond) ((cond) ? true : ::vb::vb_dcheck_fail(__LINE__))
+unsigned vb_check_take()
+{
+    unsigned w = 0;
+    const unsigned z = 0;
+    if (cudaMemcpyFromSymbol(&w, vb_check_word, sizeof w) != cudaSuccess) return 0;
+    cudaMemcpyToSymbol(vb_check_word, &z, sizeof z);
+    return w;
+}
+struct VbCheckRegistrar {
+    VbCheckRegistrar() { check_register(&vb_check_take); }
+} vb_check_registrar;
+}  // namespace
+#define VB_DCHECK(cond) ((cond) ? true : vb_dcheck_fail(__LINE__))
 #else
 #define VB_DCHECK(cond) true
 #endif

@@ -63,6 +63,8 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
     using namespace t2;
     using T = typename std::conditional<MIXED, float, double>::type;
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    // check build only: TMA destinations need a 128-byte aligned base (uniform)
+    if (!VB_DCHECK(((uintptr_t)smem_raw & 127) == 0)) return;
     t2::Smem<T, NS> &S = *reinterpret_cast<t2::Smem<T, NS> *>(smem_raw);
     __shared__ double red[32];
     __shared__ int item_sh;
@@ -79,6 +81,7 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
     const Geom &g = B.g;
     Ctrl *ctrl = B.ctrl;
     const CUtensorMap *tm = B.map[STAGE - 1];
+    if (!VB_DCHECK(((uintptr_t)tm & 63) == 0)) return;  // check build only (uniform)
     const double *__restrict__ Uin = STAGE == 1 ? B.U : B.U1;
     const double *U0 = B.U;
     double *Uout = STAGE == 1 ? B.U1 : B.U;

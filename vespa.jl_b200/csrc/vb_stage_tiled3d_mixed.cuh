@@ -187,6 +187,8 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     using namespace t3;
     using namespace t3m;
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    // check build only: TMA destinations need a 128-byte aligned base (uniform)
+    if (!VB_DCHECK(((uintptr_t)smem_raw & 127) == 0)) return;
     t3m::Smem<NS> &S = *reinterpret_cast<t3m::Smem<NS> *>(smem_raw);
     __shared__ double red[32];
     __shared__ int item_sh;
@@ -232,6 +234,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
     }
     const Geom &g = B.g;
     const CUtensorMap *tm = B.map[STAGE - 1];
+    if (!VB_DCHECK(((uintptr_t)tm & 63) == 0)) return;  // check build only (uniform)
     const double *__restrict__ Uin = STAGE == 1 ? B.U : B.U1;
     const double *U0 = B.U;
     double *Uout = STAGE == 1 ? B.U1 : B.U;
