@@ -84,6 +84,7 @@ struct vb_amr {
     // leaf and cell lists of stride lv_cap, face lists of stride lv_fcap,
     // lv_levels levels; counts on the device and their host copy
     int *lv_leaf = nullptr, *lv_cell = nullptr, *lv_face = nullptr, *lv_cnt = nullptr;
+    int *lv_bc = nullptr, *lv_off = nullptr;  // scratch of the list passes
     int64_t lv_cap = 0, lv_fcap = 0;
     int lv_levels = 0;
     int lv_n[3 * vb::AMR_LIST_STRIDE] = {};
@@ -101,7 +102,7 @@ void release(vb_amr *a)
     void *p[] = {a->U, a->U1, a->U2, a->lev2, a->cx2, a->reg, a->lev, a->cx, a->rep, a->faceid, a->kind, a->off,
                  a->fbase, a->cnt, a->fcnt, a->ecnt, a->bsum, a->tag, a->F, a->farea,
                  a->fL, a->fR, a->ent, a->fax, a->hkey, a->hval, a->word, a->ctrl,
-                 a->partials, a->totals, a->lv_leaf, a->lv_cell, a->lv_face, a->lv_cnt};
+                 a->partials, a->totals, a->lv_leaf, a->lv_cell, a->lv_face, a->lv_cnt, a->lv_bc, a->lv_off};
     for (void *q : p) cudaFree(q);
     cudaFreeHost(a->hword);
     cudaFreeHost(a->hctrl);
@@ -409,9 +410,12 @@ int build_level_lists(vb_amr *a)
 {
     const int L = a->maxlev + 1;
     if (a->lv_cap != a->cap || a->lv_fcap != a->fcap || a->lv_levels < L) {
+        const int64_t nb = ((a->cap > a->fcap ? a->cap : a->fcap) + 255) / 256 + 1;
         int rc = realloc_dev(&a->lv_leaf, L * a->cap);
         if (!rc) rc = realloc_dev(&a->lv_cell, L * a->cap);
         if (!rc) rc = realloc_dev(&a->lv_face, L * (a->fcap > 0 ? a->fcap : 1));
+        if (!rc) rc = realloc_dev(&a->lv_bc, nb * 2 * vb::AMR_LIST_STRIDE);
+        if (!rc) rc = realloc_dev(&a->lv_off, nb * vb::AMR_LIST_STRIDE);
         if (!rc && !a->lv_cnt) rc = realloc_dev(&a->lv_cnt, 3 * vb::AMR_LIST_STRIDE);
         if (rc) {
             a->lv_cap = a->lv_fcap = 0;
@@ -424,7 +428,7 @@ int build_level_lists(vb_amr *a)
     }
     cudaStream_t s = a->ctx->stream;
     VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_level_lists(a->dev, a->lv_leaf, a->lv_cell, a->lv_face,
-                                                       a->lv_cnt, s));
+                                                       a->lv_cnt, a->lv_bc, a->lv_off, s));
     VB_CUDA(cudaMemcpyAsync(a->lv_n, a->lv_cnt, sizeof a->lv_n, cudaMemcpyDeviceToHost, s));
     VB_CUDA(cudaStreamSynchronize(s));
     return VB_OK;

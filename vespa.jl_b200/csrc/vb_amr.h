@@ -54,8 +54,9 @@ struct AmrStageArgs {
     double *mirror;
 };
 
-// Per-level work lists of a subcycled root step, each entry once and in no
-// particular order (every thread's work is independent of the others'):
+// Per-level work lists of a subcycled root step, each entry once, in the
+// mesh tables' index order within each block of 256 elements and insertion
+// stream (vb_amr_kern.cu):
 //   leaf[l]: the leaves of level l (CFL maximum, register zeroing, reflux);
 //   cell[l]: the leaves a level-l substep's cell kernel must visit -- level l,
 //            and the level l-1 leaves with a face to a level-l leaf (their
@@ -125,9 +126,11 @@ int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cuda
 // its n leaves (all of that level) only.
 int launch_amr_cfl_bits(const AmrDev &m, const double *U, int level, unsigned long long *bits,
                         cudaStream_t s, const int *list = nullptr, int n = 0);
-// Fill the per-level work lists (counts in `cnt` zeroed here).
+// Fill the per-level work lists and their counts (`cnt`, three blocks of
+// AMR_LIST_STRIDE); `bc` and `off` are scratch of 2 * AMR_LIST_STRIDE and
+// AMR_LIST_STRIDE ints per 256 faces (or leaves, if more).
 int launch_amr_level_lists(const AmrDev &m, int *leaf, int *cell, int *face, int *cnt,
-                           cudaStream_t s);
+                           int *bc, int *off, cudaStream_t s);
 // Device-driven subcycling (graph nodes, one thread each).  plan: from the
 // level's CFL maximum and its dt target (the parent's substep dt when
 // `target_src` is set) the substep count and dt, and the WHILE condition
