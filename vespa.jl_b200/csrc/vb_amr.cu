@@ -62,9 +62,8 @@ struct vb_amr {
     int64_t hcap = 0;
     uint64_t *hkey = nullptr;
     int *hval = nullptr;
-    // small device words: [0] error bits, [1] unused, [2] max level, [3] scan total (faces
-    // in a table build), [4] tags, [5] entries of a table build, [8, 8 + BAL_GROUP) marks
-    // changed by each balance pass of a group
+    // small device words: [0] error bits, [1] unused, [2] max level, [3] scan total, [4] tags,
+    // [8, 8 + BAL_GROUP) marks changed by each balance pass of a group
     int *word = nullptr, *hword = nullptr;
     vb::Ctrl *ctrl = nullptr, *hctrl = nullptr;
     double *partials = nullptr, *totals = nullptr, *htot = nullptr;
@@ -80,14 +79,6 @@ struct vb_amr {
     int64_t sg_version = -1;
     int64_t table_version = 0;
     int sg_launches = 0;
-    // the graph's per-level work lists (vb::AmrStageArgs), built with it:
-    // leaf and cell lists of stride lv_cap, face lists of stride lv_fcap,
-    // lv_levels levels; counts on the device and their host copy
-    int *lv_leaf = nullptr, *lv_cell = nullptr, *lv_face = nullptr, *lv_cnt = nullptr;
-    int *lv_bc = nullptr, *lv_off = nullptr;  // scratch of the list passes
-    int64_t lv_cap = 0, lv_fcap = 0;
-    int lv_levels = 0;
-    int lv_n[3 * vb::AMR_LIST_STRIDE] = {};
 };
 
 namespace {
@@ -102,7 +93,7 @@ void release(vb_amr *a)
     void *p[] = {a->U, a->U1, a->U2, a->lev2, a->cx2, a->reg, a->lev, a->cx, a->rep, a->faceid, a->kind, a->off,
                  a->fbase, a->cnt, a->fcnt, a->ecnt, a->bsum, a->tag, a->F, a->farea,
                  a->fL, a->fR, a->ent, a->fax, a->hkey, a->hval, a->word, a->ctrl,
-                 a->partials, a->totals, a->lv_leaf, a->lv_cell, a->lv_face, a->lv_cnt, a->lv_bc, a->lv_off};
+                 a->partials, a->totals};
     for (void *q : p) cudaFree(q);
     cudaFreeHost(a->hword);
     cudaFreeHost(a->hctrl);
@@ -184,16 +175,18 @@ int build_tables(vb_amr *a)
         if (rc) return rc;
         a->hcap = hc;
     }
-    // Face and entry arrays sized for the most these leaves can have (a leaf
-    // emits at most its hi and lo face per axis; its CSR holds those and at
-    // most 2^(nd-1) finer faces per side), so the whole build queues behind
-    // one read of the totals and the error bits.
-    const int64_t nf_max = 2ll * a->nd * a->n;
-    const int64_t ne_max = nf_max * (1 + (1 << (a->nd - 1)));
-    int rc = VB_OK;
-    if (nf_max > a->fcap) {
+    VB_CUDA(cudaMemsetAsync(a->word, 0, sizeof(int) * NWORD, s));
+    vb::AmrTopo t = topo(a);
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_hash_build(t, a->hkey, a->hval, a->word, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_kinds(t, a->kind, a->rep, a->fcnt, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->fcnt, a->n, a->fbase, a->bsum, a->word + 3, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_csr_count(t, a->kind, a->fcnt, a->ecnt, s));
+    int rc = sync_words(a);
+    if (rc) return rc;
+    const int nf = a->hword[3];
+    if (nf > a->fcap) {
         int64_t c = a->fcap ? a->fcap : 4096;
-        while (c < nf_max) c *= 2;
+        while (c < nf) c *= 2;
         rc = realloc_dev(&a->fL, c);
         if (!rc) rc = realloc_dev(&a->fR, c);
         if (!rc) rc = realloc_dev(&a->fax, c);
@@ -202,30 +195,24 @@ int build_tables(vb_amr *a)
         if (rc) return rc;
         a->fcap = c;
     }
-    if (ne_max > a->ecap) {
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_faces(t, a->kind, a->rep, a->fbase, a->areas, a->fL,
+                                                 a->fR, a->fax, a->farea, a->faceid, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->ecnt, a->n, a->off, a->bsum, a->word + 3, s));
+    rc = sync_words(a);
+    if (rc) return rc;
+    const int ne = a->hword[3];
+    if (ne > a->ecap) {
         int64_t c = a->ecap ? a->ecap : 8192;
-        while (c < ne_max) c *= 2;
+        while (c < ne) c *= 2;
         rc = realloc_dev(&a->ent, c);
         if (rc) return rc;
         a->ecap = c;
     }
-    VB_CUDA(cudaMemsetAsync(a->word, 0, sizeof(int) * NWORD, s));
-    vb::AmrTopo t = topo(a);
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_hash_build(t, a->hkey, a->hval, a->word, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_kinds(t, a->kind, a->rep, a->fcnt, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->fcnt, a->n, a->fbase, a->bsum, a->word + 3, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_csr_count(t, a->kind, a->fcnt, a->ecnt, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_faces(t, a->kind, a->rep, a->fbase, a->areas, a->fL,
-                                                 a->fR, a->fax, a->farea, a->faceid, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->ecnt, a->n, a->off, a->bsum, a->word + 5, s));
     VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_csr_fill(t, a->kind, a->rep, a->faceid, a->off,
                                                     a->ent, a->word, s));
     rc = sync_words(a);
     if (rc) return rc;
     if (a->hword[0]) return fail(VB_ECUDA, "AMR table build failed (hash or CSR overflow)");
-    const int nf = a->hword[3];
-    const int ne = a->hword[5];
-    if (nf > a->fcap || ne > a->ecap) return fail(VB_ECUDA, "AMR table build: face count out of range");
     a->nface = nf;
     a->nent = ne;
     vb::AmrDev &m = a->dev;
@@ -403,44 +390,6 @@ struct SubBody {
     cudaGraphConditionalHandle handle;
 };
 
-// The per-level work lists for the current tables, and their counts on the
-// host (one read).  The graph's kernels are sized by these counts, so a
-// substep of level l touches only the leaves and faces it needs.
-int build_level_lists(vb_amr *a)
-{
-    const int L = a->maxlev + 1;
-    if (a->lv_cap != a->cap || a->lv_fcap != a->fcap || a->lv_levels < L) {
-        const int64_t nb = ((a->cap > a->fcap ? a->cap : a->fcap) + 255) / 256 + 1;
-        int rc = realloc_dev(&a->lv_leaf, L * a->cap);
-        if (!rc) rc = realloc_dev(&a->lv_cell, L * a->cap);
-        if (!rc) rc = realloc_dev(&a->lv_face, L * (a->fcap > 0 ? a->fcap : 1));
-        if (!rc) rc = realloc_dev(&a->lv_bc, nb * 2 * vb::AMR_LIST_STRIDE);
-        if (!rc) rc = realloc_dev(&a->lv_off, nb * vb::AMR_LIST_STRIDE);
-        if (!rc && !a->lv_cnt) rc = realloc_dev(&a->lv_cnt, 3 * vb::AMR_LIST_STRIDE);
-        if (rc) {
-            a->lv_cap = a->lv_fcap = 0;
-            a->lv_levels = 0;
-            return rc;
-        }
-        a->lv_cap = a->cap;
-        a->lv_fcap = a->fcap;
-        a->lv_levels = L;
-    }
-    cudaStream_t s = a->ctx->stream;
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_level_lists(a->dev, a->lv_leaf, a->lv_cell, a->lv_face,
-                                                       a->lv_cnt, a->lv_bc, a->lv_off, s));
-    VB_CUDA(cudaMemcpyAsync(a->lv_n, a->lv_cnt, sizeof a->lv_n, cudaMemcpyDeviceToHost, s));
-    VB_CUDA(cudaStreamSynchronize(s));
-    return VB_OK;
-}
-
-const int *lv_list(const vb_amr *a, int kind, int l)
-{
-    return kind == 2 ? a->lv_face + l * a->fcap : (kind ? a->lv_cell : a->lv_leaf) + l * a->cap;
-}
-
-int lv_count(const vb_amr *a, int kind, int l) { return a->lv_n[kind * vb::AMR_LIST_STRIDE + l]; }
-
 // In the graph being captured on `s`: level l's CFL maximum, plan and WHILE
 // node; the node's (empty) body goes to `todo`.
 int emit_level_head(vb_amr *a, cudaStream_t s, int l, std::vector<SubBody> &todo)
@@ -453,8 +402,7 @@ int emit_level_head(vb_amr *a, cudaStream_t s, int l, std::vector<SubBody> &todo
     if (st != cudaStreamCaptureStatusActive || !g) return fail(VB_ECUDA, "subcycle graph: no capture");
     cudaGraphConditionalHandle h;
     VB_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_cfl_bits(a->dev, a->U, l, &a->sub[l].invdt_bits, s,
-                                                    lv_list(a, 0, l), lv_count(a, 0, l)));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_cfl_bits(a->dev, a->U, l, &a->sub[l].invdt_bits, s));
     VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_sub_plan(a->sub, l, a->g.cfl,
                                                     l > 0 ? &a->sub[l - 1].dt_sub : nullptr, h,
                                                     a->suberr, s));
@@ -481,20 +429,11 @@ int fill_level_body(vb_amr *a, cudaStream_t s, SubBody b, std::vector<SubBody> &
                                           cudaStreamCaptureModeThreadLocal));
     int rc = VB_OK;
     auto body = [&]() -> int {
-        if (has_finer)
-            VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_zero_reg(a->dev, l, s, lv_list(a, 0, l),
-                                                            lv_count(a, 0, l)));
+        if (has_finer) VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_zero_reg(a->dev, l, s));
         vb::AmrStageArgs sa{};
         sa.dt = 0.0;
         sa.level = l;
         sa.dt_dev = &a->sub[l].dt_sub;
-        // the level's lists; U1 equals U outside them (root_step_graph, and
-        // the mirrored writes of stage 2 and the reflux)
-        sa.faces = lv_list(a, 2, l);
-        sa.nfaces = lv_count(a, 2, l);
-        sa.cells = lv_list(a, 1, l);
-        sa.ncells = lv_count(a, 1, l);
-        sa.mirror = a->U1;
         int nr = 0;
         if (l > 0) { sa.reg_level[nr] = l - 1; sa.reg_scale[nr] = 1.0; ++nr; }
         if (has_finer) { sa.reg_level[nr] = l; sa.reg_scale[nr] = -1.0; ++nr; }
@@ -505,8 +444,7 @@ int fill_level_body(vb_amr *a, cudaStream_t s, SubBody b, std::vector<SubBody> &
         if (has_finer) {
             int r = emit_level_head(a, s, l + 1, todo);
             if (r) return r;
-            VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_reflux(a->dev, a->U, l, s, lv_list(a, 0, l),
-                                                          lv_count(a, 0, l), a->U1));
+            VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_reflux(a->dev, a->U, l, s));
         }
         VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_sub_next(a->sub, l, b.handle, a->suberr, s));
         return VB_OK;
@@ -530,13 +468,12 @@ int build_subcycle_graph(vb_amr *a)
         VB_CUDA(cudaMalloc(&a->sub, sizeof(vb::AmrSubLevel) * (vb::AMR_MAX_LEVEL + 1)));
         VB_CUDA(cudaMalloc(&a->suberr, sizeof(int)));
     }
-    int rc = build_level_lists(a);
-    if (rc) return rc;
     cudaStream_t s = a->ctx->stream;
     const int64_t launches0 = a->ctx->launches;
     cudaGraph_t root = nullptr;
     VB_CUDA(cudaGraphCreate(&root, 0));
     std::vector<SubBody> todo;
+    int rc = VB_OK;
     cudaError_t e = cudaStreamBeginCaptureToGraph(s, root, nullptr, nullptr, 0,
                                                   cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) rc = fail(VB_ECUDA, std::string("subcycle capture: ") + cudaGetErrorString(e));
@@ -574,9 +511,6 @@ int root_step_graph(vb_amr *a, double dt_root)
     cudaStream_t s = a->ctx->stream;
     VB_CUDA(cudaMemsetAsync(a->sub, 0, sizeof(vb::AmrSubLevel) * (vb::AMR_MAX_LEVEL + 1), s));
     VB_CUDA(cudaMemsetAsync(a->suberr, 0, sizeof(int), s));
-    // the substeps update U1 only on their own lists' leaves, and keep it equal
-    // to U elsewhere from this copy on
-    VB_CUDA(cudaMemcpyAsync(a->U1, a->U, sizeof(double) * 5 * a->cap, cudaMemcpyDeviceToDevice, s));
     VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_sub_target(a->sub, dt_root, s));
     VB_CUDA(cudaGraphLaunch(a->sg_exec, s));
     a->ctx->launches += a->sg_launches;  // nodes of one pass (loops repeat some)
@@ -937,9 +871,8 @@ int vb_amr_evolve(vb_amr *a, double tfinal, int64_t max_steps, double refine_abo
             a->hctrl->step_limit = a->step + chunk;
             a->hctrl->active = 1;
             a->hctrl->flags = 0;
-            // queued, not awaited: the host writes hctrl again only after the
-            // pull below has synchronised the stream
-            VB_CUDA(cudaMemcpyAsync(a->ctrl, a->hctrl, sizeof(vb::Ctrl), cudaMemcpyHostToDevice, st));
+            rc = push_ctrl(a);
+            if (rc) return rc;
             VB_CUDA(cudaMemsetAsync(&a->ctrl->invdt_bits, 0, sizeof(unsigned long long), st));
             VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_cfl(a->dev, a->U, -1, a->ctrl, st));
             vb::AmrStageArgs s{};

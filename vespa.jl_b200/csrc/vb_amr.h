@@ -42,29 +42,7 @@ struct AmrStageArgs {
     // the device) and reg_scale holds the register signs (+1 / -1), the scale
     // being sign * (0.5 * dt) as evolve_level! forms it
     const double *dt_dev;
-    // set: a subcycled level's work lists (below).  The face kernel
-    // solves only `faces`, the cell kernel visits only `cells`; stage 1 then
-    // leaves the other leaves of its output alone (the caller keeps them
-    // equal to the input state) and stage 2 writes its results to `mirror`
-    // as well as to its output.
-    const int *faces;
-    int nfaces;
-    const int *cells;
-    int ncells;
-    double *mirror;
 };
-
-// Per-level work lists of a subcycled root step, each entry once, in the
-// mesh tables' index order within each block of 256 elements and insertion
-// stream (vb_amr_kern.cu):
-//   leaf[l]: the leaves of level l (CFL maximum, register zeroing, reflux);
-//   cell[l]: the leaves a level-l substep's cell kernel must visit -- level l,
-//            and the level l-1 leaves with a face to a level-l leaf (their
-//            register entries capture those faces' fluxes);
-//   face[l]: the faces with a level-l leaf on either side.
-// Lists of level l start at l * cap (leaf, cell) and l * fcap (face); the
-// counts are cnt[kind * (AMR_MAX_LEVEL + 1) + l], kind 0 leaf, 1 cell, 2 face.
-constexpr int AMR_LIST_STRIDE = AMR_MAX_LEVEL + 1;
 
 // Device state of one level of a subcycled root step (evolve_level!,
 // src/driver.jl:553-578), for the graph that runs the recursion on the
@@ -122,15 +100,9 @@ int launch_amr_csr_fill(const AmrTopo &t, const int8_t *kind, const int *rep, co
 int launch_amr_stage(const AmrDev &m, int stage, const double *Uin, const double *U0,
                      double *Uout, double *F, const AmrStageArgs &a, Ctrl *ctrl, cudaStream_t s);
 int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cudaStream_t s);
-// The same maximum into the word `bits` (not reset here); with `list`, over
-// its n leaves (all of that level) only.
+// The same maximum into the word `bits` (not reset here).
 int launch_amr_cfl_bits(const AmrDev &m, const double *U, int level, unsigned long long *bits,
-                        cudaStream_t s, const int *list = nullptr, int n = 0);
-// Fill the per-level work lists and their counts (`cnt`, three blocks of
-// AMR_LIST_STRIDE); `bc` and `off` are scratch of 2 * AMR_LIST_STRIDE and
-// AMR_LIST_STRIDE ints per 256 faces (or leaves, if more).
-int launch_amr_level_lists(const AmrDev &m, int *leaf, int *cell, int *face, int *cnt,
-                           int *bc, int *off, cudaStream_t s);
+                        cudaStream_t s);
 // Device-driven subcycling (graph nodes, one thread each).  plan: from the
 // level's CFL maximum and its dt target (the parent's substep dt when
 // `target_src` is set) the substep count and dt, and the WHILE condition
@@ -143,12 +115,8 @@ int launch_amr_sub_next(AmrSubLevel *sub, int level, cudaGraphConditionalHandle 
 int launch_amr_sub_target(AmrSubLevel *sub, double dt, cudaStream_t s);
 int launch_amr_tag(const AmrDev &m, const double *U, double above, int max_level, uint8_t *tag,
                    double *ind, int *ntag, cudaStream_t s);
-// With `list`: over its n leaves (all of that level); reflux then writes the
-// corrected state to `mirror` too.
-int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s,
-                      const int *list = nullptr, int n = 0, double *mirror = nullptr);
-int launch_amr_zero_reg(const AmrDev &m, int level, cudaStream_t s, const int *list = nullptr,
-                        int n = 0);
+int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s);
+int launch_amr_zero_reg(const AmrDev &m, int level, cudaStream_t s);
 int launch_amr_totals(const AmrDev &m, const double *U, double *partials, int npart, double *out,
                       cudaStream_t s);
 

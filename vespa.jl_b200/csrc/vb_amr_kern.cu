@@ -70,14 +70,11 @@ __device__ __forceinline__ void amr_face(const AmrDev &m, const double *__restri
 }
 
 __global__ void __launch_bounds__(256) k_amr_faces(AmrDev m, const double *__restrict__ U,
-                                                   double *__restrict__ F, const Ctrl *gate,
-                                                   const int *__restrict__ list, int nlist)
+                                                   double *__restrict__ F, const Ctrl *gate)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (list ? nlist : m.nface)) return;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nface) return;
     if (gate && !gate->active) return;
-    const int f = list ? list[t] : t;
-    if (!VB_DCHECK(f >= 0 && f < m.nface)) return;  // check build only
     switch (m.fax[f]) {
     case 0: amr_face<1>(m, U, f, F); break;
     case 1: amr_face<2>(m, U, f, F); break;
@@ -105,10 +102,9 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
         if (!ctrl->active) return;
         dt = ctrl->dt;
     }
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double invdt = 0.0;
-    const int i = t < (a.cells ? a.ncells : m.nleaf) ? (a.cells ? a.cells[t] : t) : -1;
-    if (i >= 0 && VB_DCHECK(i < m.nleaf)) {  // (the check: check build only)
+    if (i < m.nleaf) {
         const int li = m.lev[i];
         const bool upd = a.level < 0 || li == a.level;
         int rslot = -1;
@@ -159,7 +155,6 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
                     else
                         un[k] = 0.5 * U0[o] + 0.5 * (Uin[o] - invV * acc[k]);
                     Uout[o] = un[k];
-                    if (STAGE == 2 && a.mirror) a.mirror[o] = un[k];
                 }
                 if constexpr (STAGE == 2) {
                     double W[5];
@@ -171,7 +166,7 @@ k_amr_cells(AmrDev m, const double *__restrict__ Uin, const double *U0, double *
             }
         }
         if constexpr (STAGE == 1) {
-            if (!upd && !a.cells)
+            if (!upd)
 #pragma unroll
                 for (int k = 0; k < 5; ++k) Uout[(int64_t)k * m.cap + i] = Uin[(int64_t)k * m.cap + i];
         }
@@ -197,16 +192,14 @@ __global__ void __launch_bounds__(256) k_amr_cfl(AmrDev m, const double *__restr
     block_max_to(&ctrl->invdt_bits, invdt, red);
 }
 
-// the same maximum into a given word; with a list, over its leaves
+// the same maximum into a given word
 __global__ void __launch_bounds__(256) k_amr_cfl_bits(AmrDev m, const double *__restrict__ U,
-                                                      int level, unsigned long long *bits,
-                                                      const int *__restrict__ list, int nlist)
+                                                      int level, unsigned long long *bits)
 {
     __shared__ double red[32];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = t < (list ? nlist : m.nleaf) ? (list ? list[t] : t) : -1;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double invdt = 0.0;
-    if (i >= 0 && VB_DCHECK(i < m.nleaf) && (level < 0 || m.lev[i] == level)) {
+    if (i < m.nleaf && (level < 0 || m.lev[i] == level)) {
         double W[5];
         amr_prim(m, U, i, W);
         const double c = sqrt(m.gamma * W[4] / W[0]);
@@ -292,149 +285,26 @@ __global__ void __launch_bounds__(256) k_amr_tag(AmrDev m, const double *__restr
     if (on && ntag) atomicAdd(ntag, 1);
 }
 
-// _reflux_apply! (src/reflux.jl:91-101) for the leaves of one level (with a
-// list: its leaves, and the result mirrored)
-__global__ void k_amr_reflux(AmrDev m, double *U, int level, const int *__restrict__ list,
-                             int nlist, double *mirror)
+// _reflux_apply! (src/reflux.jl:91-101) for the leaves of one level
+__global__ void k_amr_reflux(AmrDev m, double *U, int level)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (list ? nlist : m.nleaf)) return;
-    const int i = list ? list[t] : t;
-    if (!VB_DCHECK(i >= 0 && i < m.nleaf) || m.lev[i] != level) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nleaf || m.lev[i] != level) return;
     const double invV = 1.0 / m.vol[level];
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
         const int64_t o = (int64_t)k * m.cap + i;
-        const double u = U[o] - invV * m.reg[o];
-        U[o] = u;
-        if (mirror) mirror[o] = u;
+        U[o] = U[o] - invV * m.reg[o];
         m.reg[o] = 0.0;
     }
 }
 
-__global__ void k_amr_zero_reg(AmrDev m, int level, const int *__restrict__ list, int nlist)
+__global__ void k_amr_zero_reg(AmrDev m, int level)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (list ? nlist : m.nleaf)) return;
-    const int i = list ? list[t] : t;
-    if (!VB_DCHECK(i >= 0 && i < m.nleaf) || m.lev[i] != level) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nleaf || m.lev[i] != level) return;
 #pragma unroll
     for (int k = 0; k < 5; ++k) m.reg[(int64_t)k * m.cap + i] = 0.0;
-}
-
-// The per-level work lists (vb_amr.h), each in ascending index order within
-// its two insertion streams (so that the kernels reading them access leaves
-// and faces in the memory order of the mesh tables).  An element inserts
-// itself into up to two lists (stream 0 and 1):
-//   kind 0, leaves: its level;
-//   kind 1, cells: its level, and its level + 1 if it has a face to a leaf
-//     one level finer (register capture during the finer level's substeps);
-//   kind 2, faces: the level of its left side, and that of its right side
-//     when different.
-// A list is built per block in three passes: per-block counts of every
-// (level, stream), an exclusive scan over blocks per level, and a scatter in
-// which each element's rank within its block comes from warp match masks.
-constexpr int LB = 256;  // elements per block of the list passes
-
-template <int KIND>
-__device__ __forceinline__ void list_keys(const AmrDev &m, int e, int &k0, int &k1)
-{
-    if (KIND == 2) {
-        const int L = m.fL[e], R = m.fR[e];
-        const bool ok = VB_DCHECK(L < m.nleaf && R < m.nleaf);  // check build only
-        const int a = (ok && L >= 0) ? m.lev[L] : -1, b = (ok && R >= 0) ? m.lev[R] : -1;
-        k0 = a;
-        k1 = (b >= 0 && b != a) ? b : -1;
-        return;
-    }
-    const int li = m.lev[e];
-    k0 = VB_DCHECK(li >= 0 && li < AMR_LIST_STRIDE) ? li : -1;  // check build only
-    k1 = -1;
-    if (KIND == 1 && k0 >= 0) {
-        bool finer = false;
-        for (int q = m.off[e]; q < m.off[e + 1] && !finer; ++q) {
-            if (!VB_DCHECK(q >= 0 && q < m.nent)) break;
-            const int code = m.ent[q];
-            const int f = code >> 1;
-            if (!VB_DCHECK(f >= 0 && f < m.nface)) break;
-            const int other = (code & 1) ? m.fL[f] : m.fR[f];
-            finer = other >= 0 && VB_DCHECK(other < m.nleaf) && m.lev[other] == li + 1;
-        }
-        if (finer) k1 = li + 1;
-    }
-}
-
-// pass 1: bc[block][2 * level + stream] = elements of this block in that list part
-template <int KIND>
-__global__ void __launch_bounds__(LB) k_amr_list_count(AmrDev m, int n, int *bc)
-{
-    __shared__ int c[2 * AMR_LIST_STRIDE];
-    if (threadIdx.x < 2 * AMR_LIST_STRIDE) c[threadIdx.x] = 0;
-    __syncthreads();
-    const int e = blockIdx.x * LB + threadIdx.x;
-    if (e < n) {
-        int k0, k1;
-        list_keys<KIND>(m, e, k0, k1);
-        if (k0 >= 0) atomicAdd(&c[2 * k0], 1);
-        if (k1 >= 0) atomicAdd(&c[2 * k1 + 1], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < 2 * AMR_LIST_STRIDE)
-        bc[(int64_t)blockIdx.x * 2 * AMR_LIST_STRIDE + threadIdx.x] = c[threadIdx.x];
-}
-
-// pass 2 (one block, a warp per level): off[block][level] = exclusive prefix of
-// the level's per-block totals; cnt[level] = the list's length
-__global__ void __launch_bounds__(32 * AMR_LIST_STRIDE) k_amr_list_scan(const int *bc, int nb,
-                                                                        int *off, int *cnt)
-{
-    const int l = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int run = 0;
-    for (int b0 = 0; b0 < nb; b0 += 32) {
-        const int b = b0 + lane;
-        const int v = b < nb ? bc[(int64_t)b * 2 * AMR_LIST_STRIDE + 2 * l] +
-                                   bc[(int64_t)b * 2 * AMR_LIST_STRIDE + 2 * l + 1]
-                             : 0;
-        int x = v;  // inclusive warp scan
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, d);
-            if (lane >= d) x += y;
-        }
-        if (b < nb) off[(int64_t)b * AMR_LIST_STRIDE + l] = run + x - v;
-        run += __shfl_sync(0xffffffffu, x, 31);
-    }
-    if (lane == 0) cnt[l] = run;
-}
-
-// pass 3: each element at its rank (block offset, stream part, warps before
-// it, lanes before it with the same key)
-template <int KIND>
-__global__ void __launch_bounds__(LB) k_amr_list_scatter(AmrDev m, int n, const int *bc,
-                                                         const int *off, int *list, int64_t stride)
-{
-    __shared__ int wc[LB / 32][AMR_LIST_STRIDE];
-    const int e = blockIdx.x * LB + threadIdx.x;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int keys[2] = {-1, -1};
-    if (e < n) list_keys<KIND>(m, e, keys[0], keys[1]);
-    const int *bcb = bc + (int64_t)blockIdx.x * 2 * AMR_LIST_STRIDE;
-    const int *offb = off + (int64_t)blockIdx.x * AMR_LIST_STRIDE;
-    for (int st = 0; st < 2; ++st) {
-        for (int q = threadIdx.x; q < (LB / 32) * AMR_LIST_STRIDE; q += LB) (&wc[0][0])[q] = 0;
-        __syncthreads();
-        const int key = keys[st];
-        const unsigned mask = __match_any_sync(0xffffffffu, key);
-        const int rank = __popc(mask & ((1u << lane) - 1u));
-        if (key >= 0 && lane == __ffs(mask) - 1) wc[w][key] = __popc(mask);
-        __syncthreads();
-        if (key >= 0) {
-            int pos = offb[key] + (st == 1 ? bcb[2 * key] : 0) + rank;
-            for (int v = 0; v < w; ++v) pos += wc[v][key];
-            list[(int64_t)key * stride + pos] = e;
-        }
-        __syncthreads();
-    }
 }
 
 // conserved_totals: fixed partition (deterministic), then one folding block
@@ -469,17 +339,14 @@ static unsigned blocks(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs 
 int launch_amr_stage(const AmrDev &m, int stage, const double *Uin, const double *U0,
                      double *Uout, double *F, const AmrStageArgs &a, Ctrl *ctrl, cudaStream_t s)
 {
-    const int nf = a.faces ? a.nfaces : m.nface;
-    const int nc = a.cells ? a.ncells : m.nleaf;
-    if (nf > 0)
-        k_amr_faces<<<blocks(nf, 256), 256, 0, s>>>(m, Uin, F,
-                                                    (a.dt < 0.0 && !a.dt_dev) ? ctrl : nullptr,
-                                                    a.faces, a.nfaces);
+    if (m.nface > 0)
+        k_amr_faces<<<blocks(m.nface, 256), 256, 0, s>>>(m, Uin, F,
+                                                         (a.dt < 0.0 && !a.dt_dev) ? ctrl : nullptr);
     if (stage == 1)
-        k_amr_cells<1><<<blocks(nc, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
+        k_amr_cells<1><<<blocks(m.nleaf, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
     else
-        k_amr_cells<2><<<blocks(nc, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
-    return nf > 0 ? 2 : 1;
+        k_amr_cells<2><<<blocks(m.nleaf, 256), 256, 0, s>>>(m, Uin, U0, Uout, F, a, ctrl);
+    return m.nface > 0 ? 2 : 1;
 }
 
 int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cudaStream_t s)
@@ -489,32 +356,10 @@ int launch_amr_cfl(const AmrDev &m, const double *U, int level, Ctrl *ctrl, cuda
 }
 
 int launch_amr_cfl_bits(const AmrDev &m, const double *U, int level, unsigned long long *bits,
-                        cudaStream_t s, const int *list, int n)
+                        cudaStream_t s)
 {
-    k_amr_cfl_bits<<<blocks(list ? n : m.nleaf, 256), 256, 0, s>>>(m, U, level, bits, list, n);
+    k_amr_cfl_bits<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, level, bits);
     return 1;
-}
-
-int launch_amr_level_lists(const AmrDev &m, int *leaf, int *cell, int *face, int *cnt,
-                           int *bc, int *off, cudaStream_t s)
-{
-    const int nl = (m.nleaf + LB - 1) / LB, nf = (m.nface + LB - 1) / LB;
-    int launches = 0;
-    auto one = [&](auto count, auto scatter, int n, int nb, int *list, int64_t stride, int *c) {
-        if (nb == 0) return cudaMemsetAsync(c, 0, sizeof(int) * AMR_LIST_STRIDE, s) == cudaSuccess;
-        count<<<nb, LB, 0, s>>>(m, n, bc);
-        k_amr_list_scan<<<1, 32 * AMR_LIST_STRIDE, 0, s>>>(bc, nb, off, c);
-        scatter<<<nb, LB, 0, s>>>(m, n, bc, off, list, stride);
-        launches += 3;
-        return true;
-    };
-    if (!one(k_amr_list_count<0>, k_amr_list_scatter<0>, m.nleaf, nl, leaf, m.cap, cnt) ||
-        !one(k_amr_list_count<1>, k_amr_list_scatter<1>, m.nleaf, nl, cell, m.cap,
-             cnt + AMR_LIST_STRIDE) ||
-        !one(k_amr_list_count<2>, k_amr_list_scatter<2>, m.nface, nf, face, m.fcap,
-             cnt + 2 * AMR_LIST_STRIDE))
-        return -1;
-    return launches;
 }
 
 int launch_amr_sub_plan(AmrSubLevel *sub, int level, double cfl, const double *target_src,
@@ -544,16 +389,15 @@ int launch_amr_tag(const AmrDev &m, const double *U, double above, int max_level
     return 1;
 }
 
-int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s, const int *list,
-                      int n, double *mirror)
+int launch_amr_reflux(const AmrDev &m, double *U, int level, cudaStream_t s)
 {
-    k_amr_reflux<<<blocks(list ? n : m.nleaf, 256), 256, 0, s>>>(m, U, level, list, n, mirror);
+    k_amr_reflux<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, U, level);
     return 1;
 }
 
-int launch_amr_zero_reg(const AmrDev &m, int level, cudaStream_t s, const int *list, int n)
+int launch_amr_zero_reg(const AmrDev &m, int level, cudaStream_t s)
 {
-    k_amr_zero_reg<<<blocks(list ? n : m.nleaf, 256), 256, 0, s>>>(m, level, list, n);
+    k_amr_zero_reg<<<blocks(m.nleaf, 256), 256, 0, s>>>(m, level);
     return 1;
 }
 
