@@ -187,10 +187,15 @@ __device__ __forceinline__ void load_plane(const MusclGeom &m, const double *__r
     if (p < 0 || p >= m.n[2]) return;
     const int64_t nx = m.n[0], ny = m.n[1], N = m.N;
     const double *plane = prim + p * nx * ny;
-    for (int e = threadIdx.x; e < PS; e += NT) {
-        const int f = e / PF, rc = e - f * PF, r = rc / PW, c = rc - r * PW;
+    // window cell w = r * PW + c, its five fields at w + f * PF
+    for (int w = threadIdx.x; w < PF; w += NT) {
+        const int r = w / PW, c = w - r * PW;
         const int64_t x = x0 - 2 + c, y = y0 - 2 + r;
-        if (x >= 0 && x < nx && y >= 0 && y < ny) cp_async8(slot + e, plane + f * N + y * nx + x);
+        if (x >= 0 && x < nx && y >= 0 && y < ny) {
+            const double *src = plane + y * nx + x;
+#pragma unroll
+            for (int f = 0; f < 5; ++f) cp_async8(slot + f * PF + w, src + f * N);
+        }
     }
 }
 
@@ -213,7 +218,7 @@ __global__ void __launch_bounds__(NT, 2) k_muscl_tile(MusclGeom m, const double 
     // a face between cells c and c + 1 along an axis of n cells is needed iff
     // one of the two is active; its stencil c - 1 .. c + 2 is then in the grid
     auto face_ok = [&](int64_t c, int64_t n) { return c >= ng - 1 && c <= n - ng - 1; };
-    auto slot = [&](int64_t p) { return ring + (int)((p + NSLOT) % NSLOT) * PS; };  // p >= -2
+    auto slot = [&](int64_t p) { return ring + ((int)p + NSLOT) % NSLOT * PS; };  // p >= -2
     const int own = (ty + 2) * PW + tx + 2;  // this column's cell in a plane window
     const int zoff[5] = {0, PF, 4 * PF, 2 * PF, 3 * PF};  // rho, eint, vz | vx, vy
 
