@@ -170,9 +170,28 @@ __device__ __forceinline__ double lap_row(const Geom &g, const GravP &P, const d
 // same CSR row order as lap_row (lo faces of lower cells z, y, x; hi faces
 // x, y, z, a 1-cell axis twice; lo faces wrapped to a higher index x, y, z),
 // with 32-bit indices: the same bits as lap_row<3> on that grid.
+// (x, y, z) of cell i of a periodic n^3 cube, x fastest: masks and shifts
+// when n is a power of two, else two unsigned divisions
+__device__ __forceinline__ void cube_coords(int n, int i, int c[3])
+{
+    const unsigned u = (unsigned)i, un = (unsigned)n;
+    if ((un & (un - 1u)) == 0u) {
+        const int sh = __ffs(n) - 1;
+        c[0] = (int)(u & (un - 1u));
+        c[1] = (int)((u >> sh) & (un - 1u));
+        c[2] = (int)(u >> (2 * sh));
+    } else {
+        const unsigned q = u / un, r = q / un;
+        c[0] = (int)(u - q * un);
+        c[1] = (int)(q - r * un);
+        c[2] = (int)r;
+    }
+}
+
 __device__ __forceinline__ double lap_cube(int n, const GravP &P, const double *__restrict__ x, int i)
 {
-    const int c[3] = {i % n, (i / n) % n, i / (n * n)};
+    int c[3];
+    cube_coords(n, i, c);
     const int st[3] = {1, n, n * n};
     const double xc = x[i];
     double s = 0.0;
@@ -525,7 +544,9 @@ __device__ __forceinline__ int mg_wrap(int a, int n) { return a < 0 ? n - 1 : (a
 __device__ __forceinline__ double mg_jacobi_cell(int n, int i, double h2, const double *phiold,
                                                  const double *__restrict__ b)
 {
-    const int x = i % n, y = (i / n) % n, z = i / (n * n);
+    int c[3];
+    cube_coords(n, i, c);
+    const int x = c[0], y = c[1], z = c[2];
     const int nn = n * n;
     const double s = phiold[i - x + mg_wrap(x - 1, n)] + phiold[i - x + mg_wrap(x + 1, n)] +
                      phiold[i - y * n + mg_wrap(y - 1, n) * n] + phiold[i - y * n + mg_wrap(y + 1, n) * n] +
@@ -568,7 +589,9 @@ __global__ void __launch_bounds__(GB, GP_SM) k_mg_residual(int n, double invh2, 
     if (gc->done) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n * n * n) return;
-    const int x = i % n, y = (i / n) % n, z = i / (n * n);
+    int c[3];
+    cube_coords(n, i, c);
+    const int x = c[0], y = c[1], z = c[2];
     const int nn = n * n;
     const double s = phi[i - x + mg_wrap(x - 1, n)] + phi[i - x + mg_wrap(x + 1, n)] +
                      phi[i - y * n + mg_wrap(y - 1, n) * n] + phi[i - y * n + mg_wrap(y + 1, n) * n] +
@@ -583,8 +606,9 @@ __global__ void __launch_bounds__(GB, GP_SM) k_mg_restrict(int nc, const double 
     if (gc->done) return;
     const int I = blockIdx.x * blockDim.x + threadIdx.x;
     if (I >= nc * nc * nc) return;
-    const int X = I % nc, Y = (I / nc) % nc, Z = I / (nc * nc);
-    const int n = 2 * nc, x = 2 * X, y = 2 * Y, z = 2 * Z;
+    int C[3];
+    cube_coords(nc, I, C);
+    const int n = 2 * nc, x = 2 * C[0], y = 2 * C[1], z = 2 * C[2];
     auto f = [&](int a, int b_, int c) { return rf[a + n * (b_ + n * c)]; };
     bc[I] = 0.125 * (f(x, y, z) + f(x + 1, y, z) + f(x, y + 1, z) + f(x + 1, y + 1, z) + f(x, y, z + 1) +
                      f(x + 1, y, z + 1) + f(x, y + 1, z + 1) + f(x + 1, y + 1, z + 1));
@@ -600,7 +624,9 @@ __global__ void __launch_bounds__(GB, GP_SM) k_mg_prolong_add(int nc, const doub
     const int n = 2 * nc;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n * n * n) return;
-    const int x = i % n, y = (i / n) % n, z = i / (n * n);
+    int c[3];
+    cube_coords(n, i, c);
+    const int x = c[0], y = c[1], z = c[2];
     const int ic[2] = {x / 2, mg_wrap(x / 2 + ((x & 1) ? 1 : -1), nc)};
     const int jc[2] = {y / 2, mg_wrap(y / 2 + ((y & 1) ? 1 : -1), nc)};
     const int kc[2] = {z / 2, mg_wrap(z / 2 + ((z & 1) ? 1 : -1), nc)};
