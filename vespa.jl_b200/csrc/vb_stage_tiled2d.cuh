@@ -137,8 +137,8 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
     auto issue = [&](int q) {
         const int p = r0 - 2 + q;
         const int y = pery ? ((p % ny) + ny) % ny : p;  // out-of-range rows read the zero fill
-        double *dst = S.u[(qb + q) % NS];
-        uint64_t *bar = &S.bar[(qb + q) % NS];
+        double *dst = S.u[(unsigned)(qb + q) % NS];
+        uint64_t *bar = &S.bar[(unsigned)(qb + q) % NS];
         const int xl = (perx && x0 == 0) ? nx - 2 : x0 - 2;
         const int xh = (perx && x0 + TX == nx) ? 0 : x0 + TX;
         mbar_expect_tx(bar, ROW_BYTES);
@@ -151,8 +151,8 @@ k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *wor
         for (int q = 0; q < NS && q < nrows; ++q) issue(q);
     }
     auto consume = [&](int q, T Wown[5], bool halo) {
-        const int b = (qb + q) % NS;
-        if (!mbar_wait(&S.bar[b], ((qb + q) / NS) & 1, WAIT_LIMIT_NS)) stall_sh = 1;
+        const int b = (unsigned)(qb + q) % NS;
+        if (!mbar_wait(&S.bar[b], ((unsigned)(qb + q) / NS) & 1, WAIT_LIMIT_NS)) stall_sh = 1;
         const double *u = S.u[b];
         double uu[5];
 #pragma unroll

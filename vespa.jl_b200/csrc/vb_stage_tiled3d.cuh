@@ -30,6 +30,7 @@ constexpr int U_XHI = U_XLO + 2 * TY * 5;
 constexpr int U_YLO = U_XHI + 2 * TY * 5;
 constexpr int U_YHI = U_YLO + 2 * TX * 5;
 constexpr uint32_t PLANE_BYTES = UPLANE * 8;
+constexpr int TMA_ISSUER = 5 * 32;  // the thread that issues a block's stage loads
 // every TMA destination in shared memory is 128-byte aligned
 static_assert((U_XLO * 8) % 128 == 0 && (U_XHI * 8) % 128 == 0 && (U_YLO * 8) % 128 == 0 &&
                   (U_YHI * 8) % 128 == 0 && (UPLANE * 8) % 128 == 0,

@@ -131,7 +131,12 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
 
     auto issue = [&](int q) {
         const int p = k0 - 2 + q;
-        const int z = perz ? ((p % nz) + nz) % nz : p;
+        // periodic wrap of the planes k0 - 2 .. k1 + 1 (a modulo only when nz < 3)
+        int z = p;
+        if (perz) {
+            z = p < 0 ? p + nz : (p >= nz ? p - nz : p);
+            if (z < 0 || z >= nz) z = ((p % nz) + nz) % nz;
+        }
         double *dst = S.u[(qb + q) % NS];
         uint64_t *bar = &S.bar[(qb + q) % NS];
         const int xl = (perx && x0 == 0) ? nx - 2 : x0 - 2;
@@ -145,7 +150,9 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
         tma_load_4d(dst + U_YLO, &tm[2], x0, yl, z, 0, bar);
         tma_load_4d(dst + U_YHI, &tm[2], x0, yh, z, 0, bar);
     };
-    if (t == 0) {
+    // the stage loads are issued by one thread of warp 5, whose share of the
+    // plane's second phase is the smallest
+    if (t == TMA_ISSUER) {
         fence_proxy_async_smem();
         for (int q = 0; q < NS && q < nplanes; ++q) issue(q);
     }
@@ -202,7 +209,7 @@ k_stage_tiled3d_f64(const __grid_constant__ BoxDesc box0, const BoxDesc *__restr
         if (keep == 1) halo_c2p(q);
     };
     auto release = [&](int q) {
-        if (t == 0 && q + NS < nplanes) {
+        if (t == TMA_ISSUER && q + NS < nplanes) {
             fence_proxy_async_smem();
             issue(q + NS);
         }
