@@ -56,8 +56,11 @@ struct Smem {
 
 }  // namespace t2
 
+// Mixed precision runs 3 CTAs per SM (80 registers, 67.5 KB of shared memory
+// each): the step is 8 % faster than at 2 CTAs with 102 registers; float64
+// keeps 2 (128 registers).
 template <bool MIXED, int NS, int STAGE, bool BF = false>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, MIXED ? 3 : 2)
 k_stage_tiled2d(const __grid_constant__ BoxDesc B, int nitems, unsigned int *work)
 {
     using namespace t2;
