@@ -16,7 +16,8 @@
 //     the plane's first barrier by warps 4..7 and after it by warps 0..3, so
 //     that it balances the halo conversions (warps 0..3) and the edge faces
 //     (warp 7) across the two phases;
-//   - face fluxes are stored once, multiplied by the face area, in float64;
+//   - x/y face fluxes are stored once in float32 and multiplied by the face
+//     area in float64 where the divergence reads them;
 //     the flux divergence and the stage update stay in float64.
 // Two barriers per plane: (1) plane k+2 converted, (2) fluxes of plane k ready.
 #pragma once
@@ -54,8 +55,8 @@ struct Smem {
     double u[NS][t3::UPLANE];  // TMA stage buffers (raw conserved state)
     double ep[2][5][NT];       // own-cell epilogue inputs (Uin, U0), fetched by cp.async
     float w[3][PSLOT];         // primitive ring
-    double gx[5][TY * (TX + 1)];  // x-face area * flux
-    double gy[5][(TY + 1) * TX];  // y-face area * flux
+    float gx[5][TY * (TX + 1)];  // x-face flux (float32; times the area in the epilogue)
+    float gy[5][(TY + 1) * TX];  // y-face flux
     uint64_t bar[NS];
 };
 
@@ -165,16 +166,16 @@ __device__ __forceinline__ void face_pair(const float *wk, const int ox[4], cons
     R = Face2{r[0], r[1], r[2], r[3], r[4]};
 }
 
-// area * flux of a packed face pair into the x / y face arrays (un-rotating
-// the y face's momentum components)
-__device__ __forceinline__ void store_pair(double (*gx)[TY * (TX + 1)], double (*gy)[(TY + 1) * TX],
-                                           int ix, int iy, double ax, double ay, const f2 F[5])
+// flux of a packed face pair into the x / y face arrays (un-rotating the y
+// face's momentum components); the epilogue multiplies by the face area
+__device__ __forceinline__ void store_pair(float (*gx)[TY * (TX + 1)], float (*gy)[(TY + 1) * TX],
+                                           int ix, int iy, const f2 F[5])
 {
-    gx[0][ix] = ax * (double)F[0].v.x;  gy[0][iy] = ay * (double)F[0].v.y;
-    gx[1][ix] = ax * (double)F[1].v.x;  gy[2][iy] = ay * (double)F[1].v.y;
-    gx[2][ix] = ax * (double)F[2].v.x;  gy[1][iy] = ay * (double)F[2].v.y;
-    gx[3][ix] = ax * (double)F[3].v.x;  gy[3][iy] = ay * (double)F[3].v.y;
-    gx[4][ix] = ax * (double)F[4].v.x;  gy[4][iy] = ay * (double)F[4].v.y;
+    gx[0][ix] = F[0].v.x;  gy[0][iy] = F[0].v.y;
+    gx[1][ix] = F[1].v.x;  gy[2][iy] = F[1].v.y;
+    gx[2][ix] = F[2].v.x;  gy[1][iy] = F[2].v.y;
+    gx[3][ix] = F[3].v.x;  gy[3][iy] = F[3].v.y;
+    gx[4][ix] = F[4].v.x;  gy[4][iy] = F[4].v.y;
 }
 
 }  // namespace t3m
@@ -445,7 +446,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         face_pair(w0, ox, oy, L, R);
         f2 F[5];
         hllc_x2(L, R, gf, ig1, F);
-        store_pair(S.gx, S.gy, ty * (TX + 1) + tx, ty * TX + tx, ax, ay, F);
+        store_pair(S.gx, S.gy, ty * (TX + 1) + tx, ty * TX + tx, F);
         if constexpr (BF) {
             if (xlo_bnd && tx == 0) {  // x-lo domain face of cell (0, y, k)
                 const double Fd[5] = {F[0].v.x, F[1].v.x, F[2].v.x, F[3].v.x, F[4].v.x};
@@ -466,7 +467,7 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         face_pair(w0, ex, ey, L, R);
         f2 F[5];
         hllc_x2(L, R, gf, ig1, F);
-        store_pair(S.gx, S.gy, j * (TX + 1) + TX, TY * TX + j, ax, ay, F);
+        store_pair(S.gx, S.gy, j * (TX + 1) + TX, TY * TX + j, F);
         if constexpr (BF) {
             if (xhi_bnd) {  // x-hi domain face of cell (nx-1, y0+j, k)
                 const double Fd[5] = {F[0].v.x, F[1].v.x, F[2].v.x, F[3].v.x, F[4].v.x};
@@ -545,10 +546,10 @@ k_stage_tiled3d_mixed(const __grid_constant__ BoxDesc box0, const BoxDesc *__res
         cp_async_wait_all();  // this thread's own epilogue inputs have landed
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
-            const double gxl = S.gx[f][ty * (TX + 1) + tx];
-            const double gxh = S.gx[f][ty * (TX + 1) + tx + 1];
-            const double gyl = S.gy[f][ty * TX + tx];
-            const double gyh = S.gy[f][(ty + 1) * TX + tx];
+            const double gxl = __dmul_rn(ax, (double)S.gx[f][ty * (TX + 1) + tx]);
+            const double gxh = __dmul_rn(ax, (double)S.gx[f][ty * (TX + 1) + tx + 1]);
+            const double gyl = __dmul_rn(ay, (double)S.gy[f][ty * TX + tx]);
+            const double gyh = __dmul_rn(ay, (double)S.gy[f][(ty + 1) * TX + tx]);
             // explicit roundings: the result must not depend on how the compiler
             // contracts this code in each kernel instantiation
             const double gzh = __dmul_rn(az, (double)Fzhi[f]);
