@@ -100,33 +100,37 @@ void release(vb_amr *a)
     cudaFreeHost(a->htot);
 }
 
+// Stream-ordered (re)allocation from the device's memory pool: a regrid that
+// grows its tables neither synchronises the device (as cudaFree does) nor
+// maps fresh memory once the pool holds enough (the pool keeps what is freed,
+// see vb_amr_create).
 template <typename T>
-int realloc_dev(T **p, int64_t count)
+int realloc_dev(T **p, int64_t count, cudaStream_t s)
 {
-    cudaFree(*p);
+    if (*p) VB_CUDA(cudaFreeAsync(*p, s));
     *p = nullptr;
-    VB_CUDA(cudaMalloc((void **)p, sizeof(T) * (size_t)(count > 0 ? count : 1)));
+    VB_CUDA(cudaMallocAsync((void **)p, sizeof(T) * (size_t)(count > 0 ? count : 1), s));
     return VB_OK;
 }
 
 // Leaf buffers other than U, lev and cx (which a refinement replaces itself).
 int alloc_leaf_buffers(vb_amr *a, int64_t c)
 {
-    int rc = realloc_dev(&a->U1, 5 * c);
-    if (!rc) rc = realloc_dev(&a->U2, 5 * c);
-    if (!rc) rc = realloc_dev(&a->lev2, c);
-    if (!rc) rc = realloc_dev(&a->cx2, 3 * c);
-    if (!rc) rc = realloc_dev(&a->reg, 5 * c);
-    if (!rc) rc = realloc_dev(&a->rep, 6 * c);
-    if (!rc) rc = realloc_dev(&a->faceid, 6 * c);
-    if (!rc) rc = realloc_dev(&a->kind, 6 * c);
-    if (!rc) rc = realloc_dev(&a->off, c + 1);
-    if (!rc) rc = realloc_dev(&a->fbase, c + 1);
-    if (!rc) rc = realloc_dev(&a->cnt, c);
-    if (!rc) rc = realloc_dev(&a->fcnt, c);
-    if (!rc) rc = realloc_dev(&a->ecnt, c);
-    if (!rc) rc = realloc_dev(&a->bsum, c / 1024 + 2);
-    if (!rc) rc = realloc_dev(&a->tag, c);
+    int rc = realloc_dev(&a->U1, 5 * c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->U2, 5 * c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->lev2, c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->cx2, 3 * c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->reg, 5 * c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->rep, 6 * c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->faceid, 6 * c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->kind, 6 * c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->off, c + 1, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->fbase, c + 1, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->cnt, c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->fcnt, c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->ecnt, c, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->bsum, c / 1024 + 2, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->tag, c, a->ctx->stream);
     if (rc) return rc;
     VB_CUDA(cudaMemsetAsync(a->reg, 0, sizeof(double) * 5 * c, a->ctx->stream));
     a->cap = c;
@@ -170,8 +174,8 @@ int build_tables(vb_amr *a)
     int64_t hc = 1024;
     while (hc < 2 * (int64_t)a->n) hc *= 2;
     if (hc != a->hcap) {
-        int rc = realloc_dev(&a->hkey, hc);
-        if (!rc) rc = realloc_dev(&a->hval, hc);
+        int rc = realloc_dev(&a->hkey, hc, a->ctx->stream);
+        if (!rc) rc = realloc_dev(&a->hval, hc, a->ctx->stream);
         if (rc) return rc;
         a->hcap = hc;
     }
@@ -187,11 +191,11 @@ int build_tables(vb_amr *a)
     if (nf > a->fcap) {
         int64_t c = a->fcap ? a->fcap : 4096;
         while (c < nf) c *= 2;
-        rc = realloc_dev(&a->fL, c);
-        if (!rc) rc = realloc_dev(&a->fR, c);
-        if (!rc) rc = realloc_dev(&a->fax, c);
-        if (!rc) rc = realloc_dev(&a->farea, c);
-        if (!rc) rc = realloc_dev(&a->F, 5 * c);
+        rc = realloc_dev(&a->fL, c, a->ctx->stream);
+        if (!rc) rc = realloc_dev(&a->fR, c, a->ctx->stream);
+        if (!rc) rc = realloc_dev(&a->fax, c, a->ctx->stream);
+        if (!rc) rc = realloc_dev(&a->farea, c, a->ctx->stream);
+        if (!rc) rc = realloc_dev(&a->F, 5 * c, a->ctx->stream);
         if (rc) return rc;
         a->fcap = c;
     }
@@ -204,7 +208,7 @@ int build_tables(vb_amr *a)
     if (ne > a->ecap) {
         int64_t c = a->ecap ? a->ecap : 8192;
         while (c < ne) c *= 2;
-        rc = realloc_dev(&a->ent, c);
+        rc = realloc_dev(&a->ent, c, a->ctx->stream);
         if (rc) return rc;
         a->ecap = c;
     }
@@ -282,22 +286,22 @@ int refine_marked(vb_amr *a, const int *gate = nullptr, int64_t *ntag = nullptr)
         // grow: fresh targets of the new capacity; the other leaf buffers follow
         double *Unew = nullptr;
         int *lev_new = nullptr, *cx_new = nullptr;
-        cudaError_t e = cudaMalloc(&Unew, sizeof(double) * 5 * cap_new);
-        if (e == cudaSuccess) e = cudaMalloc(&lev_new, sizeof(int) * cap_new);
-        if (e == cudaSuccess) e = cudaMalloc(&cx_new, sizeof(int) * 3 * cap_new);
+        cudaError_t e = cudaMallocAsync(&Unew, sizeof(double) * 5 * cap_new, s);
+        if (e == cudaSuccess) e = cudaMallocAsync(&lev_new, sizeof(int) * cap_new, s);
+        if (e == cudaSuccess) e = cudaMallocAsync(&cx_new, sizeof(int) * 3 * cap_new, s);
         if (e == cudaSuccess) e = cudaMemsetAsync(cx_new, 0, sizeof(int) * 3 * cap_new, s);
         if (e != cudaSuccess) {
-            cudaFree(Unew);
-            cudaFree(lev_new);
-            cudaFree(cx_new);
+            if (Unew) cudaFreeAsync(Unew, s);
+            if (lev_new) cudaFreeAsync(lev_new, s);
+            if (cx_new) cudaFreeAsync(cx_new, s);
             return fail(VB_ENOMEM, std::string("regrid buffers: ") + cudaGetErrorString(e));
         }
         VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_emit(t, a->tag, a->fbase, lev_new, cx_new, cap_new,
                                                     a->U, Unew, s));
-        VB_CUDA(cudaStreamSynchronize(s));
-        cudaFree(a->U);
-        cudaFree(a->lev);
-        cudaFree(a->cx);
+        // stream order: the frees follow the emit that reads the old buffers
+        VB_CUDA(cudaFreeAsync(a->U, s));
+        VB_CUDA(cudaFreeAsync(a->lev, s));
+        VB_CUDA(cudaFreeAsync(a->cx, s));
         a->U = Unew;
         a->lev = lev_new;
         a->cx = cx_new;
@@ -543,6 +547,17 @@ int vb_amr_create(vb_ctx *ctx, const vb_problem_desc *d, vb_amr **out)
         if (g.n[k] >= (1LL << CBITS)) return fail(VB_EINVAL, "base grid too large for AMR keys");
     rc = use(ctx);
     if (rc) return rc;
+    {
+        // the regrids' stream-ordered allocations come from the device's
+        // default memory pool of this process: let it keep freed memory for
+        // reuse instead of returning it at every synchronisation
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
     vb_amr *a = new (std::nothrow) vb_amr;
     if (!a) return fail(VB_ENOMEM, "host allocation failed");
     a->ctx = ctx;
@@ -599,9 +614,9 @@ int vb_amr_create(vb_ctx *ctx, const vb_problem_desc *d, vb_amr **out)
         cx0[cap + i] = (int)((i / a->base[0]) % a->base[1]);
         cx0[2 * cap + i] = (int)(i / (a->base[0] * a->base[1]));
     }
-    rc = realloc_dev(&a->U, 5 * cap);
-    if (!rc) rc = realloc_dev(&a->lev, cap);
-    if (!rc) rc = realloc_dev(&a->cx, 3 * cap);
+    rc = realloc_dev(&a->U, 5 * cap, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->lev, cap, a->ctx->stream);
+    if (!rc) rc = realloc_dev(&a->cx, 3 * cap, a->ctx->stream);
     if (!rc) rc = alloc_leaf_buffers(a, cap);
     if (!rc && (cudaMemcpy(a->lev, lev0.data(), sizeof(int) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
                 cudaMemcpy(a->cx, cx0.data(), sizeof(int) * 3 * cap, cudaMemcpyHostToDevice) != cudaSuccess))
