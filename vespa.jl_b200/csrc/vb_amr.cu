@@ -753,12 +753,12 @@ int vb_amr_indicator(vb_amr *a, double *out)
     if (rc) return rc;
     const int64_t n = a->n;
     double *d = nullptr;
-    VB_CUDA(cudaMalloc(&d, sizeof(double) * (n > 0 ? n : 1)));
+    VB_CUDA(cudaMallocAsync(&d, sizeof(double) * (n > 0 ? n : 1), a->ctx->stream));
     VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_tag(a->dev, a->U, INFINITY, 0, a->tag, d, nullptr,
                                                a->ctx->stream));
     cudaError_t e = cudaMemcpyAsync(out, d, sizeof(double) * n, cudaMemcpyDeviceToHost, a->ctx->stream);
+    cudaFreeAsync(d, a->ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(a->ctx->stream);
-    cudaFree(d);
     if (e != cudaSuccess) return fail(VB_ECUDA, cudaGetErrorString(e));
     return VB_OK;
 }
