@@ -62,8 +62,9 @@ struct vb_amr {
     int64_t hcap = 0;
     uint64_t *hkey = nullptr;
     int *hval = nullptr;
-    // small device words: [0] error bits, [1] unused, [2] max level, [3] scan total, [4] tags,
-    // [8, 8 + BAL_GROUP) marks changed by each balance pass of a group
+    // small device words: [0] error bits, [1] unused, [2] max level, [3] scan total (faces
+    // in a table build), [4] tags, [5] entries of a table build, [8, 8 + BAL_GROUP) marks
+    // changed by each balance pass of a group
     int *word = nullptr, *hword = nullptr;
     vb::Ctrl *ctrl = nullptr, *hctrl = nullptr;
     double *partials = nullptr, *totals = nullptr, *htot = nullptr;
@@ -179,18 +180,16 @@ int build_tables(vb_amr *a)
         if (rc) return rc;
         a->hcap = hc;
     }
-    VB_CUDA(cudaMemsetAsync(a->word, 0, sizeof(int) * NWORD, s));
-    vb::AmrTopo t = topo(a);
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_hash_build(t, a->hkey, a->hval, a->word, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_kinds(t, a->kind, a->rep, a->fcnt, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->fcnt, a->n, a->fbase, a->bsum, a->word + 3, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_csr_count(t, a->kind, a->fcnt, a->ecnt, s));
-    int rc = sync_words(a);
-    if (rc) return rc;
-    const int nf = a->hword[3];
-    if (nf > a->fcap) {
+    // Face and entry arrays sized for the most these leaves can have (a leaf
+    // emits at most its hi and lo face per axis; its CSR holds those and at
+    // most 2^(nd-1) finer faces per side), so the whole build queues behind
+    // one read of the totals and the error bits.
+    const int64_t nf_max = 2ll * a->nd * a->n;
+    const int64_t ne_max = nf_max * (1 + (1 << (a->nd - 1)));
+    int rc = VB_OK;
+    if (nf_max > a->fcap) {
         int64_t c = a->fcap ? a->fcap : 4096;
-        while (c < nf) c *= 2;
+        while (c < nf_max) c *= 2;
         rc = realloc_dev(&a->fL, c, a->ctx->stream);
         if (!rc) rc = realloc_dev(&a->fR, c, a->ctx->stream);
         if (!rc) rc = realloc_dev(&a->fax, c, a->ctx->stream);
@@ -199,24 +198,30 @@ int build_tables(vb_amr *a)
         if (rc) return rc;
         a->fcap = c;
     }
-    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_faces(t, a->kind, a->rep, a->fbase, a->areas, a->fL,
-                                                 a->fR, a->fax, a->farea, a->faceid, s));
-    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->ecnt, a->n, a->off, a->bsum, a->word + 3, s));
-    rc = sync_words(a);
-    if (rc) return rc;
-    const int ne = a->hword[3];
-    if (ne > a->ecap) {
+    if (ne_max > a->ecap) {
         int64_t c = a->ecap ? a->ecap : 8192;
-        while (c < ne) c *= 2;
+        while (c < ne_max) c *= 2;
         rc = realloc_dev(&a->ent, c, a->ctx->stream);
         if (rc) return rc;
         a->ecap = c;
     }
+    VB_CUDA(cudaMemsetAsync(a->word, 0, sizeof(int) * NWORD, s));
+    vb::AmrTopo t = topo(a);
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_hash_build(t, a->hkey, a->hval, a->word, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_kinds(t, a->kind, a->rep, a->fcnt, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->fcnt, a->n, a->fbase, a->bsum, a->word + 3, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_csr_count(t, a->kind, a->fcnt, a->ecnt, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_faces(t, a->kind, a->rep, a->fbase, a->areas, a->fL,
+                                                 a->fR, a->fax, a->farea, a->faceid, s));
+    VB_CHECK_LAUNCH(a->ctx, vb::amr_scan(a->ecnt, a->n, a->off, a->bsum, a->word + 5, s));
     VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_csr_fill(t, a->kind, a->rep, a->faceid, a->off,
                                                     a->ent, a->word, s));
     rc = sync_words(a);
     if (rc) return rc;
+    const int nf = a->hword[3];
+    const int ne = a->hword[5];
     if (a->hword[0]) return fail(VB_ECUDA, "AMR table build failed (hash or CSR overflow)");
+    if (nf > a->fcap || ne > a->ecap) return fail(VB_ECUDA, "AMR table build: face count out of range");
     a->nface = nf;
     a->nent = ne;
     vb::AmrDev &m = a->dev;
@@ -886,8 +891,9 @@ int vb_amr_evolve(vb_amr *a, double tfinal, int64_t max_steps, double refine_abo
             a->hctrl->step_limit = a->step + chunk;
             a->hctrl->active = 1;
             a->hctrl->flags = 0;
-            rc = push_ctrl(a);
-            if (rc) return rc;
+            // queued, not awaited: the host writes hctrl again only after the
+            // pull below has synchronised the stream
+            VB_CUDA(cudaMemcpyAsync(a->ctrl, a->hctrl, sizeof(vb::Ctrl), cudaMemcpyHostToDevice, st));
             VB_CUDA(cudaMemsetAsync(&a->ctrl->invdt_bits, 0, sizeof(unsigned long long), st));
             VB_CHECK_LAUNCH(a->ctx, vb::launch_amr_cfl(a->dev, a->U, -1, a->ctrl, st));
             vb::AmrStageArgs s{};
