@@ -349,8 +349,10 @@ def run_ours(args, ranks: Ranks):
         vb.run_steps_async(warm, 8)
         ctx.synchronize()
     warm.close()
+    drift = {}
     for prec in ("fp64", "mixed"):
         sim = vb.Simulation(mesh, prob, precision=prec, ctx=ctx, initial=U0)
+        tot0 = np.array(vb.conserved_totals(sim))
         kz, _ = sim.autotune(3)  # setup: pick the z-chunk; state and clock restored
         vb.run_steps_async(sim, W)
         ctx.synchronize()
@@ -366,6 +368,11 @@ def run_ours(args, ranks: Ranks):
         ranks.barrier()
         ms_max = ranks.max(ms)
         finals[prec] = sim.state()[0]  # density after W + K steps, for the L1 check
+        # conservation over the W + K steps of this periodic box: relative
+        # drift of mass and energy (the momenta start near zero)
+        tot1 = np.array(vb.conserved_totals(sim))
+        drift[prec] = {"mass": float(abs(tot1[0] - tot0[0]) / abs(tot0[0])),
+                       "energy": float(abs(tot1[4] - tot0[4]) / abs(tot0[4]))}
         out[prec] = {"ms": ms_max, "launches": launches, "kernel": sim.kernel, "kz": kz,
                      "taper": sim.taper, **sim.profile_step(5)}
         sim.close()
@@ -440,7 +447,7 @@ def run_ours(args, ranks: Ranks):
                    "l2": "inputs larger than L2 (671 MB per state buffer)",
                    "parallelism": f"one independent instance per GPU x{ranks.world}"},
         "accuracy": {"l1_rho_mixed_vs_fp64_rel": l1_mixed, "after_steps": W + K,
-                     "bound": 1e-6},
+                     "bound": 1e-6, "conservation_drift_rel": drift},
         "fp64": {"value": round(fp64_value, 1), "unit": UNIT,
                  "ms_per_step": round(out["fp64"]["ms"] / K, 4),
                  "tile": f"16x16 columns, z chunk {out['fp64']['kz']}, "
