@@ -41,9 +41,9 @@ struct alignas(64) BoxDesc {
 // planes: a remainder of 16 planes or more gives up half of itself (rounded
 // down), a smaller one is taken whole.  With kz >= 16 every piece then has 8
 // to kz planes and the last one fewer than 16, so that the work queue ends on
-// short items and the blocks finish together.  The tapered form is used by
-// single VB_MIXED grids (measured 2 % faster at 256^3); the float64 and batch
-// launches keep the uniform chunks.
+// short items and the blocks finish together.  Single grids take the form the
+// autotuner timed faster (the tapered one at 256^3 in both precisions; a
+// VB_MIXED grid defaults to it); batches keep the uniform chunks.
 __host__ __device__ inline int chunk_tail_piece(int r, int kz)
 {
     const int p = r >= 16 ? r / 2 : r;
