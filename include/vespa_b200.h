@@ -291,8 +291,9 @@ int vb_bflux_plane(vb_grid *grid, int dim, int source, const int64_t *start, con
  * While gravity is enabled: vb_evolve and vb_run_steps_async solve once per
  * step before the stages (evolve!, src/driver.jl:498) and synchronise with
  * the host for it; vb_step uses the field of the last solve (or set_phi), as
- * step! does; the stages take the cell-centric kernel.  The adjoint refuses
- * a grid with gravity (VB_ENOTSUP). */
+ * step! does; the stages of a 3D grid take the tiled kernels with the source
+ * added (1D and 2D grids the cell-centric kernel).  The adjoint refuses a
+ * grid with gravity (VB_ENOTSUP). */
 enum {
     VB_GRAV_PRECOND_NONE = 0, /* plain CG (the reference's default) */
     VB_GRAV_PRECOND_MG = 1    /* CG preconditioned by one base-grid multigrid cycle

@@ -50,7 +50,7 @@ struct vb_grid {
     uint64_t gkey = 0;                  // kernel configuration it was captured for
     int64_t glaunches = 0;              // kernels per replay
     bool warmed = false;                // one direct step ran (launch setup done)
-    vb_gravity *grav = nullptr;         // self-gravity (stages take the cell-centric kernel)
+    vb_gravity *grav = nullptr;         // self-gravity (a solve per step; source in the stages)
     bool slab = false;                  // a z window is set (vb_grid_set_zwindow): tiled kernels only
 };
 

@@ -8,8 +8,8 @@
 // k_stage_tiled3d_mixed (VB_MIXED, vb_stage_tiled3d_mixed.cuh).
 //
 // Requirements (checked on the host): nx % 16 == 0, ny % 16 == 0, nz >= 2, and
-// a periodic axis is periodic on both sides.  Boundary-flux capture is not
-// done here (the cell-centric kernel handles grids with bflux enabled).
+// a periodic axis is periodic on both sides.  The BF instantiations record the
+// domain-boundary faces' fluxes in the boundary-flux register (bflux_add).
 #pragma once
 
 #include <cstring>
