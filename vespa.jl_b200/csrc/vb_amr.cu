@@ -104,7 +104,7 @@ void release(vb_amr *a)
 // Stream-ordered (re)allocation from the device's memory pool: a regrid that
 // grows its tables neither synchronises the device (as cudaFree does) nor
 // maps fresh memory once the pool holds enough (the pool keeps what is freed,
-// see vb_amr_create).
+// see vb_ctx_create).
 template <typename T>
 int realloc_dev(T **p, int64_t count, cudaStream_t s)
 {
@@ -552,17 +552,6 @@ int vb_amr_create(vb_ctx *ctx, const vb_problem_desc *d, vb_amr **out)
         if (g.n[k] >= (1LL << CBITS)) return fail(VB_EINVAL, "base grid too large for AMR keys");
     rc = use(ctx);
     if (rc) return rc;
-    {
-        // the regrids' stream-ordered allocations come from the device's
-        // default memory pool of this process: let it keep freed memory for
-        // reuse instead of returning it at every synchronisation
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
-            uint64_t keep = UINT64_MAX;
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-        }
-        cudaGetLastError();
-    }
     vb_amr *a = new (std::nothrow) vb_amr;
     if (!a) return fail(VB_ENOMEM, "host allocation failed");
     a->ctx = ctx;

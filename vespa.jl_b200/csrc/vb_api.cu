@@ -577,6 +577,20 @@ int vb_ctx_create(int device, vb_ctx **out)
         delete ctx;
         return fail(VB_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
     }
+    {
+        // scratch that comes and goes (autotuner copies, the AMR tables as
+        // they grow) is allocated stream-ordered from the device's default
+        // memory pool of this process; let the pool keep freed memory for
+        // reuse instead of returning it at every synchronisation (a
+        // cudaFree synchronises the whole device and at times took hundreds
+        // of milliseconds)
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
     *out = ctx;
     return VB_OK;
 }
@@ -781,7 +795,7 @@ int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
     }
     const size_t bytes = sizeof(double) * 5 * (size_t)gr->g.ncell;
     double *save = nullptr;
-    VB_CUDA(cudaMalloc(&save, bytes));
+    VB_CUDA(cudaMallocAsync(&save, bytes, gr->ctx->stream));
     cudaStream_t s = gr->ctx->stream;
     rc = pull_ctrl(gr);
     vb::Ctrl ctrl0 = *gr->hctrl;
@@ -829,7 +843,7 @@ int vb_grid_autotune(vb_grid *gr, int nsteps, int64_t *best_kz, double *best_ms)
     cudaMemcpyAsync(gr->U, save, bytes, cudaMemcpyDeviceToDevice, s);
     *gr->hctrl = ctrl0;
     int rc2 = push_ctrl(gr);
-    cudaFree(save);
+    cudaFreeAsync(save, s);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     gr->invdt_valid = false;

@@ -339,14 +339,15 @@ int vb_batch_autotune(vb_batch *b, int nsteps, int64_t *best_cap, double *best_m
     // candidates' steps are undone afterwards
     std::vector<double *> save(b->nbox, nullptr);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    auto cleanup = [&]() {
-        for (double *p : save) cudaFree(p);
+    auto cleanup = [&]() {  // stream-ordered: no device-wide synchronisation
+        for (double *p : save)
+            if (p) cudaFreeAsync(p, s);
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
     };
     for (int i = 0; i < b->nbox && !rc; ++i) {
         const size_t bytes = sizeof(double) * 5 * (size_t)b->geom[i].ncell;
-        if (cudaMalloc(&save[i], bytes) != cudaSuccess ||
+        if (cudaMallocAsync(&save[i], bytes, s) != cudaSuccess ||
             cudaMemcpyAsync(save[i], b->U[i], bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
             rc = fail(VB_ENOMEM, "autotune: no room for a copy of the batch state");
     }
